@@ -1,0 +1,95 @@
+"""ctypes binding of ``libfastpls_b200.so`` (the C ABI in include/fastpls_b200.h).
+
+There is no CPU fallback: importing works without a GPU, but every compute
+call goes through the CUDA library, and a missing library raises at load.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfastpls_b200.so")
+
+_vp, _i, _d, _sz = C.c_void_p, C.c_int, C.c_double, C.c_size_t
+_ull = C.c_ulonglong
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+_cp = C.c_char_p
+
+# name -> (restype, argtypes); mirrors include/fastpls_b200.h
+SIGNATURES = {
+    "fastpls_cuda_gemm": (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _cp, _sz]),
+    "fastpls_resident_simpls_cv_classification": (
+        _i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _i, _i, _i, _i, _i, _ull, _i,
+             _i, _vp, _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_simpls_cv_regression": (
+        _i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _i, _i, _i, _i, _i, _ull, _i,
+             _vp, _vp, _vp, _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_plssvd_cv_classification": (
+        _i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _i, _i, _i, _i, _i, _ull, _i,
+             _i, _vp, _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_plssvd_cv_regression": (
+        _i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _i, _i, _i, _i, _i, _ull, _i,
+             _vp, _vp, _vp, _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_simpls_create": (
+        _vp, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _ull, _cp, _sz]),
+    "fastpls_resident_plssvd_create": (
+        _vp, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _ull, _cp, _sz]),
+    "fastpls_resident_opls_create": (
+        _vp, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _ull, _i, _cp,
+              _sz]),
+    "fastpls_resident_kernelpls_create": (
+        _vp, [_vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i, _ull, _i, _d,
+              _i, _d, _cp, _sz]),
+    "fastpls_resident_predict_path": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp, _cp, _sz]),
+    "fastpls_resident_simpls_destroy": (None, [_vp]),
+    "fastpls_resident_export": (_i, [_vp, _i, _vp, _sz, _cp, _sz]),
+    "fastpls_resident_classify_path": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp, _cp, _sz]),
+    "fastpls_resident_classify_response_path": (
+        _i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_response_sums": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp, _cp, _sz]),
+    "fastpls_resident_project": (_i, [_vp, _vp, _i, _i, _vp, _cp, _sz]),
+    "fastpls_resident_controls": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_resident_compact": (_i, [_vp, _i, _cp, _sz]),
+    "fastpls_b200_device_count": (_i, []),
+    "fastpls_b200_launch_count": (_ull, []),
+    "fastpls_b200_simpls_cv_permutation": (
+        _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp,
+             _vp, _vp, _vp, _cp, _sz]),
+    "fastpls_b200_simpls_cv_permutation_device": (
+        _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp,
+             _vp, _vp, _vp, _cp, _sz]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the library once; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m fastpls_b200.build`"
+                " (the fitting path has no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class FastplsError(RuntimeError):
+    """Error reported by the CUDA library through its error buffer."""
+
+
+def error_buffer(size: int = 1024):
+    return C.create_string_buffer(size), C.c_size_t(size)
+
+
+def check(rc: int, err) -> None:
+    if rc != 0:
+        raise FastplsError(err.value.decode(errors="replace"))

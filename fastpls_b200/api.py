@@ -1,0 +1,334 @@
+"""Python mirror of the fastPLS R API for the CUDA path (``backend = "cuda"``).
+
+Names, arguments and defaults follow the reference's R functions
+(R/main.R: pls 9746, predict.fastPLS 5206, pls.single.cv 10985;
+R/native_api.R: has_cuda 601); the computation happens in
+``libfastpls_b200.so`` through its C ABI. Matrices are numpy arrays with
+rows = samples; they are handed to the library column-major.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+SCALING = {"centering": 1, "autoscaling": 2, "none": 3}
+METHODS = {"plssvd": 1, "simpls": 3, "opls": 4, "kernelpls": 5}
+KERNELS = {"rbf": 2, "poly": 3}
+METRICS = {"r2": 2, "q2": 3, "rmsd": 4}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _mat(a, dtype):
+    a = np.asarray(a, dtype=dtype)
+    if a.ndim == 1:
+        a = a[:, None]
+    return np.asfortranarray(a)
+
+
+def _dtype(precision):
+    if precision not in (32, 64):
+        raise ValueError("precision must be 32 or 64")
+    return np.float32 if precision == 32 else np.float64
+
+
+def has_cuda() -> bool:
+    """True when a CUDA device is visible (has_cuda(), R/native_api.R:601)."""
+    return _lib.load().fastpls_b200_device_count() > 0
+
+
+def launch_count() -> int:
+    return int(_lib.load().fastpls_b200_launch_count())
+
+
+def encode_labels(y):
+    """Factor-style encoding: sorted unique levels -> one-based codes."""
+    levels, codes = np.unique(np.asarray(y), return_inverse=True)
+    return (codes + 1).astype(np.int32), levels
+
+
+@dataclass
+class ResidentModel:
+    """A model resident on the GPU (the R package's EXTPTR handle)."""
+
+    handle: int
+    precision: int
+    n: int
+    p: int
+    q: int
+    ncomp: int
+    method: str
+    classification: bool
+    levels: np.ndarray | None = None
+    _freed: bool = field(default=False, repr=False)
+
+    @property
+    def dtype(self):
+        return _dtype(self.precision)
+
+    def close(self):
+        if not self._freed and self.handle:
+            _lib.load().fastpls_resident_simpls_destroy(C.c_void_p(self.handle))
+            self._freed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- exports (fastpls_resident_export field ids) ----
+    def export(self, field_id: int) -> np.ndarray:
+        a, q, p, n = self.ncomp, self.q, self.p, self.n
+        shapes = {0: (p, a), 1: (q, a), 2: (n, a), 3: (p,), 4: (p,), 5: (q,),
+                  6: (p, a), 7: (a + 1,)}
+        shape = shapes[field_id]
+        out = np.zeros(shape, dtype=self.dtype, order="F")
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_export(
+            C.c_void_p(self.handle), field_id, _p(out), out.size, err, cap)
+        _lib.check(rc, err)
+        return out
+
+    def weights(self):
+        return self.export(0)
+
+    def loadings(self):
+        return self.export(1)
+
+    def scores(self):
+        return self.export(2)
+
+    def predict_path(self, x, prefixes, lda=False) -> np.ndarray:
+        x = _mat(x, self.dtype)
+        pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+        rows = x.shape[0]
+        out = np.zeros(rows * self.q * len(pre), dtype=self.dtype)
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_predict_path(
+            C.c_void_p(self.handle), _p(x), rows, _p(pre), len(pre), int(lda),
+            _p(out), err, cap)
+        _lib.check(rc, err)
+        return out.reshape((len(pre), self.q, rows)).transpose(0, 2, 1)
+
+    def classify_path(self, x, prefixes, lda=False, top=1, responses=False):
+        x = _mat(x, self.dtype)
+        pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+        rows = x.shape[0]
+        labels = np.zeros(rows * top * len(pre), dtype=np.int32)
+        err, cap = _lib.error_buffer()
+        if responses:
+            resp = np.zeros(rows * self.q * len(pre), dtype=self.dtype)
+            rc = _lib.load().fastpls_resident_classify_response_path(
+                C.c_void_p(self.handle), _p(x), rows, _p(pre), len(pre),
+                int(lda), top, _p(labels), _p(resp), err, cap)
+        else:
+            resp = None
+            rc = _lib.load().fastpls_resident_classify_path(
+                C.c_void_p(self.handle), _p(x), rows, _p(pre), len(pre),
+                int(lda), top, _p(labels), err, cap)
+        _lib.check(rc, err)
+        lab = labels.reshape((len(pre), top, rows)).transpose(0, 2, 1)
+        if responses:
+            return lab, resp.reshape((len(pre), self.q, rows)).transpose(0, 2, 1)
+        return lab
+
+    def project(self, x, prefix):
+        x = _mat(x, self.dtype)
+        rows = x.shape[0]
+        out = np.zeros((rows, prefix), dtype=self.dtype, order="F")
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_project(
+            C.c_void_p(self.handle), _p(x), rows, int(prefix), _p(out), err, cap)
+        _lib.check(rc, err)
+        return out
+
+    def response_sums(self, x, y=None, labels=None, prefix=None):
+        x = _mat(x, self.dtype)
+        rows = x.shape[0]
+        prefix = self.ncomp if prefix is None else prefix
+        yy = None if y is None else _mat(y, self.dtype)
+        lab = None if labels is None else np.ascontiguousarray(labels, dtype=np.int32)
+        out = np.zeros(3 * self.q, dtype=self.dtype)
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_response_sums(
+            C.c_void_p(self.handle), _p(x), _p(yy), _p(lab), rows, int(prefix),
+            _p(out), err, cap)
+        _lib.check(rc, err)
+        return out.reshape((self.q, 3))
+
+    def controls(self):
+        vals = [C.c_int(0) for _ in range(6)]
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_controls(
+            C.c_void_p(self.handle), *[C.byref(v) for v in vals], err, cap)
+        _lib.check(rc, err)
+        keys = ["oversample", "power", "block", "block_limit",
+                "implicit_operator", "predictor_crossprod_cache"]
+        return {k: v.value for k, v in zip(keys, vals)}
+
+    def compact(self, prepare_lda=False):
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_resident_compact(
+            C.c_void_p(self.handle), int(prepare_lda), err, cap)
+        _lib.check(rc, err)
+
+
+def fit_resident(X, Y=None, labels=None, classes=None, ncomp=2,
+                 scaling="centering", method="simpls", precision=64,
+                 oversample=32, power=5, seed=1, retain_scores=True,
+                 north=1, kernel="rbf", gamma=None, degree=3, coef0=1.0):
+    """Fit one resident model through ``fastpls_resident_<method>_create``."""
+    dt = _dtype(precision)
+    x = _mat(X, dt)
+    n, p = x.shape
+    lib = _lib.load()
+    err, cap = _lib.error_buffer()
+    if labels is not None:
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        q = int(classes if classes is not None else lab.max())
+        y = None
+    else:
+        y = _mat(Y, dt)
+        q = y.shape[1]
+        lab = None
+    sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
+    common = (_p(x), _p(y), _p(lab), precision, n, p, q, int(ncomp), sc,
+              int(oversample), int(power), int(retain_scores), C.c_ulonglong(seed))
+    if method == "simpls":
+        h = lib.fastpls_resident_simpls_create(*common, err, cap)
+    elif method == "plssvd":
+        h = lib.fastpls_resident_plssvd_create(*common, err, cap)
+    elif method == "opls":
+        h = lib.fastpls_resident_opls_create(*common, int(north), err, cap)
+    elif method == "kernelpls":
+        g = float(gamma) if gamma is not None else 1.0 / p
+        h = lib.fastpls_resident_kernelpls_create(
+            *common, KERNELS[kernel], g, int(degree), float(coef0), err, cap)
+    else:
+        raise ValueError(f"unknown method {method!r}")
+    if not h:
+        raise _lib.FastplsError(err.value.decode(errors="replace"))
+    feature_p = n if method == "kernelpls" else p
+    return ResidentModel(handle=h, precision=precision, n=n, p=feature_p, q=q,
+                         ncomp=int(ncomp), method=method,
+                         classification=labels is not None)
+
+
+def cuda_gemm(left, right, precision=64):
+    dt = _dtype(precision)
+    a = _mat(left, dt)
+    b = _mat(right, dt)
+    out = np.zeros((a.shape[0], b.shape[1]), dtype=dt, order="F")
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_cuda_gemm(_p(a), _p(b), precision, a.shape[0],
+                                       a.shape[1], b.shape[1], _p(out), err, cap)
+    _lib.check(rc, err)
+    return out
+
+
+def cv_regression(X, Y, folds, prefixes, scaling="centering", method="simpls",
+                  metric="q2", precision=64, store_predictions=False,
+                  oversample=32, power=5, seed=1):
+    """``fastpls_resident_{simpls,plssvd}_cv_regression``."""
+    dt = _dtype(precision)
+    x = _mat(X, dt)
+    y = _mat(Y, dt)
+    n, p = x.shape
+    q = y.shape[1]
+    folds = np.ascontiguousarray(folds, dtype=np.int32)
+    pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+    k = len(pre)
+    nf = int(folds.max()) if folds.size else 0
+    status = np.zeros(max(nf, 1), dtype=np.int32)
+    metrics, q2, rmsd, r2 = (np.zeros(k) for _ in range(4))
+    preds = np.zeros(k * n * q) if store_predictions else None
+    sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
+    fn = {"simpls": "fastpls_resident_simpls_cv_regression",
+          "plssvd": "fastpls_resident_plssvd_cv_regression"}[method]
+    err, cap = _lib.error_buffer()
+    rc = getattr(_lib.load(), fn)(
+        _p(x), _p(y), _p(folds), precision, n, p, q, _p(pre), k, sc,
+        METRICS[metric] if isinstance(metric, str) else int(metric),
+        int(oversample), int(power), C.c_ulonglong(seed), int(store_predictions),
+        _p(preds), _p(status), _p(metrics), _p(q2), _p(rmsd), _p(r2), err, cap)
+    _lib.check(rc, err)
+    out = dict(metrics=metrics, q2=q2, rmsd=rmsd, observed_r2=r2, status=status,
+               predictions=None)
+    if preds is not None:
+        out["predictions"] = preds.reshape((k, q, n)).transpose(0, 2, 1)
+    return out
+
+
+def cv_classification(X, labels, classes, folds, prefixes, scaling="centering",
+                      method="simpls", lda=False, precision=64,
+                      store_predictions=False, store_scores=False,
+                      oversample=32, power=5, seed=1):
+    """``fastpls_resident_{simpls,plssvd}_cv_classification``."""
+    dt = _dtype(precision)
+    x = _mat(X, dt)
+    n, p = x.shape
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    folds = np.ascontiguousarray(folds, dtype=np.int32)
+    pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+    k = len(pre)
+    nf = int(folds.max()) if folds.size else 0
+    status = np.zeros(max(nf, 1), dtype=np.int32)
+    metrics = np.zeros(k)
+    preds = np.zeros(n * k, dtype=np.int32) if store_predictions else None
+    scores = np.zeros(n * int(classes) * k, dtype=dt) if store_scores else None
+    sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
+    fn = {"simpls": "fastpls_resident_simpls_cv_classification",
+          "plssvd": "fastpls_resident_plssvd_cv_classification"}[method]
+    err, cap = _lib.error_buffer()
+    rc = getattr(_lib.load(), fn)(
+        _p(x), _p(lab), _p(folds), precision, n, p, int(classes), _p(pre), k, sc,
+        int(lda), int(oversample), int(power), C.c_ulonglong(seed),
+        int(store_predictions), int(store_scores), _p(preds), _p(scores),
+        _p(status), _p(metrics), err, cap)
+    _lib.check(rc, err)
+    out = dict(metrics=metrics, status=status, predictions=None, scores=None)
+    if preds is not None:
+        out["predictions"] = preds.reshape((k, n)).T
+    if scores is not None:
+        out["scores"] = scores.reshape((k, int(classes), n)).transpose(0, 2, 1)
+    return out
+
+
+def cv_permutation(X, Y, folds, permutations, prefixes, scaling="centering",
+                   metric="q2", precision=32):
+    """Batched CV over the observed responses and their row permutations
+    (``fastpls_b200_simpls_cv_permutation``). Returns arrays of shape
+    (permutations + 1, prefixes), row 0 the observed responses."""
+    dt = _dtype(precision)
+    x = _mat(X, dt)
+    y = _mat(Y, dt)
+    n, p = x.shape
+    q = y.shape[1]
+    folds = np.ascontiguousarray(folds, dtype=np.int32)
+    perms = None
+    P = 0
+    if permutations is not None and len(permutations):
+        perms = np.ascontiguousarray(permutations, dtype=np.int32)
+        P = perms.shape[0]
+    pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+    k = len(pre)
+    metrics, q2, rmsd, r2 = (np.zeros((P + 1) * k) for _ in range(4))
+    status = np.zeros(int(folds.max()), dtype=np.int32)
+    sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_b200_simpls_cv_permutation(
+        _p(x), _p(y), _p(folds), _p(perms), P, precision, n, p, q, _p(pre), k,
+        sc, METRICS[metric] if isinstance(metric, str) else int(metric),
+        _p(metrics), _p(q2), _p(rmsd), _p(r2), _p(status), err, cap)
+    _lib.check(rc, err)
+    shape = (P + 1, k)
+    return dict(metrics=metrics.reshape(shape), q2=q2.reshape(shape),
+                rmsd=rmsd.reshape(shape), observed_r2=r2.reshape(shape),
+                status=status)

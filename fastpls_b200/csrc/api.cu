@@ -1,0 +1,490 @@
+// The C ABI of the library (declared in include/fastpls_b200.h).
+//
+// The first twenty entry points keep the names, signatures, argument meaning
+// and error behaviour of the reference's CUDA ABI (src/cuda_resident_api.h
+// and the extern "C" shims of src/cuda_resident_api.cuh:1026-1353): return
+// 0 / non-null on success, 1 / NULL on error with a NUL-terminated message
+// in the caller's buffer; nothing throws across the boundary.
+#include "../../include/fastpls_b200.h"
+
+#include "batched.cuh"
+#include "cv.cuh"
+#include "handle.cuh"
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+
+namespace fpls {
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+void write_error(char* out, size_t cap, const char* message) noexcept {
+  if (out && cap) std::snprintf(out, cap, "%s", message);
+}
+
+template <class F>
+int guarded(char* error, size_t cap, const char* fallback, F&& body) noexcept {
+  write_error(error, cap, "");
+  try {
+    body();
+    return 0;
+  } catch (const std::exception& e) {
+    write_error(error, cap, e.what());
+    return 1;
+  } catch (...) {
+    write_error(error, cap, fallback);
+    return 1;
+  }
+}
+
+template <class F>
+void* guarded_create(char* error, size_t cap, const char* fallback, F&& body) noexcept {
+  write_error(error, cap, "");
+  try {
+    return body();
+  } catch (const std::exception& e) {
+    write_error(error, cap, e.what());
+    return nullptr;
+  } catch (...) {
+    write_error(error, cap, fallback);
+    return nullptr;
+  }
+}
+
+template <class T>
+void host_gemm(const T* left, const T* right, int rows, int inner, int columns,
+               T* output) {
+  cudaStream_t s = nullptr;
+  FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct Guard {
+    cudaStream_t s;
+    ~Guard() {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  } guard{s};
+  DeviceArray<T> a((size_t)rows * inner, s), b((size_t)inner * columns, s);
+  DeviceArray<double> c((size_t)rows * columns, s);
+  FPLS_CHECK(cudaMemcpyAsync(a.get(), left, sizeof(T) * rows * inner, cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(b.get(), right, sizeof(T) * inner * columns, cudaMemcpyHostToDevice, s));
+  GemmArgs g;
+  g.M = rows;
+  g.N = columns;
+  g.K = inner;
+  g.A = a.get();
+  g.lda = rows;
+  g.a_f32 = std::is_same<T, float>::value;
+  g.B = b.get();
+  g.ldb = inner;
+  g.b_f32 = g.a_f32;
+  g.C = c.get();
+  g.ldc = rows;
+  gemm_f64(g, s);
+  std::vector<double> host((size_t)rows * columns);
+  FPLS_CHECK(cudaMemcpyAsync(host.data(), c.get(), sizeof(double) * host.size(), cudaMemcpyDeviceToHost, s));
+  FPLS_CHECK(cudaStreamSynchronize(s));
+  for (size_t k = 0; k < host.size(); ++k) output[k] = static_cast<T>(host[k]);
+}
+
+FitRequest request(int method, const void* x, const void* y, const int* labels,
+                   int n, int p, int q, int components, int scaling,
+                   int oversample, int power, int retain, unsigned long long seed) {
+  FitRequest r;
+  r.method = method;
+  r.x = x;
+  r.y = y;
+  r.labels = labels;
+  r.n = n;
+  r.p = p;
+  r.q = q;
+  r.components = components;
+  r.scaling = scaling;
+  r.oversample = oversample;
+  r.power = power;
+  r.retain_scores = retain == 1;
+  r.seed = seed;
+  return r;
+}
+
+template <class T>
+void cv_permutation(const void* predictors, const void* responses,
+                    const int* folds, const int* permutations,
+                    int permutation_count, int n, int p, int q,
+                    const int* prefixes, int prefix_count, int scaling,
+                    int metric, double* metrics, double* q2, double* rmsd,
+                    double* observed_r2, int* status, bool device_inputs) {
+  if (!predictors || !responses || !folds || !prefixes || !metrics || n < 2 ||
+      p < 1 || q < 1 || prefix_count < 1 || scaling < 1 || scaling > 3 ||
+      metric < 2 || metric > 4 || permutation_count < 0 ||
+      (permutation_count > 0 && !permutations))
+    throw std::invalid_argument("invalid batched CUDA CV permutation input");
+  cudaStream_t s = nullptr;
+  FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct Guard {
+    cudaStream_t s;
+    ~Guard() {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  } guard{s};
+  {
+    DeviceArray<T> X, Y;
+    DeviceArray<int> P;
+    std::vector<int> host_folds;
+    const T* xd = static_cast<const T*>(predictors);
+    const T* yd = static_cast<const T*>(responses);
+    const int* pd = permutations;
+    const int* fh = folds;
+    if (!device_inputs) {
+      X.allocate((size_t)n * p, s);
+      Y.allocate((size_t)n * q, s);
+      FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+      FPLS_CHECK(cudaMemcpyAsync(Y.get(), responses, sizeof(T) * n * q, cudaMemcpyHostToDevice, s));
+      if (permutation_count > 0) {
+        P.allocate((size_t)permutation_count * n, s);
+        FPLS_CHECK(cudaMemcpyAsync(P.get(), permutations, sizeof(int) * permutation_count * n,
+                                   cudaMemcpyHostToDevice, s));
+      }
+      xd = X.get();
+      yd = Y.get();
+      pd = P.get();
+    } else {
+      host_folds.resize(n);
+      FPLS_CHECK(cudaMemcpyAsync(host_folds.data(), folds, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+      FPLS_CHECK(cudaStreamSynchronize(s));
+      fh = host_folds.data();
+    }
+    BatchedCv<T> engine;
+    engine.run(xd, n, p, yd, q, fh, pd, permutation_count, prefixes, prefix_count, scaling, s);
+    engine.metrics(metric, metrics, q2, rmsd, observed_r2);
+    if (status)
+      for (size_t f = 0; f < engine.status.size(); ++f) status[f] = engine.status[f];
+  }
+}
+
+}  // namespace
+}  // namespace fpls
+
+using namespace fpls;
+
+extern "C" {
+
+int fastpls_cuda_gemm(const void* left, const void* right, int precision,
+                      int rows, int inner, int columns, void* output,
+                      char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown CUDA matrix multiplication error", [&] {
+    if (!left || !right || !output || (precision != 32 && precision != 64) ||
+        rows < 1 || inner < 1 || columns < 1)
+      throw std::invalid_argument("invalid CUDA matrix multiplication input");
+    if (precision == 32)
+      host_gemm(static_cast<const float*>(left), static_cast<const float*>(right), rows, inner, columns,
+                static_cast<float*>(output));
+    else
+      host_gemm(static_cast<const double*>(left), static_cast<const double*>(right), rows, inner, columns,
+                static_cast<double*>(output));
+  });
+}
+
+int fastpls_resident_simpls_cv_classification(
+    const void* predictors, const int* labels, const int* folds, int precision,
+    int n, int p, int classes, const int* prefixes, int prefix_count,
+    int scaling, int lda, int oversample, int power, unsigned long long seed,
+    int store_predictions, int store_scores, int* predictions, void* scores,
+    int* status, double* metrics, char* error, size_t error_capacity) {
+  (void)oversample;
+  (void)power;
+  (void)seed;
+  return guarded(error, error_capacity, "unknown resident CUDA CV error", [&] {
+    if ((precision != 32 && precision != 64) || (lda != 0 && lda != 1) ||
+        (store_predictions != 0 && store_predictions != 1) ||
+        (store_scores != 0 && store_scores != 1))
+      throw std::invalid_argument("invalid resident CUDA CV controls");
+    if (precision == 32)
+      cv_classification<float>(kSimpls, static_cast<const float*>(predictors), labels, folds, n, p, classes,
+                               prefixes, prefix_count, scaling, lda == 1, store_predictions == 1,
+                               store_scores == 1, predictions, static_cast<float*>(scores), status, metrics);
+    else
+      cv_classification<double>(kSimpls, static_cast<const double*>(predictors), labels, folds, n, p, classes,
+                                prefixes, prefix_count, scaling, lda == 1, store_predictions == 1,
+                                store_scores == 1, predictions, static_cast<double*>(scores), status, metrics);
+  });
+}
+
+int fastpls_resident_simpls_cv_regression(
+    const void* predictors, const void* responses, const int* folds,
+    int precision, int n, int p, int q, const int* prefixes, int prefix_count,
+    int scaling, int metric, int oversample, int power, unsigned long long seed,
+    int store_predictions, double* predictions, int* status, double* metrics,
+    double* q2, double* rmsd, double* observed_r2, char* error,
+    size_t error_capacity) {
+  (void)oversample;
+  (void)power;
+  (void)seed;
+  return guarded(error, error_capacity, "unknown resident CUDA regression CV error", [&] {
+    if ((precision != 32 && precision != 64) || !q2 || !rmsd || !observed_r2 ||
+        (store_predictions != 0 && store_predictions != 1))
+      throw std::invalid_argument("invalid resident CUDA regression CV controls");
+    if (precision == 32)
+      cv_regression<float>(kSimpls, static_cast<const float*>(predictors), static_cast<const float*>(responses),
+                           folds, n, p, q, prefixes, prefix_count, scaling, metric, store_predictions == 1,
+                           predictions, status, metrics, q2, rmsd, observed_r2);
+    else
+      cv_regression<double>(kSimpls, static_cast<const double*>(predictors), static_cast<const double*>(responses),
+                            folds, n, p, q, prefixes, prefix_count, scaling, metric, store_predictions == 1,
+                            predictions, status, metrics, q2, rmsd, observed_r2);
+  });
+}
+
+int fastpls_resident_plssvd_cv_classification(
+    const void* predictors, const int* labels, const int* folds, int precision,
+    int n, int p, int classes, const int* prefixes, int prefix_count,
+    int scaling, int lda, int oversample, int power, unsigned long long seed,
+    int store_predictions, int store_scores, int* predictions, void* scores,
+    int* status, double* metrics, char* error, size_t error_capacity) {
+  (void)oversample;
+  (void)power;
+  (void)seed;
+  return guarded(error, error_capacity, "unknown resident CUDA PLS-SVD CV error", [&] {
+    if ((precision != 32 && precision != 64) || (lda != 0 && lda != 1) ||
+        (store_predictions != 0 && store_predictions != 1) ||
+        (store_scores != 0 && store_scores != 1))
+      throw std::invalid_argument("invalid resident CUDA PLS-SVD CV controls");
+    if (precision == 32)
+      cv_classification<float>(kPlssvd, static_cast<const float*>(predictors), labels, folds, n, p, classes,
+                               prefixes, prefix_count, scaling, lda == 1, store_predictions == 1,
+                               store_scores == 1, predictions, static_cast<float*>(scores), status, metrics);
+    else
+      cv_classification<double>(kPlssvd, static_cast<const double*>(predictors), labels, folds, n, p, classes,
+                                prefixes, prefix_count, scaling, lda == 1, store_predictions == 1,
+                                store_scores == 1, predictions, static_cast<double*>(scores), status, metrics);
+  });
+}
+
+int fastpls_resident_plssvd_cv_regression(
+    const void* predictors, const void* responses, const int* folds,
+    int precision, int n, int p, int q, const int* prefixes, int prefix_count,
+    int scaling, int metric, int oversample, int power, unsigned long long seed,
+    int store_predictions, double* predictions, int* status, double* metrics,
+    double* q2, double* rmsd, double* observed_r2, char* error,
+    size_t error_capacity) {
+  (void)oversample;
+  (void)power;
+  (void)seed;
+  return guarded(error, error_capacity, "unknown resident CUDA PLS-SVD regression CV error", [&] {
+    if ((precision != 32 && precision != 64) || !q2 || !rmsd || !observed_r2 ||
+        (store_predictions != 0 && store_predictions != 1))
+      throw std::invalid_argument("invalid resident CUDA PLS-SVD regression CV controls");
+    if (precision == 32)
+      cv_regression<float>(kPlssvd, static_cast<const float*>(predictors), static_cast<const float*>(responses),
+                           folds, n, p, q, prefixes, prefix_count, scaling, metric, store_predictions == 1,
+                           predictions, status, metrics, q2, rmsd, observed_r2);
+    else
+      cv_regression<double>(kPlssvd, static_cast<const double*>(predictors), static_cast<const double*>(responses),
+                            folds, n, p, q, prefixes, prefix_count, scaling, metric, store_predictions == 1,
+                            predictions, status, metrics, q2, rmsd, observed_r2);
+  });
+}
+
+void* fastpls_resident_simpls_create(const void* x, const void* y, const int* labels,
+                                     int precision, int n, int p, int q, int components,
+                                     int scaling, int oversample, int power, int retain_scores,
+                                     unsigned long long seed, char* error, size_t error_capacity) {
+  return guarded_create(error, error_capacity, "unknown resident CUDA fitting error", [&]() -> void* {
+    if (!x || (precision != 32 && precision != 64))
+      throw std::invalid_argument("invalid resident matrix or precision");
+    if (retain_scores != 0 && retain_scores != 1)
+      throw std::invalid_argument("invalid resident score-retention request");
+    return make_handle(precision, request(kSimpls, x, y, labels, n, p, q, components, scaling,
+                                          oversample, power, retain_scores, seed));
+  });
+}
+
+void* fastpls_resident_plssvd_create(const void* x, const void* y, const int* labels,
+                                     int precision, int n, int p, int q, int components,
+                                     int scaling, int oversample, int power, int retain_scores,
+                                     unsigned long long seed, char* error, size_t error_capacity) {
+  return guarded_create(error, error_capacity, "unknown resident CUDA PLS-SVD fitting error", [&]() -> void* {
+    if (!x || (precision != 32 && precision != 64))
+      throw std::invalid_argument("invalid resident matrix or precision");
+    if (retain_scores != 0 && retain_scores != 1)
+      throw std::invalid_argument("invalid resident score-retention request");
+    return make_handle(precision, request(kPlssvd, x, y, labels, n, p, q, components, scaling,
+                                          oversample, power, retain_scores, seed));
+  });
+}
+
+void* fastpls_resident_opls_create(const void* x, const void* y, const int* labels,
+                                   int precision, int n, int p, int q, int components,
+                                   int scaling, int oversample, int power, int retain_scores,
+                                   unsigned long long seed, int north, char* error,
+                                   size_t error_capacity) {
+  return guarded_create(error, error_capacity, "unknown resident CUDA OPLS fitting error", [&]() -> void* {
+    if (!x || (precision != 32 && precision != 64) || north < 0)
+      throw std::invalid_argument("invalid resident CUDA OPLS input");
+    FitRequest r = request(kOpls, x, y, labels, n, p, q, components, scaling, oversample, power,
+                           retain_scores, seed);
+    r.north = north;
+    return make_handle(precision, r);
+  });
+}
+
+void* fastpls_resident_kernelpls_create(const void* x, const void* y, const int* labels,
+                                        int precision, int n, int p, int q, int components,
+                                        int scaling, int oversample, int power, int retain_scores,
+                                        unsigned long long seed, int kernel, double gamma,
+                                        int degree, double coef0, char* error,
+                                        size_t error_capacity) {
+  return guarded_create(error, error_capacity, "unknown resident CUDA nonlinear kernel PLS fitting error",
+                        [&]() -> void* {
+    if (!x || (precision != 32 && precision != 64) || (kernel != 2 && kernel != 3))
+      throw std::invalid_argument("invalid resident CUDA nonlinear kernel PLS input");
+    FitRequest r = request(kKernelPls, x, y, labels, n, p, q, components, scaling, oversample, power,
+                           retain_scores, seed);
+    r.kernel = kernel;
+    r.gamma = gamma;
+    r.degree = degree;
+    r.coef0 = coef0;
+    return make_handle(precision, r);
+  });
+}
+
+int fastpls_resident_predict_path(void* model, const void* x, int rows, const int* prefixes,
+                                  int prefix_count, int lda, void* predictions, char* error,
+                                  size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident prediction-path error", [&] {
+    if (!model || (lda != 0 && lda != 1))
+      throw std::invalid_argument("invalid resident prediction-path model");
+    static_cast<ResidentHandle*>(model)->predict_path(x, rows, prefixes, prefix_count, lda == 1, predictions);
+  });
+}
+
+void fastpls_resident_simpls_destroy(void* model) {
+  delete static_cast<ResidentHandle*>(model);
+}
+
+int fastpls_resident_export(void* model, int field, void* out, size_t elements, char* error,
+                            size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident export error", [&] {
+    if (!model) throw std::invalid_argument("null resident model");
+    static_cast<ResidentHandle*>(model)->export_field(field, out, elements);
+  });
+}
+
+int fastpls_resident_classify_path(void* model, const void* x, int rows, const int* prefixes,
+                                   int prefix_count, int lda, int top, int* labels, char* error,
+                                   size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident classification-path error", [&] {
+    if (!model || (lda != 0 && lda != 1))
+      throw std::invalid_argument("invalid resident classification-path model");
+    static_cast<ResidentHandle*>(model)->classify_path(x, rows, prefixes, prefix_count, lda == 1, top,
+                                                       labels, nullptr);
+  });
+}
+
+int fastpls_resident_classify_response_path(void* model, const void* x, int rows,
+                                            const int* prefixes, int prefix_count, int lda, int top,
+                                            int* labels, void* predictions, char* error,
+                                            size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident classification-response path error", [&] {
+    if (!model) throw std::invalid_argument("null resident model");
+    if (!predictions)
+      throw std::invalid_argument("invalid resident classification-response path request");
+    static_cast<ResidentHandle*>(model)->classify_path(x, rows, prefixes, prefix_count, lda != 0, top,
+                                                       labels, predictions);
+  });
+}
+
+int fastpls_resident_response_sums(void* model, const void* x, const void* y, const int* labels,
+                                   int rows, int prefix, void* out, char* error,
+                                   size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident metric error", [&] {
+    if (!model) throw std::invalid_argument("null resident model");
+    static_cast<ResidentHandle*>(model)->response_sums(x, y, labels, rows, prefix, out);
+  });
+}
+
+int fastpls_resident_project(void* model, const void* x, int rows, int prefix, void* out,
+                             char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident projection error", [&] {
+    if (!model) throw std::invalid_argument("null resident model");
+    static_cast<ResidentHandle*>(model)->project(x, rows, prefix, out);
+  });
+}
+
+int fastpls_resident_controls(void* model, int* oversample, int* power, int* block,
+                              int* block_limit, int* implicit_operator,
+                              int* predictor_crossprod_cache, char* error,
+                              size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident control error", [&] {
+    if (!model) throw std::invalid_argument("null resident model");
+    static_cast<ResidentHandle*>(model)->controls(oversample, power, block, block_limit,
+                                                  implicit_operator, predictor_crossprod_cache);
+  });
+}
+
+int fastpls_resident_compact(void* model, int prepare_lda, char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown resident compaction error", [&] {
+    if (!model || (prepare_lda != 0 && prepare_lda != 1))
+      throw std::invalid_argument("invalid resident compaction request");
+    static_cast<ResidentHandle*>(model)->compact(prepare_lda == 1);
+  });
+}
+
+// ------------------------------------------------------------------ additions
+int fastpls_b200_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return count;
+}
+
+unsigned long long fastpls_b200_launch_count(void) { return launch_count(); }
+
+int fastpls_b200_simpls_cv_permutation(
+    const void* predictors, const void* responses, const int* folds,
+    const int* permutations, int permutation_count, int precision, int n,
+    int p, int q, const int* prefixes, int prefix_count, int scaling,
+    int metric, double* metrics, double* q2, double* rmsd, double* observed_r2,
+    int* status, char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown batched CUDA CV error", [&] {
+    if (precision != 32 && precision != 64)
+      throw std::invalid_argument("invalid batched CUDA CV precision");
+    if (precision == 32)
+      cv_permutation<float>(predictors, responses, folds, permutations, permutation_count, n, p, q,
+                            prefixes, prefix_count, scaling, metric, metrics, q2, rmsd, observed_r2,
+                            status, false);
+    else
+      cv_permutation<double>(predictors, responses, folds, permutations, permutation_count, n, p, q,
+                             prefixes, prefix_count, scaling, metric, metrics, q2, rmsd, observed_r2,
+                             status, false);
+  });
+}
+
+int fastpls_b200_simpls_cv_permutation_device(
+    const void* predictors, const void* responses, const int* folds,
+    const int* permutations, int permutation_count, int precision, int n,
+    int p, int q, const int* prefixes, int prefix_count, int scaling,
+    int metric, double* metrics, double* q2, double* rmsd, double* observed_r2,
+    int* status, char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown batched CUDA CV error", [&] {
+    if (precision != 32 && precision != 64)
+      throw std::invalid_argument("invalid batched CUDA CV precision");
+    if (precision == 32)
+      cv_permutation<float>(predictors, responses, folds, permutations, permutation_count, n, p, q,
+                            prefixes, prefix_count, scaling, metric, metrics, q2, rmsd, observed_r2,
+                            status, true);
+    else
+      cv_permutation<double>(predictors, responses, folds, permutations, permutation_count, n, p, q,
+                             prefixes, prefix_count, scaling, metric, metrics, q2, rmsd, observed_r2,
+                             status, true);
+  });
+}
+
+}  // extern "C"

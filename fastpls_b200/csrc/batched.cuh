@@ -1,0 +1,45 @@
+// Batched SIMPLS over CV folds x response permutations x component path
+// (host interface; see batched.cu).
+#pragma once
+
+#include "kernels.cuh"
+
+#include <vector>
+
+namespace fpls {
+
+constexpr int kBatchMaxResponses = 32;
+
+template <class T>
+struct BatchedCv {
+  // Runs every (fold, permutation) instance. X, Y and perms are device
+  // pointers (X n x p, Y n x q column-major; perms P x n zero-based source
+  // rows, instance 0 uses the observed order); folds and prefixes are host.
+  void run(const T* X, int n, int p, const T* Y, int q, const int* folds,
+           const int* perms, int perm_count, const int* prefixes,
+           int prefix_count, int scaling, cudaStream_t stream);
+  // Metrics per (permutation + 1) x prefix, row-major by instance group:
+  // index b * prefix_count + j, b = 0 the observed responses.
+  void metrics(int metric, double* metric_out, double* q2, double* rmsd,
+               double* r2) const;
+
+  std::vector<int> status;          // per fold: 1 fitted, 2 empty
+  std::vector<double> inst_sse;     // (P+1) x folds x prefixes
+  std::vector<double> inst_sst;     // (P+1) x folds
+  long double total_ss = 0.0L;
+
+ private:
+  void form_gram(const double* kscale, cudaStream_t s);
+  void run_group(const std::vector<int>& inst_fold,
+                 const std::vector<int>& inst_perm, cudaStream_t s);
+
+  const T* X = nullptr;
+  const int* perms = nullptr;
+  int n = 0, p = 0, q = 0, P = 0, prefix_count = 0, scaling = 1, kmax = 0;
+  int folds = 0, max_test = 1;
+  bool center = true;
+  DeviceArray<double> gram, Y64;
+  DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag;
+};
+
+}  // namespace fpls

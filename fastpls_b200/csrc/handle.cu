@@ -1,0 +1,470 @@
+// Resident model handle (host orchestration of the fitting and prediction
+// kernels). Behavioural contract: src/cuda_resident_api.cuh:69-479 of the
+// reference (validation order, error strings, field sizes, synchronous
+// calls on a per-handle non-blocking stream).
+#include "handle.cuh"
+#include "lda.cuh"
+#include "reduce.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace fpls {
+
+namespace {
+
+template <class T>
+__global__ void convert_kernel(const double* __restrict__ in, long count,
+                               T* __restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count;
+       i += (long)gridDim.x * blockDim.x)
+    out[i] = static_cast<T>(in[i]);
+}
+
+template <class T>
+void convert(const double* in, long count, T* out, cudaStream_t s) {
+  if (count <= 0) return;
+  convert_kernel<T><<<(unsigned)std::min<long>((count + 255) / 256, 8L * num_sms()), 256, 0, s>>>(in, count, out);
+  count_launch();
+  FPLS_LAUNCH("convert");
+}
+
+// SSE, SS about the training mean, SS about the observed mean, per response
+// (response_sums, src/cuda_resident_metrics.cuh:9-43), FP64.
+template <class T>
+__global__ void response_sums_kernel(const double* __restrict__ pred,
+                                     const T* __restrict__ y,
+                                     const int* __restrict__ labels,
+                                     const double* __restrict__ ymean, int n,
+                                     int q, double* out, int* flag) {
+  __shared__ double scratch[32];
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (labels && (labels[i] < 1 || labels[i] > q)) flag_error(flag, 4);
+    const double v = labels ? (labels[i] == c + 1 ? 1.0 : 0.0)
+                            : as_f64(y[i + (long)c * n]);
+    if (!isfinite(v)) flag_error(flag, 4);
+    s += v;
+  }
+  const double mu = block_sum(s, scratch) / n;
+  double sse = 0.0, st = 0.0, so = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = labels ? (labels[i] == c + 1 ? 1.0 : 0.0)
+                            : as_f64(y[i + (long)c * n]);
+    const double f = pred[i + (long)c * n];
+    if (!isfinite(f)) flag_error(flag, 4);
+    const double e = v - f, d = v - ymean[c], o = v - mu;
+    sse = fma(e, e, sse);
+    st = fma(d, d, st);
+    so = fma(o, o, so);
+  }
+  sse = block_sum(sse, scratch);
+  st = block_sum(st, scratch);
+  so = block_sum(so, scratch);
+  if (threadIdx.x == 0) {
+    out[3 * c] = sse;
+    out[3 * c + 1] = st;
+    out[3 * c + 2] = so;
+  }
+}
+
+// Loadings P and sequential residual loadings (variance_loadings,
+// src/cuda_resident_variance.cuh:10-24), FP64, one thread per predictor.
+__global__ void variance_loadings_kernel(const double* __restrict__ cross,
+                                         const double* __restrict__ gram,
+                                         int p, int a, double* loadings,
+                                         double* sequential) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < p;
+       f += gridDim.x * blockDim.x) {
+    for (int j = 0; j < a; ++j) {
+      const double den = gram[j + (long)j * a];
+      const bool ok = isfinite(den) && den > 0.0;
+      double v = cross[f + (long)j * p];
+      loadings[f + (long)j * p] = ok ? v / den : 0.0;
+      for (int i = 0; i < j; ++i) v -= sequential[f + (long)i * p] * gram[i + (long)j * a];
+      sequential[f + (long)j * p] = ok ? v / den : 0.0;
+    }
+  }
+}
+
+// cross = (X^T T - mean * colsum(T)) / scale  (in place)
+__global__ void standardize_cross(double* cross, int p, int a,
+                                  const double* __restrict__ mean,
+                                  const double* __restrict__ scale,
+                                  const double* __restrict__ tsum) {
+  const long total = (long)p * a;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(idx % p), k = (int)(idx / p);
+    cross[idx] = (cross[idx] - mean[j] * tsum[k]) / scale[j];
+  }
+}
+
+__global__ void column_sums_kernel(const double* __restrict__ M, int rows,
+                                   long ld, double* out) {
+  __shared__ double scratch[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) s += M[i + (long)blockIdx.x * ld];
+  s = block_sum(s, scratch);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// result[j] = ||sequential_j||^2 * gram_jj ; result[a] = sum_j column SS of Xs
+__global__ void variance_finish_kernel(const double* __restrict__ sequential,
+                                       const double* __restrict__ gram,
+                                       const double* __restrict__ sum,
+                                       const double* __restrict__ sumsq,
+                                       const double* __restrict__ mean,
+                                       const double* __restrict__ scale,
+                                       int n, int p, int a, double* result) {
+  __shared__ double scratch[32];
+  for (int j = blockIdx.x; j <= a; j += gridDim.x) {
+    double acc = 0.0;
+    if (j < a) {
+      for (int f = threadIdx.x; f < p; f += blockDim.x) {
+        const double v = sequential[f + (long)j * p];
+        acc = fma(v, v, acc);
+      }
+    } else {
+      for (int f = threadIdx.x; f < p; f += blockDim.x) {
+        const double mu = mean[f], sd = scale[f];
+        const double ss = sumsq[f] - 2.0 * mu * sum[f] + (double)n * mu * mu;
+        acc += fmax(ss, 0.0) / (sd * sd);
+      }
+    }
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) {
+      if (j < a) {
+        const double g = acc * gram[j + (long)j * a];
+        result[j] = (isfinite(g) && g > 0.0) ? g : 0.0;
+      } else {
+        result[a] = acc;
+      }
+    }
+  }
+}
+
+void check_path(const int* prefixes, int count, int a) {
+  require(prefixes != nullptr && count >= 1, "invalid resident prediction-path request");
+  int previous = 0;
+  for (int j = 0; j < count; ++j) {
+    if (prefixes[j] <= previous || prefixes[j] > a)
+      throw std::invalid_argument("component path must be strictly increasing");
+    previous = prefixes[j];
+  }
+}
+
+}  // namespace
+
+template <class T>
+class TypedHandle final : public ResidentHandle {
+ public:
+  explicit TypedHandle(const FitRequest& rq) : rq_(rq) {
+    try {
+      FPLS_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      fit();
+    } catch (...) {
+      release();
+      throw;
+    }
+  }
+  ~TypedHandle() override { release(); }
+
+  void predict_path(const void* x, int rows, const int* prefixes, int count,
+                    bool lda, void* out) override {
+    if (!x || !out || rows < 1 || count < 1)
+      throw std::invalid_argument("invalid resident prediction-path request");
+    check_path(prefixes, count, model_.a);
+    if (lda && !model_.classification)
+      throw std::invalid_argument("LDA requires class labels");
+    const int kmax = prefixes[count - 1];
+    upload_rows(x, rows);
+    project_rows<T>(model_, xbuf_.get(), rows, rows, kmax, scores(rows, kmax), rows, ws_, stream_);
+    const int q = model_.m;
+    pred_.reserve((size_t)rows * q, stream_);
+    conv_.reserve((size_t)rows * q, stream_);
+    T* dst = static_cast<T*>(out);
+    for (int j = 0; j < count; ++j) {
+      const int k = prefixes[j];
+      if (lda) lda_state().discriminants(scores_.get(), rows, rows, k, pred_.get(), rows, stream_);
+      else predict_from_scores(model_, scores_.get(), rows, rows, k, pred_.get(), rows, stream_);
+      download(pred_.get(), (long)rows * q, dst + (size_t)j * rows * q);
+    }
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void classify_path(const void* x, int rows, const int* prefixes, int count,
+                     bool lda, int top, int* out, void* response_out) override {
+    const int q = model_.m;
+    if (!model_.classification || !x || !out || count < 1 || top < 1 || top > q || rows < 1)
+      throw std::invalid_argument(response_out
+          ? "invalid resident classification-response path request"
+          : "invalid resident classification-path request");
+    check_path(prefixes, count, model_.a);
+    const int kmax = prefixes[count - 1];
+    upload_rows(x, rows);
+    project_rows<T>(model_, xbuf_.get(), rows, rows, kmax, scores(rows, kmax), rows, ws_, stream_);
+    pred_.reserve((size_t)rows * q, stream_);
+    disc_.reserve((size_t)rows * q, stream_);
+    conv_.reserve((size_t)rows * q, stream_);
+    top_.reserve((size_t)rows * top, stream_);
+    T* resp = static_cast<T*>(response_out);
+    for (int j = 0; j < count; ++j) {
+      const int k = prefixes[j];
+      const double* decoded = pred_.get();
+      if (!lda || resp) {
+        predict_from_scores(model_, scores_.get(), rows, rows, k, pred_.get(), rows, stream_);
+        if (resp) download(pred_.get(), (long)rows * q, resp + (size_t)j * rows * q);
+      }
+      if (lda) {
+        lda_state().discriminants(scores_.get(), rows, rows, k, disc_.get(), rows, stream_);
+        decoded = disc_.get();
+      }
+      topk_rows(decoded, rows, q, top, top_.get(), rows, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(out + (size_t)j * rows * top, top_.get(),
+                                 sizeof(int) * rows * top,
+                                 cudaMemcpyDeviceToHost, stream_));
+    }
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void project(const void* x, int rows, int prefix, void* out) override {
+    if (!x || !out || rows < 1 || prefix < 1 || prefix > model_.a)
+      throw std::invalid_argument("invalid resident score request");
+    upload_rows(x, rows);
+    project_rows<T>(model_, xbuf_.get(), rows, rows, prefix, scores(rows, prefix), rows, ws_, stream_);
+    conv_.reserve((size_t)rows * prefix, stream_);
+    download(scores_.get(), (long)rows * prefix, static_cast<T*>(out));
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void response_sums(const void* x, const void* y, const int* labels, int rows,
+                     int prefix, void* out) override {
+    if (!out || (!y && !labels) || (y && labels) ||
+        (model_.classification != (labels != nullptr)))
+      throw std::invalid_argument("invalid resident response representation");
+    if (!x || rows < 1 || prefix < 1 || prefix > model_.a)
+      throw std::invalid_argument("invalid resident prediction input");
+    const int q = model_.m;
+    upload_rows(x, rows);
+    project_rows<T>(model_, xbuf_.get(), rows, rows, prefix, scores(rows, prefix), rows, ws_, stream_);
+    pred_.reserve((size_t)rows * q, stream_);
+    predict_from_scores(model_, scores_.get(), rows, rows, prefix, pred_.get(), rows, stream_);
+    DeviceArray<T> yd;
+    DeviceArray<int> ld;
+    if (labels) {
+      ld.allocate(rows, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(ld.get(), labels, sizeof(int) * rows, cudaMemcpyHostToDevice, stream_));
+    } else {
+      yd.allocate((size_t)rows * q, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(yd.get(), y, sizeof(T) * rows * q, cudaMemcpyHostToDevice, stream_));
+    }
+    DeviceArray<double> sums((size_t)3 * q, stream_);
+    FPLS_CHECK(cudaMemsetAsync(ws_.flag.get(), 0, sizeof(int), stream_));
+    response_sums_kernel<T><<<q, 256, 0, stream_>>>(pred_.get(), yd.get(), ld.get(),
+                                                    model_.ymean.get(), rows, q,
+                                                    sums.get(), ws_.flag.get());
+    count_launch();
+    FPLS_LAUNCH("response_sums");
+    conv_.reserve((size_t)3 * q, stream_);
+    download(sums.get(), 3L * q, static_cast<T*>(out));
+    raise_on_flag(ws_, stream_, "nonfinite response/prediction or invalid class label in resident metrics");
+  }
+
+  void export_field(int field, void* out, std::size_t size) override {
+    const std::size_t a = model_.a, q = model_.m, p = model_.p, fp = model_.feature_p;
+    const std::size_t counts[] = {fp * a, q * a, (size_t)model_.n * a, p, p, q, fp * a, a + 1};
+    if (field < 0 || field > 7 || !out || size != counts[field])
+      throw std::invalid_argument("invalid resident field output size");
+    const double* src = nullptr;
+    switch (field) {
+      case 0: src = model_.R.get(); break;
+      case 1: src = q_export(); break;
+      case 2: src = model_.T.get(); break;
+      case 3: src = model_.mean.get(); break;
+      case 4: src = model_.scale.get(); break;
+      case 5: src = model_.ymean.get(); break;
+      default: ensure_variance(); src = field == 6 ? loadings_.get() : var_ss_.get(); break;
+    }
+    if (!src) throw std::invalid_argument("resident field is not available after compaction");
+    conv_.reserve(size, stream_);
+    download(src, (long)size, static_cast<T*>(out));
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void controls(int* oversample, int* power, int* block, int* block_limit,
+                int* implicit_operator, int* crossprod_cache) override {
+    if (!oversample || !power || !block || !block_limit || !implicit_operator || !crossprod_cache)
+      throw std::invalid_argument("null resident control output");
+    *oversample = rq_.oversample;
+    *power = rq_.power;
+    *block = 1;
+    *block_limit = 0;
+    *implicit_operator = 0;
+    *crossprod_cache = 0;
+  }
+
+  void compact(bool prepare_lda) override {
+    if (prepare_lda) {
+      if (!model_.classification)
+        throw std::invalid_argument("LDA compaction requires classification labels");
+      lda_state();
+    }
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+    xtrain_.release();
+    model_.V.release();
+    ws_.stream_partial.release();
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+ private:
+  void fit() {
+    const int n = rq_.n, p = rq_.p, q = rq_.q, a = rq_.components;
+    const bool cls = rq_.labels != nullptr;
+    if (!rq_.x) throw std::invalid_argument("invalid resident matrix or precision");
+    if ((rq_.y == nullptr) == (rq_.labels == nullptr))
+      throw std::invalid_argument("provide responses or labels, not both");
+    if (n < 2 || p < 1 || q < 1 || a < 1 || a > std::min(n - 1, p) || rq_.scaling < 1 || rq_.scaling > 3)
+      throw std::invalid_argument(rq_.method == kPlssvd ? "invalid resident PLS-SVD dimensions"
+                                                        : "invalid resident SIMPLS dimensions");
+    if (cls && q < 2) throw std::invalid_argument("classification requires at least two classes");
+    if (rq_.method != kSimpls && rq_.method != kPlssvd)
+      throw std::invalid_argument("this build fits SIMPLS and PLS-SVD resident models only");
+    xtrain_.allocate((size_t)n * p, stream_);
+    FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
+    DeviceArray<T> y;
+    if (cls) {
+      model_.labels.allocate(n, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(model_.labels.get(), rq_.labels, sizeof(int) * n, cudaMemcpyHostToDevice, stream_));
+      model_.class_counts.assign(q, 0);
+      for (int i = 0; i < n; ++i)
+        if (rq_.labels[i] >= 1 && rq_.labels[i] <= q) ++model_.class_counts[rq_.labels[i] - 1];
+    } else {
+      y.allocate((size_t)n * q, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(y.get(), rq_.y, sizeof(T) * n * q, cudaMemcpyHostToDevice, stream_));
+    }
+    model_.classification = cls;
+    ws_.ensure(n, p, q, a, stream_);
+    FPLS_CHECK(cudaMemsetAsync(ws_.flag.get(), 0, sizeof(int), stream_));
+    DeviceArray<double> yc((size_t)n * q, stream_);
+    DeviceArray<double> ycsum(q, stream_);
+    model_.ymean.allocate(q, stream_);
+    prepare_responses<T>(y.get(), model_.labels.get(), n, q, yc.get(),
+                         model_.ymean.get(), ycsum.get(), ws_.flag.get(), stream_);
+    if (rq_.method == kPlssvd)
+      fit_plssvd<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
+    else
+      fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
+    raise_on_flag(ws_, stream_, rq_.method == kPlssvd
+        ? "resident PLS-SVD failed: invalid labels, decomposition or score Gram"
+        : "resident SIMPLS failed: invalid labels, decomposition or component norm");
+  }
+
+  const double* q_export() { return model_.Q.get(); }
+
+  double* scores(int rows, int k) {
+    scores_.reserve((size_t)rows * k, stream_);
+    return scores_.get();
+  }
+
+  void upload_rows(const void* x, int rows) {
+    xbuf_.reserve((size_t)rows * model_.p, stream_);
+    FPLS_CHECK(cudaMemcpyAsync(xbuf_.get(), x, sizeof(T) * rows * model_.p, cudaMemcpyHostToDevice, stream_));
+  }
+
+  void download(const double* src, long count, T* dst) {
+    const T* from = nullptr;
+    if (std::is_same<T, double>::value) {
+      from = reinterpret_cast<const T*>(src);
+    } else {
+      convert<T>(src, count, conv_.get(), stream_);
+      from = conv_.get();
+    }
+    FPLS_CHECK(cudaMemcpyAsync(dst, from, sizeof(T) * count, cudaMemcpyDeviceToHost, stream_));
+    if (!std::is_same<T, double>::value) FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  LdaState& lda_state() {
+    if (!lda_) {
+      if (!model_.classification) throw std::invalid_argument("LDA requires class labels");
+      auto next = std::make_unique<LdaState>();
+      next->train(model_.T.get(), model_.n, model_.n, model_.a, model_.labels.get(),
+                  model_.m, model_.class_counts, ws_.flag.get(), stream_);
+      lda_ = std::move(next);
+    }
+    return *lda_;
+  }
+
+  void ensure_variance() {
+    if (loadings_) return;
+    if (!xtrain_) throw std::invalid_argument("resident variance requires the training predictors (call before compaction)");
+    const int n = model_.n, p = model_.p, a = model_.a;
+    DeviceArray<double> cross((size_t)p * a, stream_), seq((size_t)p * a, stream_);
+    DeviceArray<double> gram((size_t)a * a, stream_), tsum(a, stream_);
+    DeviceArray<double> mom((size_t)2 * p, stream_);
+    loadings_.allocate((size_t)p * a, stream_);
+    var_ss_.allocate(a + 1, stream_);
+    xtv_product<T>(xtrain_.get(), n, p, n, model_.T.get(), n, a, cross.get(), p, ws_.stream_partial, stream_);
+    column_moments<T>(xtrain_.get(), n, p, n, nullptr, 0, mom.get(), mom.get() + p, nullptr, ws_.stream_partial, stream_);
+    column_sums_kernel<<<a, 256, 0, stream_>>>(model_.T.get(), n, n, tsum.get());
+    count_launch();
+    standardize_cross<<<std::min<unsigned>(ceil_div((size_t)p * a, 256), 8 * num_sms()), 256, 0, stream_>>>(
+        cross.get(), p, a, model_.mean.get(), model_.scale.get(), tsum.get());
+    count_launch();
+    GemmArgs g;
+    g.M = a; g.N = a; g.K = n;
+    g.A = model_.T.get(); g.lda = n; g.trans_a = true;
+    g.B = model_.T.get(); g.ldb = n;
+    g.C = gram.get(); g.ldc = a;
+    gemm_f64(g, stream_);
+    variance_loadings_kernel<<<std::min<unsigned>(ceil_div(p, 256), 8 * num_sms()), 256, 0, stream_>>>(
+        cross.get(), gram.get(), p, a, loadings_.get(), seq.get());
+    count_launch();
+    variance_finish_kernel<<<std::min(a + 1, 4 * num_sms()), 256, 0, stream_>>>(
+        seq.get(), gram.get(), mom.get(), mom.get() + p, model_.mean.get(),
+        model_.scale.get(), n, p, a, var_ss_.get());
+    count_launch();
+    FPLS_LAUNCH("variance");
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void release() noexcept {
+    if (stream_) cudaStreamSynchronize(stream_);
+    lda_.reset();
+    model_ = DeviceModel();
+    ws_ = Workspace();
+    xtrain_.release();
+    xbuf_.release();
+    scores_.release();
+    pred_.release();
+    disc_.release();
+    conv_.release();
+    top_.release();
+    loadings_.release();
+    var_ss_.release();
+    if (stream_) {
+      cudaStreamSynchronize(stream_);
+      cudaStreamDestroy(stream_);
+    }
+    stream_ = nullptr;
+  }
+
+  FitRequest rq_;
+  cudaStream_t stream_ = nullptr;
+  DeviceModel model_;
+  Workspace ws_;
+  DeviceArray<T> xtrain_, xbuf_, conv_;
+  DeviceArray<double> scores_, pred_, disc_, loadings_, var_ss_;
+  DeviceArray<int> top_;
+  std::unique_ptr<LdaState> lda_;
+};
+
+ResidentHandle* make_handle(int precision, const FitRequest& rq) {
+  if (precision == 32) return new TypedHandle<float>(rq);
+  if (precision == 64) return new TypedHandle<double>(rq);
+  throw std::invalid_argument("invalid resident matrix or precision");
+}
+
+}  // namespace fpls

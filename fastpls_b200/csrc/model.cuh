@@ -1,0 +1,88 @@
+// Resident model state and fitting entry points (host declarations).
+#pragma once
+
+#include "common.cuh"
+
+namespace fpls {
+
+constexpr int kMaxResponses = 64;  // m x m direction eigenproblem in one block
+
+enum Method { kPlssvd = 1, kSimpls = 3, kOpls = 4, kKernelPls = 5 };
+
+// Scratch reused across the kernels of one fit / prediction.
+struct Workspace {
+  DeviceArray<double> stream_partial;  // xr / xtv per-chunk partials
+  DeviceArray<double> block_partial;   // last-block reductions
+  DeviceArray<unsigned> counters;      // tickets of last-block reductions
+  DeviceArray<double> vec_p[5];        // p-length vectors
+  DeviceArray<double> vec_n[2];        // n-length vectors
+  DeviceArray<double> small;           // small scalars / m x m blocks
+  DeviceArray<int> flag;               // device error flag
+  void ensure(int n, int p, int m, int a, cudaStream_t s);
+};
+
+// A fitted model resident on the device. Every matrix is FP64 and
+// column-major. Linear methods predict Yhat = ymean + Xs R_k Q_k^T with
+// Xs = (X - mean) / scale; PLS-SVD uses per-prefix weights instead of Q.
+struct DeviceModel {
+  int method = kSimpls;
+  int n = 0, p = 0, m = 0, a = 0;  // rows, input columns, responses, components
+  int feature_p = 0;               // rows of R (p; n for kernel PLS)
+  int scaling = 1;
+  bool classification = false;
+  DeviceArray<double> mean, scale, ymean;  // p, p, m
+  DeviceArray<double> R, Q, V, T;          // p x a, m x a, p x a, n x a
+  DeviceArray<double> S0;                  // p x m centred cross-product
+  DeviceArray<double> sigma;               // PLS-SVD singular values (a)
+  DeviceArray<double> W;                   // PLS-SVD per-prefix weights (a x m x a)
+  DeviceArray<int> labels;                 // training labels (classification)
+  std::vector<int> class_counts;           // host copy (classification)
+};
+
+// Centre responses (dense Y, or one-hot minus prior for one-based labels).
+// Yc: n x m FP64; ymean: m; ycsum: column sums of Yc (rounding residue).
+template <class T>
+void prepare_responses(const T* Y, const int* labels, int n, int m,
+                       double* Yc, double* ymean, double* ycsum, int* flag,
+                       cudaStream_t stream);
+
+// SIMPLS fit on raw X (n x p, ld) with centred responses Yc (n x m).
+// Fills model.{mean, scale, ymean (caller), R, Q, V, T, S0, a}.
+template <class T>
+void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
+                const double* ycsum, int m, int components, int scaling,
+                DeviceModel& model, Workspace& ws, cudaStream_t stream);
+
+// PLS-SVD fit (exact SVD of the m-column cross-product).
+template <class T>
+void fit_plssvd(const T* X, int n, int p, long ld, const double* Yc,
+                const double* ycsum, int m, int components, int scaling,
+                DeviceModel& model, Workspace& ws, cudaStream_t stream);
+
+// Column centre/scale (model.mean, model.scale) and the scaled centred
+// cross-product S = Xs^T Yc (written to S and model.S0), one pass over X.
+template <class T>
+void compute_crossprod(const T* X, int n, int p, long ld, const double* Yc,
+                       const double* ycsum, int m, int scaling,
+                       DeviceModel& model, double* S, Workspace& ws,
+                       cudaStream_t stream);
+
+// Packed lower triangle of S^T S (m x m) for S p x m, into gpk.
+void gram_of_columns(double* S, int p, int m, double* gpk, Workspace& ws,
+                     cudaStream_t stream);
+
+// Latent scores of new rows: out (rows x k) = Xs R[:, :k] (FP64).
+template <class T>
+void project_rows(const DeviceModel& model, const T* X, int rows, long ld,
+                  int k, double* out, long ldo, Workspace& ws,
+                  cudaStream_t stream);
+
+// Responses for prefix k from scores (rows x >= k): out = ymean + T_k B_k.
+void predict_from_scores(const DeviceModel& model, const double* scores,
+                         int rows, long lds, int k, double* out, long ldo,
+                         cudaStream_t stream);
+
+// Throws when the device error flag was raised (synchronises the stream).
+void raise_on_flag(Workspace& ws, cudaStream_t stream, const char* message);
+
+}  // namespace fpls

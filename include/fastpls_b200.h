@@ -1,0 +1,209 @@
+/*
+ * C ABI of the B200 fastPLS fitting library (libfastpls_b200.so).
+ *
+ * The first block keeps, symbol for symbol, the CUDA ABI that the fastPLS R
+ * package links against (fastPLS src/cuda_resident_api.h), so the package's
+ * .Call glue (src/cuda_resident_r.cpp) links to this library unchanged.
+ * Conventions (unchanged from the reference):
+ *   - precision is 32 or 64; FP32 data are IEEE-754 floats;
+ *   - matrices are column-major with leading dimension = rows;
+ *   - labels are one-based (1..classes); folds are one-based (1..K);
+ *   - component paths are strictly increasing and <= the fitted count;
+ *   - scaling: 1 = centre, 2 = autoscale (sd with n-1), 3 = none;
+ *   - regression metric: 2 = R2, 3 = Q2, 4 = RMSD;
+ *   - every pointer is host memory borrowed for the call; outputs are
+ *     caller-allocated; functions return 0 (or a handle) on success and 1
+ *     (or NULL) on error, writing a NUL-terminated message into `error`
+ *     (capacity `error_capacity`); nothing throws across the boundary;
+ *   - a handle owns one CUDA stream; calls are synchronous and a handle is
+ *     not safe for concurrent calls. Every handle, whatever the method, is
+ *     released with fastpls_resident_simpls_destroy.
+ * Arithmetic: all products and reductions are FP64 on the device whatever
+ * the storage precision, so results agree with the reference's FP64 CPU
+ * path to ~1e-10 relative.
+ */
+#ifndef FASTPLS_B200_H
+#define FASTPLS_B200_H
+#include <stddef.h>
+#if defined(__GNUC__)
+#define FASTPLS_B200_API __attribute__((visibility("default")))
+#else
+#define FASTPLS_B200_API
+#endif
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference ABI (fastPLS src/cuda_resident_api.h) ------------------- */
+
+/* replaces src/cuda_resident_api.h:11 -- output = left (rows x inner) *
+ * right (inner x columns), accumulated in FP64, returned in `precision`. */
+FASTPLS_B200_API int fastpls_cuda_gemm(const void* left, const void* right, int precision,
+                      int rows, int inner, int columns, void* output,
+                      char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:14 -- SIMPLS classification CV.
+ * predictions: n x prefix_count labels; scores: n x classes x prefix_count;
+ * status per fold: 1 fitted, 2 empty fold, 4 single active class;
+ * metrics: accuracy per prefix. oversample/power/seed are accepted and
+ * recorded; directions are exact (see the library documentation). */
+FASTPLS_B200_API int fastpls_resident_simpls_cv_classification(
+    const void* predictors, const int* labels, const int* folds,
+    int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, int lda, int oversample, int power,
+    unsigned long long seed, int store_predictions, int store_scores,
+    int* predictions, void* scores, int* status, double* metrics,
+    char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:20 -- SIMPLS regression CV.
+ * predictions: n x q x prefix_count (double); metrics per prefix is the
+ * selected metric; q2 / rmsd / observed_r2 are always filled. */
+FASTPLS_B200_API int fastpls_resident_simpls_cv_regression(
+    const void* predictors, const void* responses, const int* folds,
+    int precision, int n, int p, int q, const int* prefixes,
+    int prefix_count, int scaling, int metric, int oversample, int power,
+    unsigned long long seed, int store_predictions, double* predictions,
+    int* status, double* metrics, double* q2, double* rmsd,
+    double* observed_r2, char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:27 -- PLS-SVD classification CV. */
+FASTPLS_B200_API int fastpls_resident_plssvd_cv_classification(
+    const void* predictors, const int* labels, const int* folds,
+    int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, int lda, int oversample, int power,
+    unsigned long long seed, int store_predictions, int store_scores,
+    int* predictions, void* scores, int* status, double* metrics,
+    char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:33 -- PLS-SVD regression CV. */
+FASTPLS_B200_API int fastpls_resident_plssvd_cv_regression(
+    const void* predictors, const void* responses, const int* folds,
+    int precision, int n, int p, int q, const int* prefixes,
+    int prefix_count, int scaling, int metric, int oversample, int power,
+    unsigned long long seed, int store_predictions, double* predictions,
+    int* status, double* metrics, double* q2, double* rmsd,
+    double* observed_r2, char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:40 -- fit a resident SIMPLS model
+ * (responses y n x q, or one-based labels with q classes). */
+FASTPLS_B200_API void* fastpls_resident_simpls_create(
+    const void* x, const void* y, const int* labels, int precision, int n,
+    int p, int q, int components, int scaling, int oversample, int power,
+    int retain_scores, unsigned long long seed, char* error,
+    size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:44 -- fit a resident PLS-SVD model. */
+FASTPLS_B200_API void* fastpls_resident_plssvd_create(
+    const void* x, const void* y, const int* labels, int precision, int n,
+    int p, int q, int components, int scaling, int oversample, int power,
+    int retain_scores, unsigned long long seed, char* error,
+    size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:48 -- fit a resident OPLS model. */
+FASTPLS_B200_API void* fastpls_resident_opls_create(
+    const void* x, const void* y, const int* labels, int precision, int n,
+    int p, int q, int components, int scaling, int oversample, int power,
+    int retain_scores, unsigned long long seed, int north, char* error,
+    size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:52 -- fit a resident kernel PLS model
+ * (kernel 2 = RBF, 3 = polynomial). */
+FASTPLS_B200_API void* fastpls_resident_kernelpls_create(
+    const void* x, const void* y, const int* labels, int precision, int n,
+    int p, int q, int components, int scaling, int oversample, int power,
+    int retain_scores, unsigned long long seed, int kernel, double gamma,
+    int degree, double coef0, char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:57 -- predictions (rows x q per prefix,
+ * concatenated) for new rows; lda = 1 returns LDA discriminant scores. */
+FASTPLS_B200_API int fastpls_resident_predict_path(void* model, const void* x, int rows,
+                                  const int* prefixes, int prefix_count,
+                                  int lda, void* predictions, char* error,
+                                  size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:60 -- release any resident handle. */
+FASTPLS_B200_API void fastpls_resident_simpls_destroy(void* model);
+
+/* replaces src/cuda_resident_api.h:61 -- copy a model field to the host:
+ * 0 R (feature_p x a), 1 Q (q x a), 2 T (n x a), 3 mX (p), 4 vX (p),
+ * 5 mY (q), 6 P loadings (feature_p x a), 7 variance SS (a + 1).
+ * `elements` must equal the field size exactly. */
+FASTPLS_B200_API int fastpls_resident_export(void* model, int field, void* out,
+                            size_t elements, char* error,
+                            size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:63 -- top-k class labels per prefix
+ * (rows x top per prefix, concatenated). */
+FASTPLS_B200_API int fastpls_resident_classify_path(void* model, const void* x, int rows,
+                                   const int* prefixes, int prefix_count,
+                                   int lda, int top, int* labels, char* error,
+                                   size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:66 -- labels plus response scores. */
+FASTPLS_B200_API int fastpls_resident_classify_response_path(
+    void* model, const void* x, int rows, const int* prefixes,
+    int prefix_count, int lda, int top, int* labels, void* predictions,
+    char* error, size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:69 -- per response: SSE, SS about the
+ * training mean, SS about the observed mean (3 x q). */
+FASTPLS_B200_API int fastpls_resident_response_sums(void* model, const void* x, const void* y,
+                                   const int* labels, int rows, int prefix,
+                                   void* out, char* error,
+                                   size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:71 -- latent scores (rows x prefix). */
+FASTPLS_B200_API int fastpls_resident_project(void* model, const void* x, int rows,
+                             int prefix, void* out, char* error,
+                             size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:73 -- solver controls in effect. */
+FASTPLS_B200_API int fastpls_resident_controls(void* model, int* oversample, int* power,
+                              int* block, int* block_limit,
+                              int* implicit_operator,
+                              int* predictor_crossprod_cache, char* error,
+                              size_t error_capacity);
+
+/* replaces src/cuda_resident_api.h:76 -- release training buffers
+ * (optionally preparing LDA first). */
+FASTPLS_B200_API int fastpls_resident_compact(void* model, int prepare_lda, char* error,
+                             size_t error_capacity);
+
+/* ---- additions (no counterpart in the reference ABI) ------------------- */
+
+/* Number of CUDA devices visible (0 when none); backs has_cuda()
+ * (fastPLS R/native_api.R:601, src/core_cuda_backend.cu:118-121). */
+FASTPLS_B200_API int fastpls_b200_device_count(void);
+
+/* Kernels launched by this library since load (benchmark accounting). */
+FASTPLS_B200_API unsigned long long fastpls_b200_launch_count(void);
+
+/* Batched SIMPLS regression CV over the observed responses and
+ * `permutation_count` row permutations of them (pls.single.cv /
+ * pls.double.cv with perm.test; R/main.R:9419-9450, 12048-12080), all
+ * sharing one device-resident X. permutations: permutation_count x n
+ * zero-based source rows (row i of instance b uses responses[perm_b[i]]);
+ * folds are shared by every instance. Outputs are
+ * (permutation_count + 1) x prefix_count, row-major by instance, row 0 the
+ * observed responses: the selected metric, Q2, RMSD and R2; status per fold.
+ */
+FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation(
+    const void* predictors, const void* responses, const int* folds,
+    const int* permutations, int permutation_count, int precision, int n,
+    int p, int q, const int* prefixes, int prefix_count, int scaling,
+    int metric, double* metrics, double* q2, double* rmsd,
+    double* observed_r2, int* status, char* error, size_t error_capacity);
+
+/* As above with predictors, responses, folds and permutations already in
+ * device memory (prefixes and outputs stay on the host). */
+FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_device(
+    const void* predictors, const void* responses, const int* folds,
+    const int* permutations, int permutation_count, int precision, int n,
+    int p, int q, const int* prefixes, int prefix_count, int scaling,
+    int metric, double* metrics, double* q2, double* rmsd,
+    double* observed_r2, int* status, char* error, size_t error_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTPLS_B200_H */

@@ -1,0 +1,63 @@
+"""Cross-validation entry points and the batched permutation engine vs the oracle."""
+import numpy as np
+import pytest
+
+from fastpls_b200 import api, workloads as W
+from oracle import pls_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("method,family", [("simpls", 3), ("plssvd", 1)])
+@pytest.mark.parametrize("scaling", [1, 2])
+def test_cv_regression(method, family, scaling):
+    x, y = W.latent_regression(240, 150, 3, 4, 0.4, 21, dtype=np.float64)
+    folds = W.uneven_folds(240, 5, 21)
+    pre = [1, 2, 3] if method == "plssvd" else [1, 2, 4, 6, 8]
+    got = api.cv_regression(x, y, folds, pre, scaling=scaling, method=method,
+                            store_predictions=True)
+    ref = O.cv_regression(x, y, folds, pre, scaling=scaling, family=family,
+                          store_predictions=True)
+    for key in ("q2", "rmsd", "observed_r2"):
+        assert np.allclose(got[key], ref[key], rtol=1e-9, atol=1e-11), key
+    assert O.rel_err(got["predictions"], ref["predictions"]) < 1e-9
+    assert list(got["status"]) == [1] * 5
+
+
+@pytest.mark.parametrize("lda", [False, True])
+def test_cv_classification(lda):
+    x, lab = W.latent_classification(260, 120, 4, 3, 0.5, 23, dtype=np.float64)
+    folds = W.uneven_folds(260, 4, 23)
+    pre = [1, 2, 3]
+    got = api.cv_classification(x, lab, 4, folds, pre, lda=lda,
+                                store_predictions=True)
+    ref = O.cv_classification(x, lab, 4, folds, pre, head=int(lda),
+                              store_predictions=True)
+    assert np.array_equal(got["predictions"], ref["predictions"])
+    assert np.allclose(got["metrics"], ref["metrics"])
+
+
+@pytest.mark.parametrize("scaling", [1, 2, 3])
+def test_batched_cv_permutation(scaling):
+    n, p = 300, 420
+    x, y = W.latent_regression(n, p, 3, 5, 0.3, 31, dtype=np.float32)
+    folds = W.uneven_folds(n, 5, 31)
+    perms = W.permutations(n, 3, 31)
+    pre = [1, 2, 3, 5, 8]
+    got = api.cv_permutation(x, y, folds, perms, pre, scaling=scaling, precision=32)
+    x64, y64 = x.astype(np.float64), y.astype(np.float64)
+    for b in range(4):
+        yb = y64 if b == 0 else y64[perms[b - 1]]
+        ref = O.cv_regression(x64, yb, folds, pre, scaling=scaling, family=3)
+        for key in ("q2", "rmsd", "observed_r2"):
+            assert np.allclose(got[key][b], ref[key], rtol=1e-9, atol=1e-11), (b, key)
+
+
+def test_batched_matches_plain_cv():
+    n, p = 200, 90
+    x, y = W.latent_regression(n, p, 2, 3, 0.3, 41, dtype=np.float64)
+    folds = W.uneven_folds(n, 4, 41)
+    pre = [1, 2, 3, 4]
+    plain = api.cv_regression(x, y, folds, pre)
+    batched = api.cv_permutation(x, y, folds, None, pre, precision=64)
+    assert np.allclose(batched["q2"][0], plain["q2"], rtol=1e-10, atol=1e-12)
