@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the batched fitting path on B200: fits per second.
+
+Workload (the cross-validation x permutation configuration): X 5000 x 10000
+FP32 from the latent-factor generator (k = 10, noise 0.3), Y with 3
+continuous responses, 10 uneven folds (480-520 rows), the ncomp path 1..20
+and 200 seeded row permutations of Y -> (1 + 200) x 10 = 2010 SIMPLS fits per
+step, all sharing one device-resident X. Arithmetic is FP64 on the device.
+
+One JSON line on rank 0 with
+  value    fits/s with X, Y, folds and permutations resident in HBM,
+  e2e      fits/s through the host-pointer C ABI call (H2D of every input and
+           D2H of every result inside the timed region, pinned host buffers),
+  roofline the dominant kernel (FP64 GEMM) against the measured FP64 FMA rate,
+  cpu_baseline the reference's own FP64 C++ core (oracle/_ref, OpenBLAS on all
+           host cores) on a bounded sample of the same workload.
+`--impl reference` times that CPU reference alone (the reference arm).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("PLS fits/sec, p50/p99 ms: batched+served vs plain on 1 B200 at "
+          "rel err≤1e-5")
+N, P, Q, FOLDS, NCOMP = 5000, 10000, 3, 10, 20
+
+
+def args_parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--perms", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(rank: int, perms: int):
+    from fastpls_b200 import workloads as W
+    x, y, folds = W.config_cv_permutation(N, P, dtype=np.float32)
+    pm = W.permutations(N, perms, 3 + 1000 * rank)
+    prefixes = np.arange(1, NCOMP + 1, dtype=np.int32)
+    return x, y, folds, pm, prefixes
+
+
+def clock_sampler_start(path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        f = open(path, "w")
+        p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                              "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def clock_sampler_stop(handle, path, device_index):
+    p, f = handle
+    if p is None:
+        return None
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except Exception:
+        p.kill()
+    f.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [s.strip() for s in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for name, val in zip(names, parts[5:9]):
+            if val.lower() == "active":
+                reasons.add(name)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(x, y, folds, prefixes):
+    """The reference FP64 core (oracle/_ref) on the observed-response CV
+    (10 fold fits of the workload) with OpenBLAS on all host cores."""
+    from oracle import ref
+    if not ref.available():
+        return None, None
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    x64 = np.asfortranarray(x, dtype=np.float64)
+    y64 = np.asfortranarray(y, dtype=np.float64)
+    t0 = time.perf_counter()
+    out = ref.cv_regression(x64, y64, folds, prefixes, scaling=1, family=3)
+    dt = time.perf_counter() - t0
+    fits = int(folds.max())
+    return ({"value": fits / dt, "unit": "fits/s", "cores": cores,
+             "kind": "reference",
+             "sample": f"observed-response {fits}-fold CV, ncomp path 1..{NCOMP} "
+                       f"({fits} of the {fits * 201} fits), {dt:.1f} s"}, out)
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import ref
+    x, y, folds, _, prefixes = make_workload(0, 0)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "oracle/_ref/libfastpls_ref.so not built"}))
+        return 0
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    x64 = np.asfortranarray(x, dtype=np.float64)
+    y64 = np.asfortranarray(y, dtype=np.float64)
+    test = np.nonzero(folds == 1)[0]
+    train = np.nonzero(folds != 1)[0]
+    xtr, ytr, xte = x64[train], y64[train], x64[test]
+
+    def one_fit():
+        # one fold fit plus its held-out prefix-path predictions = 1 fit unit
+        m = ref.simpls_fit(xtr, ytr, ncomp=NCOMP, scaling=1)
+        xs = (xte - m["centre"]) / m["scale"]
+        t = xs @ m["R"]
+        for k in range(1, NCOMP + 1):
+            _ = m["ymean"] + t[:, :k] @ m["Q"][:, :k].T
+
+    for _ in range(a.warmup):
+        one_fit()
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        one_fit()
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = a.steps / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000 * tot / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(a.perms),
+        "latency_ms": {"p50": 1000 * float(np.percentile(times, 50)),
+                       "p99": 1000 * float(np.percentile(times, 99))},
+        "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": "one fold fit (4500 x 10000, ncomp 20) + its "
+                                   "held-out prefix-path predictions per step"},
+        "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(perms):
+    return {"workload": f"cv{FOLDS}_perm{perms}_ncomp{NCOMP}_{N}x{P}_f32",
+            "n": N, "p": P, "q": Q, "folds": FOLDS, "fold_sizes": "480-520",
+            "permutations": perms, "ncomp_path": f"1..{NCOMP}",
+            "fits_per_step": (perms + 1) * FOLDS, "storage": "f32",
+            "arithmetic": "f64", "method": "simpls", "scaling": "centering",
+            "l2": "inputs larger than L2 (X 200 MB FP32, Gram 200 MB FP64)",
+            "parallelism": "replicas"}
+
+
+def main():
+    a = args_parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+
+    import torch
+    import torch.distributed as dist
+    from fastpls_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    lib = _lib.load()
+    dev = torch.device("cuda", local)
+
+    x, y, folds, perms, prefixes = make_workload(rank, a.perms)
+    Pn = perms.shape[0]
+    fits_per_step = (Pn + 1) * FOLDS
+    stream = torch.cuda.Stream(device=dev)
+    lib.fastpls_b200_set_stream(C.c_void_p(stream.cuda_stream))
+
+    Xd = torch.from_numpy(np.ravel(x, order="F").copy()).to(dev)
+    Yd = torch.from_numpy(np.ravel(y, order="F").copy()).to(dev)
+    Fd = torch.from_numpy(folds.astype(np.int32)).to(dev)
+    Pd = torch.from_numpy(np.ascontiguousarray(perms, dtype=np.int32).ravel()).to(dev)
+    k = len(prefixes)
+    outs = [np.zeros((Pn + 1) * k) for _ in range(4)]
+    status = np.zeros(FOLDS, dtype=np.int32)
+    err, cap = _lib.error_buffer()
+
+    def ptr(a_):
+        return a_.ctypes.data_as(C.c_void_p)
+
+    def step_device():
+        rc = lib.fastpls_b200_simpls_cv_permutation_device(
+            C.c_void_p(Xd.data_ptr()), C.c_void_p(Yd.data_ptr()),
+            C.c_void_p(Fd.data_ptr()), C.c_void_p(Pd.data_ptr()), Pn, 32, N, P, Q,
+            ptr(prefixes), k, 1, 3, *[ptr(o) for o in outs], ptr(status), err, cap)
+        _lib.check(rc, err)
+
+    # pinned host copies for the end-to-end (host-pointer ABI) measurement
+    Xh = torch.from_numpy(np.ravel(x, order="F").copy()).pin_memory()
+    Yh = torch.from_numpy(np.ravel(y, order="F").copy()).pin_memory()
+    Ph = torch.from_numpy(np.ascontiguousarray(perms, dtype=np.int32).ravel()).pin_memory()
+    folds32 = np.ascontiguousarray(folds, dtype=np.int32)
+
+    def step_host():
+        rc = lib.fastpls_b200_simpls_cv_permutation(
+            C.c_void_p(Xh.data_ptr()), C.c_void_p(Yh.data_ptr()), ptr(folds32),
+            C.c_void_p(Ph.data_ptr()), Pn, 32, N, P, Q, ptr(prefixes), k, 1, 3,
+            *[ptr(o) for o in outs], ptr(status), err, cap)
+        _lib.check(rc, err)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # measured FP64 FMA peak (roofline denominator)
+    pk = C.c_double(0)
+    _lib.check(lib.fastpls_b200_fp64_peak(C.byref(pk), err, cap), err)
+    fp64_peak = pk.value
+
+    for _ in range(max(a.warmup, 3)):
+        step_device()
+    barrier()
+    clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
+    clk = clock_sampler_start(clk_path)
+    launches0 = lib.fastpls_b200_launch_count()
+    lib.fastpls_b200_profile_gemm(1)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    barrier()
+    ev[0].record(stream)
+    for s in range(a.steps):
+        step_device()
+        ev[s + 1].record(stream)
+    barrier()
+    lib.fastpls_b200_profile_gemm(0)
+    launches = lib.fastpls_b200_launch_count() - launches0
+    clocks = clock_sampler_stop(clk, clk_path, local)
+    step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(a.steps)]
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    gms, gfl, gl = C.c_double(0), C.c_double(0), C.c_ulonglong(0)
+    lib.fastpls_b200_profile_gemm_read(C.byref(gms), C.byref(gfl), C.byref(gl))
+    observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
+
+    # end to end through the host-pointer ABI
+    for _ in range(2):
+        step_host()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step_host()
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / a.steps
+
+    ms_per_step = total_ms / a.steps
+    value = world * fits_per_step / (ms_per_step / 1000.0)
+    achieved = gfl.value / (gms.value * 1e-3) / 1e12 if gms.value > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("dgemm_traffic_bytes_per_launch")
+        except Exception:
+            traffic = None
+    h2d = Xh.numel() * 4 + Yh.numel() * 4 + Ph.numel() * 4 + folds32.nbytes
+    d2h = fits_per_step * (k + 1) * 8 + 4
+    line = {
+        "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world,
+        "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(Pn),
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                       "p99": float(np.percentile(step_ms, 99))},
+        "e2e": {"value": world * fits_per_step / (e2e_ms / 1000.0), "unit": "fits/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "fp64", "kernel": "dgemm_tiled (FP64 DFMA)",
+                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": (achieved / fp64_peak) if achieved else None,
+                     "peak_source": "measured in this run (FP64 FMA-chain probe); "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "launches": int(gl.value),
+                     "gemm_share_of_step": (gms.value / a.steps) / ms_per_step,
+                     "traffic": traffic},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu, ref_out = cpu_reference_sample(x, y, folds, prefixes)
+        line["cpu_baseline"] = cpu
+        if ref_out is not None:
+            line["parity"] = {
+                "observed_q2_max_rel_err_vs_fp64_reference": float(
+                    np.max(np.abs(observed_q2 - ref_out["q2"]) /
+                           np.maximum(np.abs(ref_out["q2"]), 1e-300)))}
+    if rank == 0:
+        print(json.dumps(line))
+    lib.fastpls_b200_set_stream(None)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

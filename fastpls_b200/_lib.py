@@ -54,6 +54,10 @@ SIGNATURES = {
     "fastpls_resident_compact": (_i, [_vp, _i, _cp, _sz]),
     "fastpls_b200_device_count": (_i, []),
     "fastpls_b200_launch_count": (_ull, []),
+    "fastpls_b200_set_stream": (None, [_vp]),
+    "fastpls_b200_fp64_peak": (_i, [_dp, _cp, _sz]),
+    "fastpls_b200_profile_gemm": (None, [_i]),
+    "fastpls_b200_profile_gemm_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
     "fastpls_b200_simpls_cv_permutation": (
         _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp,
              _vp, _vp, _vp, _cp, _sz]),

@@ -20,6 +20,10 @@ namespace fpls {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+cudaStream_t& caller_stream() {
+  static cudaStream_t s = nullptr;
+  return s;
+}
 
 namespace {
 
@@ -123,15 +127,17 @@ void cv_permutation(const void* predictors, const void* responses,
       metric < 2 || metric > 4 || permutation_count < 0 ||
       (permutation_count > 0 && !permutations))
     throw std::invalid_argument("invalid batched CUDA CV permutation input");
-  cudaStream_t s = nullptr;
-  FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaStream_t s = caller_stream();
+  const bool own = s == nullptr;
+  if (own) FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   struct Guard {
     cudaStream_t s;
+    bool own;
     ~Guard() {
       cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
+      if (own) cudaStreamDestroy(s);
     }
-  } guard{s};
+  } guard{s, own};
   {
     DeviceArray<T> X, Y;
     DeviceArray<int> P;
@@ -446,6 +452,24 @@ int fastpls_b200_device_count(void) {
 }
 
 unsigned long long fastpls_b200_launch_count(void) { return launch_count(); }
+
+void fastpls_b200_set_stream(void* stream) {
+  caller_stream() = static_cast<cudaStream_t>(stream);
+}
+
+void fastpls_b200_profile_gemm(int enable) { gemm_profile_enable(enable != 0); }
+
+int fastpls_b200_fp64_peak(double* tflops, char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown probe error", [&] {
+    if (!tflops) throw std::invalid_argument("null output");
+    *tflops = fp64_fma_tflops();
+  });
+}
+
+void fastpls_b200_profile_gemm_read(double* milliseconds, double* flops,
+                                    unsigned long long* launches) {
+  gemm_profile_read(milliseconds, flops, launches);
+}
 
 int fastpls_b200_simpls_cv_permutation(
     const void* predictors, const void* responses, const int* folds,

@@ -16,6 +16,10 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 namespace fpls {
 
 namespace {
@@ -196,9 +200,50 @@ void dispatch(const GemmArgs& g, const TA* A, const TB* B, cudaStream_t s) {
 
 }  // namespace
 
+// Live timing of GEMM launches (benchmark instrumentation): when enabled,
+// every gemm_f64 call is bracketed by CUDA events on its own stream.
+namespace {
+struct GemmTiming {
+  bool enabled = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+  std::vector<double> flops;
+};
+GemmTiming& timing() {
+  static GemmTiming t;
+  return t;
+}
+}  // namespace
+
+void gemm_profile_enable(bool on) { timing().enabled = on; }
+
+void gemm_profile_read(double* ms, double* flops, unsigned long long* launches) {
+  GemmTiming& t = timing();
+  double total_ms = 0.0, total_flops = 0.0;
+  for (size_t k = 0; k < t.events.size(); ++k) {
+    float e = 0.f;
+    cudaEventSynchronize(t.events[k].second);
+    cudaEventElapsedTime(&e, t.events[k].first, t.events[k].second);
+    total_ms += e;
+    total_flops += t.flops[k];
+    cudaEventDestroy(t.events[k].first);
+    cudaEventDestroy(t.events[k].second);
+  }
+  if (ms) *ms = total_ms;
+  if (flops) *flops = total_flops;
+  if (launches) *launches = t.events.size();
+  t.events.clear();
+  t.flops.clear();
+}
+
 void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
   require(g.M >= 0 && g.N >= 0 && g.K >= 0, "invalid GEMM dimensions");
   if (g.M == 0 || g.N == 0) return;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (timing().enabled) {
+    FPLS_CHECK(cudaEventCreate(&ev0));
+    FPLS_CHECK(cudaEventCreate(&ev1));
+    FPLS_CHECK(cudaEventRecord(ev0, stream));
+  }
   require(g.splits >= 1, "invalid GEMM split count");
   require(g.splits == 1 || g.beta == 0.0, "split-K GEMM requires beta == 0");
   if (g.a_f32 && g.b_f32)
@@ -216,6 +261,11 @@ void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
                                                    g.split_stride, g.splits);
     count_launch();
     FPLS_LAUNCH("gemm_reduce_splits");
+  }
+  if (ev0) {
+    FPLS_CHECK(cudaEventRecord(ev1, stream));
+    timing().events.emplace_back(ev0, ev1);
+    timing().flops.push_back(2.0 * g.M * (double)g.N * g.K);
   }
 }
 

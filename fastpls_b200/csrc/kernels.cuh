@@ -23,6 +23,15 @@ struct GemmArgs {
 };
 void gemm_f64(const GemmArgs& g, cudaStream_t stream);
 int gemm_pick_splits(int M, int N, int K);
+void gemm_profile_enable(bool on);
+void gemm_profile_read(double* ms, double* flops, unsigned long long* launches);
+
+// Stream that the batched entry points run on when the caller set one
+// (fastpls_b200_set_stream); nullptr means "create a private stream".
+cudaStream_t& caller_stream();
+
+// Measured FP64 FMA throughput of the device (TFLOP/s), probe.cu.
+double fp64_fma_tflops();
 
 // -------------------------------------------------------------- stream.cu
 // Column moments of X (n x p, column-major, leading dimension ld):

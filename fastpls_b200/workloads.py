@@ -80,6 +80,8 @@ def uneven_folds(n, k, seed, low=None, high=None):
 def permutations(n, count, seed):
     """``count`` seeded row permutations (0-based int32, one per row)."""
     g = rng(seed, STREAM_PERM)
+    if count <= 0:
+        return np.zeros((0, n), dtype=np.int32)
     return np.stack([g.permutation(n).astype(np.int32) for _ in range(count)])
 
 

@@ -178,6 +178,23 @@ FASTPLS_B200_API int fastpls_b200_device_count(void);
 /* Kernels launched by this library since load (benchmark accounting). */
 FASTPLS_B200_API unsigned long long fastpls_b200_launch_count(void);
 
+/* Stream on which the batched entry points run (a cudaStream_t; NULL =
+ * each call creates a private stream). Lets a caller time the work with
+ * events on its own stream. Calls stay synchronous. */
+FASTPLS_B200_API void fastpls_b200_set_stream(void* stream);
+
+/* Benchmark instrumentation: bracket every FP64 GEMM launch with CUDA
+ * events on its stream; read returns (and resets) the summed device time,
+ * the algorithmic FLOPs (2 M N K per launch) and the launch count. */
+FASTPLS_B200_API void fastpls_b200_profile_gemm(int enable);
+FASTPLS_B200_API void fastpls_b200_profile_gemm_read(
+    double* milliseconds, double* flops, unsigned long long* launches);
+
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (a short
+ * register-resident FMA-chain kernel timed with CUDA events). */
+FASTPLS_B200_API int fastpls_b200_fp64_peak(double* tflops, char* error,
+                                            size_t error_capacity);
+
 /* Batched SIMPLS regression CV over the observed responses and
  * `permutation_count` row permutations of them (pls.single.cv /
  * pls.double.cv with perm.test; R/main.R:9419-9450, 12048-12080), all
