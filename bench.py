@@ -318,7 +318,7 @@ def main():
         "e2e": {"value": world * fits_per_step / (e2e_ms / 1000.0), "unit": "fits/s",
                 "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "fp64", "kernel": "dgemm_tiled (FP64 DFMA)",
+        "roofline": {"bound": "fp64", "kernel": "dgemm_mma (FP64 DMMA tensor path)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": (achieved / fp64_peak) if achieved else None,
                      "peak_source": "measured in this run (FP64 FMA-chain probe); "

@@ -20,6 +20,25 @@ namespace fpls {
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void keep_pool_memory() {
+  static thread_local int configured_device = -1;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (dev == configured_device) return;
+  cudaMemPool_t pool;
+  size_t free_b = 0, total_b = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+      cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    unsigned long long threshold = total_b / 2;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  cudaGetLastError();
+  configured_device = dev;
+}
+
 cudaStream_t& caller_stream() {
   static cudaStream_t s = nullptr;
   return s;

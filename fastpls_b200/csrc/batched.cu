@@ -263,6 +263,7 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   for (int k = warp; k < a; k += warps) {
     double acc = 0.0;
+#pragma unroll 4
     for (int r = lane; r < n; r += 32) acc = fma(kw[r + (long)k * n], t[r], acc);
     acc = warp_sum(acc);
     if (lane == 0) h[k] = acc;
@@ -274,6 +275,7 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     if (v.fold_of_row[r] != f + 1) {
       double wr = t[r], kr = y[r] - mu;
+#pragma unroll 4
       for (int k = 0; k < a; ++k) {
         wr = fma(-w[r + (long)k * n], h[k], wr);
         kr = fma(-kw[r + (long)k * n], h[k], kr);
@@ -356,6 +358,19 @@ __global__ void fold_kscale(const double* tsum, const double* tsumsq,
   }
 }
 
+// out = X * sqrt(kscale) column-wise (kscale = 1 / sd^2 under autoscaling)
+template <class T>
+__global__ void scale_columns_f64(const T* __restrict__ X, int n, int p,
+                                  const double* __restrict__ kscale,
+                                  double* __restrict__ out) {
+  const long total = (long)n * p;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < total;
+       k += (long)gridDim.x * blockDim.x) {
+    const double v = as_f64(X[k]);
+    out[k] = kscale ? v * sqrt(kscale[k / n]) : v;
+  }
+}
+
 __global__ void response_moments(const double* __restrict__ Y, int n, double* out) {
   __shared__ double scratch[32];
   double s = 0.0, ss = 0.0;
@@ -377,21 +392,27 @@ __global__ void response_moments(const double* __restrict__ Y, int n, double* ou
 // ---------------------------------------------------------------------------
 template <class T>
 void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
+  // FP64 copy of X with the scaling folded in (X D^1/2), then the symmetric
+  // product on the FP64 tensor-core path (lower tiles + mirror).
   gram.reserve((size_t)n * n, s);
+  x64.reserve((size_t)n * p, s);
+  const long total = (long)n * p;
+  scale_columns_f64<T><<<(unsigned)std::min<long>((total + 255) / 256, 16L * num_sms()), 256, 0, s>>>(
+      X, n, p, kscale, x64.get());
+  count_launch();
+  FPLS_LAUNCH("scale_columns_f64");
   GemmArgs g;
   g.M = n;
   g.N = n;
   g.K = p;
-  g.A = X;
+  g.A = x64.get();
   g.lda = n;
-  g.a_f32 = std::is_same<T, float>::value;
-  g.B = X;
+  g.B = x64.get();
   g.ldb = n;
-  g.b_f32 = g.a_f32;
   g.trans_b = true;
-  g.kscale = kscale;
   g.C = gram.get();
   g.ldc = n;
+  g.lower = gemm_mma_supported(g);
   gemm_f64(g, s);
 }
 

@@ -38,7 +38,7 @@ struct BatchedCv {
   int n = 0, p = 0, q = 0, P = 0, prefix_count = 0, scaling = 1, kmax = 0;
   int folds = 0, max_test = 1;
   bool center = true;
-  DeviceArray<double> gram, Y64;
+  DeviceArray<double> gram, Y64, x64;
   DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag;
 };
 

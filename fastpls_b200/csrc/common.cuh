@@ -30,6 +30,11 @@ inline void require(bool ok, const char* message) {
   if (!ok) throw std::invalid_argument(message);
 }
 
+// Let the device's stream-ordered pool keep freed memory (up to half the
+// device) instead of returning it to the driver at every synchronisation:
+// repeated fits then reuse mapped pages rather than remapping gigabytes.
+void keep_pool_memory();
+
 // Device buffer owned by the host object that allocated it (stream-ordered).
 template <class T>
 class DeviceArray {
@@ -49,6 +54,7 @@ class DeviceArray {
   }
   void allocate(std::size_t count, cudaStream_t stream) {
     release();
+    keep_pool_memory();
     stream_ = stream;
     count_ = count;
     if (count) FPLS_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&ptr_),

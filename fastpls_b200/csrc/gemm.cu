@@ -246,7 +246,12 @@ void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
   }
   require(g.splits >= 1, "invalid GEMM split count");
   require(g.splits == 1 || g.beta == 0.0, "split-K GEMM requires beta == 0");
-  if (g.a_f32 && g.b_f32)
+  const bool use_mma = gemm_mma_supported(g);
+  require(!g.lower || (g.M == g.N && use_mma && g.splits == 1 && g.beta == 0.0),
+          "symmetric GEMM needs the FP64 tensor-core path");
+  if (use_mma)
+    gemm_mma_launch(g, g.lower, stream);
+  else if (g.a_f32 && g.b_f32)
     dispatch(g, static_cast<const float*>(g.A), static_cast<const float*>(g.B), stream);
   else if (g.a_f32)
     dispatch(g, static_cast<const float*>(g.A), static_cast<const double*>(g.B), stream);
@@ -254,6 +259,7 @@ void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
     dispatch(g, static_cast<const double*>(g.A), static_cast<const float*>(g.B), stream);
   else
     dispatch(g, static_cast<const double*>(g.A), static_cast<const double*>(g.B), stream);
+  if (g.lower) mirror_lower_triangle(g.C, g.M, g.ldc, stream);
   if (g.splits > 1) {
     const long total = (long)g.M * g.N;
     const unsigned blocks = (unsigned)std::min<long>((total + 255) / 256, 4L * num_sms());
@@ -265,7 +271,9 @@ void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
   if (ev0) {
     FPLS_CHECK(cudaEventRecord(ev1, stream));
     timing().events.emplace_back(ev0, ev1);
-    timing().flops.push_back(2.0 * g.M * (double)g.N * g.K);
+    // algorithmic FLOPs: a symmetric product needs only its lower triangle
+    timing().flops.push_back(g.lower ? (double)g.M * (g.M + 1.0) * g.K
+                                     : 2.0 * g.M * (double)g.N * g.K);
   }
 }
 

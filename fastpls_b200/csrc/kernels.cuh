@@ -20,10 +20,16 @@ struct GemmArgs {
   long ldc = 0;
   int splits = 1;         // split-K slices (beta must be 0 when > 1)
   long split_stride = 0;  // element stride between partial slices of C
+  bool lower = false;     // symmetric result: compute lower tiles, mirror
 };
 void gemm_f64(const GemmArgs& g, cudaStream_t stream);
 int gemm_pick_splits(int M, int N, int K);
 void gemm_profile_enable(bool on);
+// DMMA tensor-core path (gemm_mma.cu): FP64 A (not transposed), FP64 B,
+// 16-byte aligned operands with even leading dimensions.
+bool gemm_mma_supported(const GemmArgs& g);
+void gemm_mma_launch(const GemmArgs& g, bool lower, cudaStream_t stream);
+void mirror_lower_triangle(double* C, int n, long ldc, cudaStream_t stream);
 void gemm_profile_read(double* ms, double* flops, unsigned long long* launches);
 
 // Stream that the batched entry points run on when the caller set one

@@ -88,6 +88,17 @@ def test_plssvd(classify):
     model.close()
 
 
+@pytest.mark.parametrize("m,k,n", [(256, 300, 190), (130, 78, 211), (384, 64, 128),
+                                   (2, 2, 2), (258, 34, 130)])
+def test_cuda_gemm_fp64_tensor_path(m, k, n):
+    """Even shapes take the DMMA path (gemm_mma.cu); ragged tiles included."""
+    rng = np.random.default_rng(m + k + n)
+    a = rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n))
+    got = api.cuda_gemm(a, b, precision=64)
+    assert O.rel_err(got, a @ b) < 1e-14
+
+
 def test_cuda_gemm():
     rng = np.random.default_rng(3)
     a = rng.standard_normal((130, 77))
