@@ -46,6 +46,8 @@ def args_parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--perms", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-perms", type=int, default=3,
+                    help="permutations sampled for the one-fit-at-a-time path")
     return ap.parse_args()
 
 
@@ -296,6 +298,40 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / a.steps
 
+    # the plain drop-in: one CV call per permutation through the reference's
+    # regression CV entry point (per-fold fits, FP32 storage), sampled
+    plain = None
+    if a.plain_perms > 0:
+        k_ = len(prefixes)
+        pm_, q2_, rm_, r2_ = (np.zeros(k_) for _ in range(4))
+        st_ = np.zeros(FOLDS, dtype=np.int32)
+        xf = np.asfortranarray(x)
+        yf = np.asfortranarray(y)
+        fo = np.ascontiguousarray(folds, dtype=np.int32)
+
+        def plain_call(b_):
+            yb = yf if b_ == 0 else np.asfortranarray(yf[perms[b_ - 1]])
+            rc = lib.fastpls_resident_simpls_cv_regression(
+                ptr(xf), ptr(yb), ptr(fo), 32, N, P, Q, ptr(prefixes), k_, 1, 3,
+                32, 5, C.c_ulonglong(1), 0, None, ptr(st_), ptr(pm_), ptr(q2_),
+                ptr(rm_), ptr(r2_), err, cap)
+            _lib.check(rc, err)
+        plain_call(0)
+        plain_q2_observed = q2_.copy()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for b_ in range(a.plain_perms):
+            plain_call(b_)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        plain_fits = a.plain_perms * FOLDS
+        plain = {"value": plain_fits / dt, "unit": "fits/s",
+                 "sample": f"{a.plain_perms} permutations x {FOLDS} folds through "
+                           "fastpls_resident_simpls_cv_regression (one fold fit at a "
+                           "time, FP32 storage, host buffers)",
+                 "q2_path_max_abs_diff_vs_batched": float(
+                     np.max(np.abs(plain_q2_observed - observed_q2)))}
+
     ms_per_step = total_ms / a.steps
     value = world * fits_per_step / (ms_per_step / 1000.0)
     achieved = gfl.value / (gms.value * 1e-3) / 1e12 if gms.value > 0 else None
@@ -327,6 +363,9 @@ def main():
                      "gemm_share_of_step": (gms.value / a.steps) / ms_per_step,
                      "traffic": traffic},
         "gpu_launches": int(launches),
+        "plain": plain,
+        "batched_over_plain_e2e": (world * fits_per_step / (e2e_ms / 1000.0)) / plain["value"]
+        if plain else None,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
