@@ -220,6 +220,24 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_device(
     int metric, double* metrics, double* q2, double* rmsd,
     double* observed_r2, int* status, char* error, size_t error_capacity);
 
+/* out (p x nb, FP64) = X^T V for device-resident X (n x p, leading
+ * dimension ldx, FP32 or FP64 by `precision`), V (n x nb FP64, ldv) and out
+ * (ldo), without any memory allocation by the library: for callers whose
+ * host owns all device memory (a fixed memory plan, admission by memory
+ * footprint) or that must not stall on the allocator. No counterpart in the
+ * reference ABI. Partial sums live in one file-scope device array of
+ * 2097152 doubles (16 MiB) that every GPU loading the library keeps until
+ * exit; requests with p * nb above that size, or nb above 32, are rejected
+ * with an error. The array's address is looked up on the first call made on
+ * each device, so make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. Runs on `stream` (a cudaStream_t, NULL = default stream)
+ * and returns after the work completes. */
+FASTPLS_B200_API int fastpls_b200_crossprod_noalloc(
+    const void* x, int precision, int n, int p, long ldx, const double* v,
+    long ldv, int nb, double* out, long ldo, void* stream, char* error,
+    size_t error_capacity);
+
 #ifdef __cplusplus
 }
 #endif
