@@ -117,18 +117,16 @@ __global__ void initial_gram(InstanceView v, const double* C0, const double* KC0
     }
 }
 
-// Dominant direction: u = C z / sqrt(lambda) (zero on held-out rows,
-// re-centred over the training rows), written to column i of U.
-__global__ void direction_batched(InstanceView v, const double* G,
-                                  const double* C, double* U, int* flag) {
-  extern __shared__ double sm[];
-  __shared__ double scratch[32];
-  __shared__ double zs[kBatchMaxResponses];
-  const int i = blockIdx.x;
+// Dominant direction of instance i: u = C z / sqrt(lambda) (zero on held-out
+// rows, re-centred over the training rows), written to column i of U. When
+// KC0 is given (first component, C = C0) the product K u is formed directly
+// as (K C0) z / sqrt(lambda) into column i of Y1, replacing one GEMM.
+__device__ void direction_body(const InstanceView& v, int i, const double* G,
+                               const double* C, double* U, const double* KC0,
+                               double* Y1, int* flag, double* A, double* E,
+                               double* zs, double* scratch) {
   const int f = v.inst_fold[i];
   const int n = v.n, q = v.q;
-  double* A = sm;
-  double* E = sm + q * q;
   const double* g = G + (long)i * q * (q + 1) / 2;
   for (int c = threadIdx.x; c < q; c += blockDim.x)
     for (int d = 0; d <= c; ++d) {
@@ -167,6 +165,24 @@ __global__ void direction_batched(InstanceView v, const double* G,
     for (int r = threadIdx.x; r < n; r += blockDim.x)
       if (v.fold_of_row[r] != f + 1) u[r] -= mu;
   }
+  if (KC0) {
+    const double* kc = KC0 + (long)i * n * q;
+    double* y = Y1 + (long)i * n;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      double val = 0.0;
+      for (int k = 0; k < q; ++k) val = fma(kc[r + (long)k * n], zs[k], val);
+      y[r] = val;
+    }
+  }
+}
+
+__global__ void direction_batched(InstanceView v, const double* G,
+                                  const double* C, double* U,
+                                  const double* KC0, double* Y1, int* flag) {
+  extern __shared__ double sm[];
+  __shared__ double scratch[32];
+  __shared__ double zs[kBatchMaxResponses];
+  direction_body(v, blockIdx.x, G, C, U, KC0, Y1, flag, sm, sm + v.q * v.q, zs, scratch);
 }
 
 // Scores from Y1 = K U: centre over training rows, normalise, emit the
@@ -241,9 +257,9 @@ __global__ void scores_batched(InstanceView v, const double* Y1, double* Tm,
 // Kw = Kt - KW h ; normalise by sqrt(w^T Kw) ; row = Kw^T C ; C -= w row ;
 // G -= row row^T.
 __global__ void deflate_batched(InstanceView v, const double* Y2,
-                                const double* Tm, double* W, double* KW,
+                                double* Tm, double* W, double* KW,
                                 double* C, double* G, int a, int* flag) {
-  extern __shared__ double sm[];  // h (a) + row (q)
+  extern __shared__ double sm[];  // h (kmax) + row (q) + 2 q^2 (direction)
   __shared__ double scratch[32];
   const int i = blockIdx.x;
   const int f = v.inst_fold[i];
@@ -314,6 +330,11 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
     for (int cc = 0; cc < q; ++cc)
       for (int d = 0; d <= cc; ++d) g[cc * (cc + 1) / 2 + d] -= row[cc] * row[d];
   }
+  __syncthreads();
+  // next component's direction, written over this instance's t~ column
+  __shared__ double zs[kBatchMaxResponses];
+  direction_body(v, i, G, C, Tm, nullptr, nullptr, flag, sm + kmax + q,
+                 sm + kmax + q + q * q, zs, scratch);
 }
 
 template <class T>
@@ -446,7 +467,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   DeviceArray<double> ym((size_t)I * q, s), sst(I, s), sse((size_t)I * prefix_count, s);
   DeviceArray<double> yhat((size_t)I * max_test * q, s);
   DeviceArray<double> Wb((size_t)I * n * kmax, s), KWb((size_t)I * n * kmax, s);
-  DeviceArray<double> U((size_t)n * I, s), Y1(std::max(nq * I, (size_t)n * I), s);
+  DeviceArray<double> U((size_t)n * I, s), Y1((size_t)n * I, s), KC0(nq * I, s);
 
   init_instances<<<I, BT, 0, s>>>(v, C0.get(), C.get(), ym.get(), sst.get(),
                                   yhat.get(), max_test, sse.get(), prefix_count);
@@ -461,18 +482,20 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   g.lda = n;
   g.B = C0.get();
   g.ldb = n;
-  g.C = Y1.get();
+  g.C = KC0.get();
   g.ldc = n;
   gemm_f64(g, s);
-  initial_gram<<<I, BT, 0, s>>>(v, C0.get(), Y1.get(), G.get());
+  initial_gram<<<I, BT, 0, s>>>(v, C0.get(), KC0.get(), G.get());
   count_launch();
   FPLS_LAUNCH("initial_gram");
 
   const size_t smem_dir = 2 * (size_t)q * q * sizeof(double);
+  // first direction; K u comes from K C0 (no GEMM)
+  direction_batched<<<I, BT, smem_dir, s>>>(v, G.get(), C.get(), U.get(), KC0.get(), Y1.get(), flag.get());
+  count_launch();
+  FPLS_LAUNCH("direction_batched");
+  KC0.release();
   for (int a = 0; a < kmax; ++a) {
-    direction_batched<<<I, BT, smem_dir, s>>>(v, G.get(), C.get(), U.get(), flag.get());
-    count_launch();
-    FPLS_LAUNCH("direction_batched");
     GemmArgs k1;
     k1.M = n;
     k1.N = I;
@@ -483,17 +506,15 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     k1.ldb = n;
     k1.C = Y1.get();
     k1.ldc = n;
-    gemm_f64(k1, s);
+    if (a > 0) gemm_f64(k1, s);  // Y1 = K u (a = 0: formed from K C0)
     scores_batched<<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(),
                                     yhat.get(), max_test, a, d_slot.get(),
                                     prefix_count, sse.get(), nullptr, flag.get());
     count_launch();
     FPLS_LAUNCH("scores_batched");
     if (a + 1 == kmax) break;  // the last deflation is never used
-    GemmArgs k2 = k1;
-    k2.B = U.get();  // masked training scores t~ (written by scores_batched)
-    gemm_f64(k2, s);
-    deflate_batched<<<I, BT, (kmax + q) * sizeof(double), s>>>(
+    gemm_f64(k1, s);  // Y1 = K t~ (U now holds the masked training scores)
+    deflate_batched<<<I, BT, (kmax + q + 2 * q * q) * sizeof(double), s>>>(
         v, Y1.get(), U.get(), Wb.get(), KWb.get(), C.get(), G.get(), a, flag.get());
     count_launch();
     FPLS_LAUNCH("deflate_batched");

@@ -17,6 +17,7 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <utility>
 #include <vector>
 
@@ -179,6 +180,38 @@ __global__ void gemm_reduce_splits(int M, int N, double* C, long ldc,
   }
 }
 
+// C[:, :] = sum of `splits` contiguous M x N slices (fixed order)
+__global__ void sum_slices(const double* __restrict__ slices, int splits, int M,
+                           int N, double* C, long ldc) {
+  const long total = (long)M * N;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    double v = slices[idx];
+    for (int z = 1; z < splits; ++z) v += slices[idx + z * total];
+    C[(idx % M) + (idx / M) * ldc] = v;
+  }
+}
+
+// Split-K factor (1..4) that best fills whole waves of SMs for an MMA tile
+// grid, each split keeping at least 512 of K; 1 when no split helps.
+int gemm_mma_wave_splits(int M, int N, int K) {
+  const double tiles = (double)ceil_div(M, 128) * ceil_div(N, 128);
+  const double sms = num_sms();
+  int best = 1;
+  double best_score = 0.0;
+  for (int s = 1; s <= 4; ++s) {
+    if (s > 1 && K / s < 512) break;
+    const double waves = tiles * s / sms;
+    const double eff = waves / std::ceil(waves);
+    const double score = eff - 0.01 * (s - 1);
+    if (score > best_score + 1e-9) {
+      best_score = score;
+      best = s;
+    }
+  }
+  return best;
+}
+
 template <class TA, class TB, bool TA_T, bool TB_T>
 void launch(const GemmArgs& g, const TA* A, const TB* B, cudaStream_t stream) {
   const dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), g.splits);
@@ -249,7 +282,25 @@ void gemm_f64(const GemmArgs& g, cudaStream_t stream) {
   const bool use_mma = gemm_mma_supported(g);
   require(!g.lower || (g.M == g.N && use_mma && g.splits == 1 && g.beta == 0.0),
           "symmetric GEMM needs the FP64 tensor-core path");
-  if (use_mma)
+  const int wave_splits = use_mma && !g.lower && g.splits == 1 && g.beta == 0.0
+                              ? gemm_mma_wave_splits(g.M, g.N, g.K) : 1;
+  DeviceArray<double> slices;
+  if (wave_splits > 1) {
+    // split K so the tile count fills whole waves of SMs; the slices are
+    // summed in a fixed order afterwards (deterministic)
+    slices.allocate((size_t)wave_splits * g.M * g.N, stream);
+    GemmArgs h = g;
+    h.C = slices.get();
+    h.ldc = g.M;
+    h.splits = wave_splits;
+    h.split_stride = (long)g.M * g.N;
+    gemm_mma_launch(h, false, stream);
+    const long total = (long)g.M * g.N;
+    sum_slices<<<(unsigned)std::min<long>((total + 255) / 256, 16L * num_sms()), 256, 0, stream>>>(
+        slices.get(), wave_splits, g.M, g.N, g.C, g.ldc);
+    count_launch();
+    FPLS_LAUNCH("sum_slices");
+  } else if (use_mma)
     gemm_mma_launch(g, g.lower, stream);
   else if (g.a_f32 && g.b_f32)
     dispatch(g, static_cast<const float*>(g.A), static_cast<const float*>(g.B), stream);
