@@ -408,6 +408,26 @@ void prepare_responses(const T* Y, const int* labels, int n, int m, double* Yc,
   FPLS_LAUNCH("prepare_responses");
 }
 
+__global__ void s_times_z(const double* __restrict__ S, int p, int m,
+                          const double* __restrict__ zs, double* w) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p; j += gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int c = 0; c < m; ++c) v = fma(S[j + (long)c * p], zs[c], v);
+    w[j] = v;
+  }
+}
+
+void dominant_direction(const double* S, int p, int m, const double* gpk,
+                        double* zs, double* w, Workspace& ws, cudaStream_t s) {
+  const size_t smem_dir = 2 * (size_t)m * m * sizeof(double);
+  if (smem_dir > 48 * 1024)
+    FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
+  direction_kernel<<<1, 64, smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get());
+  s_times_z<<<std::min<unsigned>(ceil_div(p, TB), 4 * num_sms()), TB, 0, s>>>(S, p, m, zs, w);
+  count_launch(2);
+  FPLS_LAUNCH("dominant_direction");
+}
+
 template <class T>
 void compute_crossprod(const T* X, int n, int p, long ld, const double* Yc,
                        const double* ycsum, int m, int scaling,

@@ -181,7 +181,7 @@ class TypedHandle final : public ResidentHandle {
       throw std::invalid_argument("LDA requires class labels");
     const int kmax = prefixes[count - 1];
     upload_rows(x, rows);
-    project_rows<T>(model_, xbuf_.get(), rows, rows, kmax, scores(rows, kmax), rows, ws_, stream_);
+    score_rows(rows, kmax);
     const int q = model_.m;
     pred_.reserve((size_t)rows * q, stream_);
     conv_.reserve((size_t)rows * q, stream_);
@@ -205,7 +205,7 @@ class TypedHandle final : public ResidentHandle {
     check_path(prefixes, count, model_.a);
     const int kmax = prefixes[count - 1];
     upload_rows(x, rows);
-    project_rows<T>(model_, xbuf_.get(), rows, rows, kmax, scores(rows, kmax), rows, ws_, stream_);
+    score_rows(rows, kmax);
     pred_.reserve((size_t)rows * q, stream_);
     disc_.reserve((size_t)rows * q, stream_);
     conv_.reserve((size_t)rows * q, stream_);
@@ -234,7 +234,7 @@ class TypedHandle final : public ResidentHandle {
     if (!x || !out || rows < 1 || prefix < 1 || prefix > model_.a)
       throw std::invalid_argument("invalid resident score request");
     upload_rows(x, rows);
-    project_rows<T>(model_, xbuf_.get(), rows, rows, prefix, scores(rows, prefix), rows, ws_, stream_);
+    score_rows(rows, prefix);
     conv_.reserve((size_t)rows * prefix, stream_);
     download(scores_.get(), (long)rows * prefix, static_cast<T*>(out));
     FPLS_CHECK(cudaStreamSynchronize(stream_));
@@ -249,7 +249,7 @@ class TypedHandle final : public ResidentHandle {
       throw std::invalid_argument("invalid resident prediction input");
     const int q = model_.m;
     upload_rows(x, rows);
-    project_rows<T>(model_, xbuf_.get(), rows, rows, prefix, scores(rows, prefix), rows, ws_, stream_);
+    score_rows(rows, prefix);
     pred_.reserve((size_t)rows * q, stream_);
     predict_from_scores(model_, scores_.get(), rows, rows, prefix, pred_.get(), rows, stream_);
     DeviceArray<T> yd;
@@ -274,7 +274,7 @@ class TypedHandle final : public ResidentHandle {
   }
 
   void export_field(int field, void* out, std::size_t size) override {
-    const std::size_t a = model_.a, q = model_.m, p = model_.p, fp = model_.feature_p;
+    const std::size_t a = model_.a, q = model_.m, p = rq_.p, fp = model_.feature_p;
     const std::size_t counts[] = {fp * a, q * a, (size_t)model_.n * a, p, p, q, fp * a, a + 1};
     if (field < 0 || field > 7 || !out || size != counts[field])
       throw std::invalid_argument("invalid resident field output size");
@@ -283,8 +283,8 @@ class TypedHandle final : public ResidentHandle {
       case 0: src = model_.R.get(); break;
       case 1: src = q_export(); break;
       case 2: src = model_.T.get(); break;
-      case 3: src = model_.mean.get(); break;
-      case 4: src = model_.scale.get(); break;
+      case 3: src = model_.method == kKernelPls ? model_.in_mean.get() : model_.mean.get(); break;
+      case 4: src = model_.method == kKernelPls ? model_.in_scale.get() : model_.scale.get(); break;
       case 5: src = model_.ymean.get(); break;
       default: ensure_variance(); src = field == 6 ? loadings_.get() : var_ss_.get(); break;
     }
@@ -314,6 +314,7 @@ class TypedHandle final : public ResidentHandle {
     }
     FPLS_CHECK(cudaStreamSynchronize(stream_));
     xtrain_.release();
+    design_.release();
     model_.V.release();
     ws_.stream_partial.release();
     FPLS_CHECK(cudaStreamSynchronize(stream_));
@@ -326,12 +327,15 @@ class TypedHandle final : public ResidentHandle {
     if (!rq_.x) throw std::invalid_argument("invalid resident matrix or precision");
     if ((rq_.y == nullptr) == (rq_.labels == nullptr))
       throw std::invalid_argument("provide responses or labels, not both");
-    if (n < 2 || p < 1 || q < 1 || a < 1 || a > std::min(n - 1, p) || rq_.scaling < 1 || rq_.scaling > 3)
+    if (rq_.method == kKernelPls && (n < 2 || p < 1 || q < 1 || a < 1 || a > n - 1))
+      throw std::invalid_argument("invalid resident CUDA nonlinear kernel PLS dimensions or controls");
+    if (rq_.method == kOpls && (n < 2 || p < 1 || q < 1 || a < 1 || a > std::min(n - 1, p)))
+      throw std::invalid_argument("invalid resident CUDA OPLS dimensions");
+    if (rq_.method != kKernelPls &&
+        (n < 2 || p < 1 || q < 1 || a < 1 || a > std::min(n - 1, p) || rq_.scaling < 1 || rq_.scaling > 3))
       throw std::invalid_argument(rq_.method == kPlssvd ? "invalid resident PLS-SVD dimensions"
                                                         : "invalid resident SIMPLS dimensions");
     if (cls && q < 2) throw std::invalid_argument("classification requires at least two classes");
-    if (rq_.method != kSimpls && rq_.method != kPlssvd)
-      throw std::invalid_argument("this build fits SIMPLS and PLS-SVD resident models only");
     xtrain_.allocate((size_t)n * p, stream_);
     FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
     DeviceArray<T> y;
@@ -355,10 +359,17 @@ class TypedHandle final : public ResidentHandle {
                          model_.ymean.get(), ycsum.get(), ws_.flag.get(), stream_);
     if (rq_.method == kPlssvd)
       fit_plssvd<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
+    else if (rq_.method == kOpls)
+      fit_opls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, rq_.north, model_, ws_,
+                  design_, stream_);
+    else if (rq_.method == kKernelPls)
+      fit_kernelpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, rq_.kernel,
+                       rq_.gamma, rq_.degree, rq_.coef0, model_, ws_, design_, stream_);
     else
       fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
     raise_on_flag(ws_, stream_, rq_.method == kPlssvd
         ? "resident PLS-SVD failed: invalid labels, decomposition or score Gram"
+        : rq_.method == kOpls ? "resident CUDA OPLS filtering failed"
         : "resident SIMPLS failed: invalid labels, decomposition or component norm");
   }
 
@@ -369,9 +380,17 @@ class TypedHandle final : public ResidentHandle {
     return scores_.get();
   }
 
+  // latent scores of the uploaded rows (xbuf_) into scores_ (rows x k)
+  void score_rows(int rows, int k) {
+    if (model_.method == kKernelPls)
+      kernel_scores<T>(model_, xbuf_.get(), rows, rows, k, scores(rows, k), rows, ws_, stream_);
+    else
+      project_rows<T>(model_, xbuf_.get(), rows, rows, k, scores(rows, k), rows, ws_, stream_);
+  }
+
   void upload_rows(const void* x, int rows) {
-    xbuf_.reserve((size_t)rows * model_.p, stream_);
-    FPLS_CHECK(cudaMemcpyAsync(xbuf_.get(), x, sizeof(T) * rows * model_.p, cudaMemcpyHostToDevice, stream_));
+    xbuf_.reserve((size_t)rows * rq_.p, stream_);
+    FPLS_CHECK(cudaMemcpyAsync(xbuf_.get(), x, sizeof(T) * rows * rq_.p, cudaMemcpyHostToDevice, stream_));
   }
 
   void download(const double* src, long count, T* dst) {
@@ -399,19 +418,41 @@ class TypedHandle final : public ResidentHandle {
 
   void ensure_variance() {
     if (loadings_) return;
+    if (design_) {
+      const int fp = model_.feature_p;
+      DeviceArray<double> zero(fp, stream_), one(fp, stream_);
+      zero.zero(stream_);
+      fill_ones(one.get(), fp);
+      variance_from<double>(design_.get(), fp, zero.get(), one.get());
+      return;
+    }
     if (!xtrain_) throw std::invalid_argument("resident variance requires the training predictors (call before compaction)");
-    const int n = model_.n, p = model_.p, a = model_.a;
+    variance_from<T>(xtrain_.get(), model_.p, model_.mean.get(), model_.scale.get());
+  }
+
+  void fill_ones(double* ptr, int count) {
+    std::vector<double> ones(count, 1.0);
+    FPLS_CHECK(cudaMemcpyAsync(ptr, ones.data(), sizeof(double) * count, cudaMemcpyHostToDevice, stream_));
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  // loadings P and per-component SS from predictors X (n x p, standardised by
+  // mean/scale) and the training scores (variance_loadings/variance_finish,
+  // src/cuda_resident_variance.cuh:10-94)
+  template <class TX>
+  void variance_from(const TX* X, int p, const double* mean, const double* scale) {
+    const int n = model_.n, a = model_.a;
     DeviceArray<double> cross((size_t)p * a, stream_), seq((size_t)p * a, stream_);
     DeviceArray<double> gram((size_t)a * a, stream_), tsum(a, stream_);
     DeviceArray<double> mom((size_t)2 * p, stream_);
     loadings_.allocate((size_t)p * a, stream_);
     var_ss_.allocate(a + 1, stream_);
-    xtv_product<T>(xtrain_.get(), n, p, n, model_.T.get(), n, a, cross.get(), p, ws_.stream_partial, stream_);
-    column_moments<T>(xtrain_.get(), n, p, n, nullptr, 0, mom.get(), mom.get() + p, nullptr, ws_.stream_partial, stream_);
+    xtv_product<TX>(X, n, p, n, model_.T.get(), n, a, cross.get(), p, ws_.stream_partial, stream_);
+    column_moments<TX>(X, n, p, n, nullptr, 0, mom.get(), mom.get() + p, nullptr, ws_.stream_partial, stream_);
     column_sums_kernel<<<a, 256, 0, stream_>>>(model_.T.get(), n, n, tsum.get());
     count_launch();
     standardize_cross<<<std::min<unsigned>(ceil_div((size_t)p * a, 256), 8 * num_sms()), 256, 0, stream_>>>(
-        cross.get(), p, a, model_.mean.get(), model_.scale.get(), tsum.get());
+        cross.get(), p, a, mean, scale, tsum.get());
     count_launch();
     GemmArgs g;
     g.M = a; g.N = a; g.K = n;
@@ -423,8 +464,7 @@ class TypedHandle final : public ResidentHandle {
         cross.get(), gram.get(), p, a, loadings_.get(), seq.get());
     count_launch();
     variance_finish_kernel<<<std::min(a + 1, 4 * num_sms()), 256, 0, stream_>>>(
-        seq.get(), gram.get(), mom.get(), mom.get() + p, model_.mean.get(),
-        model_.scale.get(), n, p, a, var_ss_.get());
+        seq.get(), gram.get(), mom.get(), mom.get() + p, mean, scale, n, p, a, var_ss_.get());
     count_launch();
     FPLS_LAUNCH("variance");
     FPLS_CHECK(cudaStreamSynchronize(stream_));
@@ -436,6 +476,7 @@ class TypedHandle final : public ResidentHandle {
     model_ = DeviceModel();
     ws_ = Workspace();
     xtrain_.release();
+    design_.release();
     xbuf_.release();
     scores_.release();
     pred_.release();
@@ -456,7 +497,7 @@ class TypedHandle final : public ResidentHandle {
   DeviceModel model_;
   Workspace ws_;
   DeviceArray<T> xtrain_, xbuf_, conv_;
-  DeviceArray<double> scores_, pred_, disc_, loadings_, var_ss_;
+  DeviceArray<double> scores_, pred_, disc_, loadings_, var_ss_, design_;
   DeviceArray<int> top_;
   std::unique_ptr<LdaState> lda_;
 };

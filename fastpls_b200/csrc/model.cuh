@@ -37,6 +37,11 @@ struct DeviceModel {
   DeviceArray<double> W;                   // PLS-SVD per-prefix weights (a x m x a)
   DeviceArray<int> labels;                 // training labels (classification)
   std::vector<int> class_counts;           // host copy (classification)
+  // kernel PLS: input standardisation (in_p columns), standardised training
+  // rows, their squared norms, training kernel column means (+ grand mean)
+  int in_p = 0, kernel_kind = 0, degree = 0;
+  double gamma = 0.0, coef0 = 0.0;
+  DeviceArray<double> in_mean, in_scale, reference, ref_norms, kcol_means;
 };
 
 // Centre responses (dense Y, or one-hot minus prior for one-based labels).
@@ -70,6 +75,33 @@ void compute_crossprod(const T* X, int n, int p, long ld, const double* Yc,
 // Packed lower triangle of S^T S (m x m) for S p x m, into gpk.
 void gram_of_columns(double* S, int p, int m, double* gpk, Workspace& ws,
                      cudaStream_t stream);
+
+// Unit dominant left singular vector w (p) of S (p x m) from its packed Gram
+// (gpk, from gram_of_columns); zs receives z / sqrt(lambda).
+void dominant_direction(const double* S, int p, int m, const double* gpk,
+                        double* zs, double* w, Workspace& ws, cudaStream_t s);
+
+// OPLS (north orthogonal filters + SIMPLS on the filtered predictors);
+// `design` keeps the filtered standardised predictors (FP64 n x p).
+template <class T>
+void fit_opls(const T* X, int n, int p, long ld, const double* Yc,
+              const double* ycsum, int m, int components, int scaling,
+              int north, DeviceModel& model, Workspace& ws,
+              DeviceArray<double>& design, cudaStream_t s);
+
+// Nonlinear kernel PLS (kind 2 = RBF, 3 = polynomial); `design` keeps the
+// centred n x n training kernel.
+template <class T>
+void fit_kernelpls(const T* X, int n, int p, long ld, const double* Yc,
+                   const double* ycsum, int m, int components, int scaling,
+                   int kind, double gamma, int degree, double coef0,
+                   DeviceModel& model, Workspace& ws, DeviceArray<double>& design,
+                   cudaStream_t s);
+
+// Kernel PLS scores of new rows (rows x k).
+template <class T>
+void kernel_scores(const DeviceModel& model, const T* X, int rows, long ld, int k,
+                   double* out, long ldo, Workspace& ws, cudaStream_t s);
 
 // Latent scores of new rows: out (rows x k) = Xs R[:, :k] (FP64).
 template <class T>

@@ -33,7 +33,8 @@ import numpy as np
 __all__ = [
     "column_statistics", "simpls_fit", "simpls_predict", "simpls_project",
     "plssvd_fit", "plssvd_predict", "lda_train", "lda_discriminants",
-    "row_argmax", "topk", "response_sums", "cv_regression",
+    "row_argmax", "topk", "response_sums", "cv_regression", "opls_fit",
+    "opls_predict", "kernelpls_fit", "kernelpls_predict",
     "cv_classification", "permutation_pvalue", "align_signs", "rel_err",
 ]
 
@@ -203,6 +204,82 @@ def plssvd_predict(model, x, prefix_index):
     j = model["prefixes"][prefix_index]
     xs = (np.asarray(x, dtype=np.float64) - model["centre"]) / model["scale"]
     return model["ymean"] + (xs @ model["R"][:, :j]) @ model["W"][prefix_index]
+
+
+# --------------------------------------------------------------------------
+# OPLS and kernel PLS
+# --------------------------------------------------------------------------
+def opls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1, north=1):
+    """OPLS filters + SIMPLS (opls.hpp:120-290, oplspls.hpp:30-74).
+
+    Each filter on the standardised Xf: w = unit dominant left singular
+    vector of Xf^T Yc; t = Xf w; p = Xf^T t / t't; w_o = normalise(p -
+    (w'p / w'w) w); t_o = Xf w_o; p_o = Xf^T t_o / t_o't_o; Xf -= t_o p_o^T.
+    The predictive SIMPLS runs on the filtered Xf (no further scaling).
+    Returns the SIMPLS dict plus Wo, Po and R_eff (weights acting on the
+    standardised, unfiltered predictors).
+    """
+    xs, _, centre, scale, ymean, yd = _prepare(x, y, labels, classes, scaling)
+    yc = yd - ymean
+    xf = xs.copy()
+    p = xf.shape[1]
+    Wo, Po = [], []
+    for _ in range(int(north)):
+        w = _dominant_left(xf.T @ yc)
+        w = w / np.linalg.norm(w)
+        t = xf @ w
+        pl = xf.T @ t / (t @ t)
+        wo = pl - (w @ pl) / (w @ w) * w
+        wo = wo / np.linalg.norm(wo)
+        to = xf @ wo
+        po = xf.T @ to / (to @ to)
+        xf = xf - np.outer(to, po)
+        Wo.append(wo)
+        Po.append(po)
+    inner = simpls_fit(xf, yd, ncomp=ncomp, scaling=3)
+    R = inner["R"].copy()
+    for wo, po in zip(reversed(Wo), reversed(Po)):
+        R = R - np.outer(wo, R.T @ po)
+    inner.update(R_eff=R, Wo=Wo, Po=Po, centre=centre, scale=scale)
+    return inner
+
+
+def opls_predict(model, x, prefix):
+    xs = (np.asarray(x, dtype=np.float64) - model["centre"]) / model["scale"]
+    return model["ymean"] + (xs @ model["R_eff"][:, :prefix]) @ model["Q"][:, :prefix].T
+
+
+def _kernel(a, b, kind, gamma, degree, coef0):
+    dots = a @ b.T
+    if kind == 2:  # RBF (kernels.hpp:41-55)
+        na = (a * a).sum(axis=1)[:, None]
+        nb = (b * b).sum(axis=1)[None, :]
+        d = np.maximum(na + nb - 2.0 * dots, 0.0)
+        return np.exp(-gamma * d)
+    return (gamma * dots + coef0) ** degree  # polynomial (kernels.hpp:29-35)
+
+
+def kernelpls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1,
+                  kind=2, gamma=1.0, degree=3, coef0=1.0):
+    """Kernel PLS (kernelpls.hpp:85-196): K = phi(Xs Xs^T) double-centred
+    with its column means and grand mean, then SIMPLS on K."""
+    xs, _, centre, scale, ymean, yd = _prepare(x, y, labels, classes, scaling)
+    K = _kernel(xs, xs, kind, gamma, degree, coef0)
+    cm = K.mean(axis=0)
+    g = cm.mean()
+    Kc = K - cm[:, None] - cm[None, :] + g
+    inner = simpls_fit(Kc, yd, ncomp=ncomp, scaling=3)
+    inner.update(reference=xs, kcol=cm, kgrand=g, kind=kind, gamma=gamma,
+                 degree=degree, coef0=coef0, centre=centre, scale=scale)
+    return inner
+
+
+def kernelpls_predict(model, x, prefix):
+    xs = (np.asarray(x, dtype=np.float64) - model["centre"]) / model["scale"]
+    Kt = _kernel(xs, model["reference"], model["kind"], model["gamma"],
+                 model["degree"], model["coef0"])
+    Kt = Kt - Kt.mean(axis=1)[:, None] - model["kcol"][None, :] + model["kgrand"]
+    return model["ymean"] + (Kt @ model["R"][:, :prefix]) @ model["Q"][:, :prefix].T
 
 
 # --------------------------------------------------------------------------

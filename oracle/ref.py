@@ -208,3 +208,34 @@ def lda(train_scores, labels, classes, prefixes, test_scores):
         raise RuntimeError(err.value.decode())
     return (disc.reshape((k, int(classes), rows)).transpose(0, 2, 1),
             pred.reshape((k, rows)).T)
+
+
+def opls_predict(x, y, ncomp, north, scaling, xtest):
+    x, xt = _f(x), _f(xtest)
+    y = _f(y if np.ndim(y) == 2 else np.asarray(y)[:, None])
+    n, p = x.shape
+    m = y.shape[1]
+    out = np.zeros((xt.shape[0], m), order="F")
+    err = _err()
+    rc = lib().ref_opls_predict(_ptr(x), _ptr(y), n, p, m, int(ncomp), int(north),
+                                int(scaling), _ptr(xt), xt.shape[0], _ptr(out),
+                                err, C.c_size_t(512))
+    if rc:
+        raise RuntimeError(err.value.decode())
+    return out
+
+
+def kernelpls_predict(x, y, ncomp, scaling, kind, gamma, degree, coef0, xtest):
+    x, xt = _f(x), _f(xtest)
+    y = _f(y if np.ndim(y) == 2 else np.asarray(y)[:, None])
+    n, p = x.shape
+    m = y.shape[1]
+    out = np.zeros((xt.shape[0], m), order="F")
+    err = _err()
+    rc = lib().ref_kernelpls_predict(_ptr(x), _ptr(y), n, p, m, int(ncomp),
+                                     int(scaling), int(kind), C.c_double(gamma),
+                                     int(degree), C.c_double(coef0), _ptr(xt),
+                                     xt.shape[0], _ptr(out), err, C.c_size_t(512))
+    if rc:
+        raise RuntimeError(err.value.decode())
+    return out

@@ -460,6 +460,63 @@ int ref_cv_classification(const double* x, const int* labels, const int* folds,
   }
 }
 
+// OPLS + SIMPLS (oplspls.hpp:30-74 fit, 86-101 predict) with the exact
+// leading-direction filter (opls.hpp:57-115, randomized_filter = false).
+// predictions: rows x m for `ncomp` components of the predictive model.
+int ref_opls_predict(const double* x, const double* y, int n, int p, int m,
+                     int ncomp, int north, int scaling, const double* xtest,
+                     int rows, double* predictions, char* error,
+                     std::size_t capacity) {
+  put_error(error, capacity, "");
+  try {
+    BlasBackend backend;
+    fastpls::core::OplsControls c;
+    c.orthogonal_components = std::size_t(north);
+    c.scaling = static_cast<fastpls::core::PredictorScaling>(scaling);
+    c.randomized_filter = false;
+    c.simpls = simpls_controls(n, p, m, std::size_t(ncomp), false, 32, 5, 1);
+    Matrix<double> responses = load(y, n, m);
+    auto model = fastpls::core::fit_opls<double>(
+        load(x, n, p), ConstMatrixView<double>(responses.view()), c, backend);
+    auto pred = fastpls::core::predict_opls<double>(model, load(xtest, rows, p),
+                                                    std::size_t(ncomp), backend);
+    store(pred, predictions);
+    return 0;
+  } catch (const std::exception& e) {
+    put_error(error, capacity, e.what());
+    return 1;
+  }
+}
+
+// Kernel PLS (kernelpls.hpp:85-196): kind 2 = RBF, 3 = polynomial.
+int ref_kernelpls_predict(const double* x, const double* y, int n, int p,
+                          int m, int ncomp, int scaling, int kind,
+                          double gamma, int degree, double coef0,
+                          const double* xtest, int rows, double* predictions,
+                          char* error, std::size_t capacity) {
+  put_error(error, capacity, "");
+  try {
+    BlasBackend backend;
+    fastpls::core::KernelPlsControls c;
+    c.kernel = static_cast<fastpls::core::KernelType>(kind);
+    c.gamma = gamma;
+    c.degree = degree;
+    c.offset = coef0;
+    c.scaling = static_cast<fastpls::core::PredictorScaling>(scaling);
+    c.simpls = simpls_controls(n, n, m, std::size_t(ncomp), false, 32, 5, 1);
+    Matrix<double> responses = load(y, n, m);
+    auto model = fastpls::core::fit_kernelpls<double>(
+        load(x, n, p), ConstMatrixView<double>(responses.view()), c, backend);
+    auto pred = fastpls::core::predict_kernelpls<double>(model, load(xtest, rows, p),
+                                                         std::size_t(ncomp), backend);
+    store(pred, predictions);
+    return 0;
+  } catch (const std::exception& e) {
+    put_error(error, capacity, e.what());
+    return 1;
+  }
+}
+
 // LDA on latent scores (lda.hpp:156-223 train, 284-318 predict).
 // discriminants (optional): prefix_count blocks of rows x classes;
 // predicted: rows x prefix_count one-based labels.

@@ -58,6 +58,15 @@ def main():
         save(f"cv_cls_h{head}", x=xc, labels=lab, folds=f2,
              prefixes=np.array([1, 2, 3]), metrics=out["metrics"],
              predictions=out["predictions"])
+    # OPLS (exact filter) and kernel PLS predictions
+    xt, _ = W.latent_regression(30, 60, 3, 4, 0.5, 106, dtype=np.float64)
+    for north in (1, 2):
+        pred = ref.opls_predict(x, y, 4, north, 2, xt)
+        save(f"opls_n{north}", x=x, y=y, xtest=xt, pred=pred)
+    for kind, gamma, degree in ((2, 0.02, 3), (3, 0.01, 2)):
+        pred = ref.kernelpls_predict(x, y, 5, 1, kind, gamma, degree, 1.0, xt)
+        save(f"kernelpls_k{kind}", x=x, y=y, xtest=xt, pred=pred,
+             gamma=np.array(gamma), degree=np.array(degree))
     # LDA on scores
     ts = W.rng(105, 0).standard_normal((60, 4))
     lab3 = (np.arange(60) % 3 + 1).astype(np.int32)

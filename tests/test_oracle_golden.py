@@ -70,3 +70,18 @@ def test_lda_golden():
         d = O.lda_discriminants(models[j], f["test"])
         assert O.rel_err(d, f["disc"][j]) < 1e-12
         assert np.array_equal(O.row_argmax(d), f["pred"][:, j])
+
+
+@pytest.mark.parametrize("north", [1, 2])
+def test_opls_golden(north):
+    f = load(f"opls_n{north}")
+    m = O.opls_fit(f["x"], f["y"], ncomp=4, scaling=2, north=north)
+    assert O.rel_err(O.opls_predict(m, f["xtest"], 4), f["pred"]) < 1e-9
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_kernelpls_golden(kind):
+    f = load(f"kernelpls_k{kind}")
+    m = O.kernelpls_fit(f["x"], f["y"], ncomp=5, scaling=1, kind=kind,
+                        gamma=float(f["gamma"]), degree=int(f["degree"]), coef0=1.0)
+    assert O.rel_err(O.kernelpls_predict(m, f["xtest"], 5), f["pred"]) < 1e-10
