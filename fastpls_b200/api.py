@@ -66,6 +66,7 @@ class ResidentModel:
     method: str
     classification: bool
     levels: np.ndarray | None = None
+    feature_p: int = 0          # rows of R (p; n for kernel PLS)
     _freed: bool = field(default=False, repr=False)
 
     @property
@@ -86,8 +87,9 @@ class ResidentModel:
     # ---- exports (fastpls_resident_export field ids) ----
     def export(self, field_id: int) -> np.ndarray:
         a, q, p, n = self.ncomp, self.q, self.p, self.n
-        shapes = {0: (p, a), 1: (q, a), 2: (n, a), 3: (p,), 4: (p,), 5: (q,),
-                  6: (p, a), 7: (a + 1,)}
+        fp = self.feature_p or p
+        shapes = {0: (fp, a), 1: (q, a), 2: (n, a), 3: (p,), 4: (p,), 5: (q,),
+                  6: (fp, a), 7: (a + 1,)}
         shape = shapes[field_id]
         out = np.zeros(shape, dtype=self.dtype, order="F")
         err, cap = _lib.error_buffer()
@@ -216,9 +218,9 @@ def fit_resident(X, Y=None, labels=None, classes=None, ncomp=2,
     if not h:
         raise _lib.FastplsError(err.value.decode(errors="replace"))
     feature_p = n if method == "kernelpls" else p
-    return ResidentModel(handle=h, precision=precision, n=n, p=feature_p, q=q,
+    return ResidentModel(handle=h, precision=precision, n=n, p=p, q=q,
                          ncomp=int(ncomp), method=method,
-                         classification=labels is not None)
+                         classification=labels is not None, feature_p=feature_p)
 
 
 def cuda_gemm(left, right, precision=64):
