@@ -55,6 +55,8 @@ SIGNATURES = {
     "fastpls_b200_device_count": (_i, []),
     "fastpls_b200_launch_count": (_ull, []),
     "fastpls_b200_set_stream": (None, [_vp]),
+    "fastpls_b200_fastcor": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _cp, _sz]),
+    "fastpls_b200_fastsvd": (_i, [_vp, _i, _i, _i, _i, _i, _i, _ull, _vp, _vp, _vp, _cp, _sz]),
     "fastpls_b200_crossprod_noalloc": (
         _i, [_vp, _i, _i, _i, C.c_long, _vp, C.c_long, _i, _vp, C.c_long, _vp, _cp, _sz]),
     "fastpls_b200_fp64_peak": (_i, [_dp, _cp, _sz]),

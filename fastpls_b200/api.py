@@ -334,3 +334,41 @@ def cv_permutation(X, Y, folds, permutations, prefixes, scaling="centering",
     return dict(metrics=metrics.reshape(shape), q2=q2.reshape(shape),
                 rmsd=rmsd.reshape(shape), observed_r2=r2.reshape(shape),
                 status=status)
+
+
+def fastcor(a, b=None, byrow=True, diag=True, precision=64):
+    """Pearson correlations between the rows (byrow) or columns of a and b
+    (fastcor(), R/main.R:12799). Without b the full a-by-a matrix."""
+    dt = _dtype(precision)
+    A = _mat(a, dt)
+    B = None if b is None else _mat(b, dt)
+    ua = A.shape[0] if byrow else A.shape[1]
+    if B is None:
+        out = np.zeros((ua, ua), order="F")
+    else:
+        ub = B.shape[0] if byrow else B.shape[1]
+        out = np.zeros(ua) if (diag and ua == ub) else np.zeros((ua, ub), order="F")
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_b200_fastcor(
+        _p(A), _p(B), precision, A.shape[0], A.shape[1],
+        0 if B is None else B.shape[0], 0 if B is None else B.shape[1],
+        int(byrow), int(diag), _p(out), err, cap)
+    _lib.check(rc, err)
+    return out
+
+
+def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64):
+    """Truncated SVD on the device (fastsvd(backend = "cuda")): u, d, v."""
+    dt = _dtype(precision)
+    X = _mat(x, dt)
+    n, p = X.shape
+    k = int(ncomp)
+    u = np.zeros((n, k), order="F")
+    v = np.zeros((p, k), order="F")
+    d = np.zeros(k)
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_b200_fastsvd(_p(X), precision, n, p, k, int(oversample),
+                                          int(power), C.c_ulonglong(seed), _p(u), _p(d),
+                                          _p(v), err, cap)
+    _lib.check(rc, err)
+    return u, d, v

@@ -220,6 +220,30 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_device(
     int metric, double* metrics, double* q2, double* rmsd,
     double* observed_r2, int* status, char* error, size_t error_capacity);
 
+/* Pearson correlations (fastcor(), R/main.R:12799; src/r_api.cpp:4054-4166):
+ * units are the rows of a (byrow = 1) or its columns; each unit is centred
+ * and scaled to unit norm in FP64 (NaN when it holds a non-finite value or
+ * has zero spread). Without b: out = units_a x units_a matrix. With b:
+ * units_a x units_b, or (diag = 1, matching unit counts) the units_a paired
+ * correlations. a, b, out are host memory; out is FP64. */
+FASTPLS_B200_API int fastpls_b200_fastcor(const void* a, const void* b, int precision,
+                                          int rows_a, int cols_a, int rows_b,
+                                          int cols_b, int byrow, int diag,
+                                          double* out, char* error,
+                                          size_t error_capacity);
+
+/* Truncated SVD of x (n x p) by FP64 randomized subspace iteration on the
+ * device (fastsvd(backend = "cuda"); the reference's CUDA route errors,
+ * R/main.R:7932-7943): sketch width min(k + oversample, min(n, p)) <= 256,
+ * `power` power iterations, Gaussian sketch from `seed`. Outputs (host, FP64):
+ * u n x k (may be NULL), d k, v p x k (may be NULL); singular values are in
+ * decreasing order, each (u, v) pair sign-normalised. */
+FASTPLS_B200_API int fastpls_b200_fastsvd(const void* x, int precision, int n, int p,
+                                          int k, int oversample, int power,
+                                          unsigned long long seed, double* u,
+                                          double* d, double* v, char* error,
+                                          size_t error_capacity);
+
 /* out (p x nb, FP64) = X^T V for device-resident X (n x p, leading
  * dimension ldx, FP32 or FP64 by `precision`), V (n x nb FP64, ldv) and out
  * (ldo), without any memory allocation by the library: for callers whose

@@ -36,6 +36,7 @@ __all__ = [
     "row_argmax", "topk", "response_sums", "cv_regression", "opls_fit",
     "opls_predict", "kernelpls_fit", "kernelpls_predict",
     "cv_classification", "permutation_pvalue", "align_signs", "rel_err",
+    "fastcor",
 ]
 
 
@@ -522,6 +523,29 @@ def cv_classification(x, labels, classes, folds, prefixes, scaling=1, family=3,
         status[f] = 1
     metrics = np.where(total > 0, correct / np.maximum(total, 1), np.nan)
     return dict(metrics=metrics, status=status, predictions=preds)
+
+
+def fastcor(a, b=None, byrow=True, diag=True):
+    """Pearson correlations (fastcor_values / normalized_units,
+    src/r_api.cpp:4054-4166): each unit (row when byrow) centred and scaled
+    to unit norm, NaN when non-finite or of zero spread; L R^T, or paired
+    dot products when diag (only with b and matching unit counts)."""
+    def units(x):
+        x = np.asarray(x, dtype=np.float64)
+        u = x if byrow else x.T
+        mean = u.mean(axis=1, keepdims=True)
+        c = u - mean
+        norm = np.sqrt((c * c).sum(axis=1, keepdims=True))
+        ok = np.all(np.isfinite(u), axis=1, keepdims=True) & (norm > 0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.where(ok, c / norm, np.nan)
+    L = units(a)
+    if b is None:
+        return L @ L.T
+    R = units(b)
+    if diag and L.shape[0] == R.shape[0]:
+        return (L * R).sum(axis=1)
+    return L @ R.T
 
 
 def permutation_pvalue(permuted, observed, lower_tail=False):
