@@ -55,6 +55,17 @@ SIGNATURES = {
     "fastpls_b200_device_count": (_i, []),
     "fastpls_b200_launch_count": (_ull, []),
     "fastpls_b200_set_stream": (None, [_vp]),
+    "fastpls_b200_server_create": (_vp, [_sz, _i, _cp, _sz]),
+    "fastpls_b200_server_destroy": (None, [_vp]),
+    "fastpls_b200_server_submit_fit": (
+        _i, [_vp, _i, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _d, _i, _d,
+             C.POINTER(C.c_ulonglong), _cp, _sz]),
+    "fastpls_b200_server_submit_predict": (
+        _i, [_vp, _ull, _vp, _i, _i, _i, _vp, _i, _i, C.POINTER(C.c_ulonglong), _cp, _sz]),
+    "fastpls_b200_server_wait": (_i, [_vp, _ull, _d, _vp, _sz, _dp, _dp, _cp, _sz]),
+    "fastpls_b200_server_release": (_i, [_vp, _ull, _cp, _sz]),
+    "fastpls_b200_server_stats": (_i, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                       C.POINTER(C.c_size_t)]),
     "fastpls_b200_fastcor": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _cp, _sz]),
     "fastpls_b200_fastsvd": (_i, [_vp, _i, _i, _i, _i, _i, _i, _ull, _vp, _vp, _vp, _cp, _sz]),
     "fastpls_b200_crossprod_noalloc": (

@@ -372,3 +372,97 @@ def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64):
                                           _p(v), err, cap)
     _lib.check(rc, err)
     return u, d, v
+
+
+class Server:
+    """Serving loop on the device (fastpls_b200_server_*): continuous
+    admission of fit and predict requests by HBM footprint, resident models,
+    merged predictions per model. Fit tickets double as model ids."""
+
+    def __init__(self, budget_bytes=150 * 10**9, workers=4):
+        err, cap = _lib.error_buffer()
+        self._lib = _lib.load()
+        self._h = self._lib.fastpls_b200_server_create(int(budget_bytes), int(workers), err, cap)
+        if not self._h:
+            raise _lib.FastplsError(err.value.decode())
+        self._models = {}
+        self._pending = {}
+
+    def submit_fit(self, X, Y=None, labels=None, classes=None, ncomp=2,
+                   method="simpls", scaling="centering", precision=32, north=1,
+                   kernel="rbf", gamma=None, degree=3, coef0=1.0):
+        dt = _dtype(precision)
+        x = _mat(X, dt)
+        n, p = x.shape
+        if labels is not None:
+            lab = np.ascontiguousarray(labels, dtype=np.int32)
+            q = int(classes if classes is not None else lab.max())
+            y = None
+        else:
+            y = _mat(Y, dt)
+            q = y.shape[1]
+            lab = None
+        g = float(gamma) if gamma is not None else 1.0 / p
+        t = C.c_ulonglong(0)
+        err, cap = _lib.error_buffer()
+        rc = self._lib.fastpls_b200_server_submit_fit(
+            self._h, METHODS[method], _p(x), _p(y), _p(lab), precision, n, p, q,
+            int(ncomp), SCALING[scaling] if isinstance(scaling, str) else int(scaling),
+            int(north), KERNELS.get(kernel, 2), g, int(degree), float(coef0),
+            C.byref(t), err, cap)
+        _lib.check(rc, err)
+        self._models[t.value] = (q, precision, p)
+        return t.value
+
+    def submit_predict(self, model, X, prefixes, lda=False):
+        q, precision, p = self._models[model]
+        x = _mat(X, _dtype(precision))
+        pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+        t = C.c_ulonglong(0)
+        err, cap = _lib.error_buffer()
+        rc = self._lib.fastpls_b200_server_submit_predict(
+            self._h, C.c_ulonglong(model), _p(x), x.shape[0], x.shape[1], precision,
+            _p(pre), len(pre), int(lda), C.byref(t), err, cap)
+        _lib.check(rc, err)
+        self._pending[t.value] = (x.shape[0], q, len(pre), precision)
+        return t.value
+
+    def wait(self, ticket, timeout=600.0):
+        """(result, queue_ms, service_ms); result is the prediction array
+        (prefixes x rows x q) for predict tickets, the model id for fits."""
+        qms, sms = C.c_double(0), C.c_double(0)
+        err, cap = _lib.error_buffer()
+        if ticket in self._pending:
+            rows, q, k, precision = self._pending.pop(ticket)
+            out = np.zeros(rows * q * k, dtype=_dtype(precision))
+            rc = self._lib.fastpls_b200_server_wait(
+                self._h, C.c_ulonglong(ticket), float(timeout), _p(out), out.nbytes,
+                C.byref(qms), C.byref(sms), err, cap)
+            _lib.check(rc, err)
+            return out.reshape((k, q, rows)).transpose(0, 2, 1), qms.value, sms.value
+        rc = self._lib.fastpls_b200_server_wait(
+            self._h, C.c_ulonglong(ticket), float(timeout), None, 0,
+            C.byref(qms), C.byref(sms), err, cap)
+        _lib.check(rc, err)
+        return ticket, qms.value, sms.value
+
+    def release(self, model):
+        err, cap = _lib.error_buffer()
+        _lib.check(self._lib.fastpls_b200_server_release(self._h, C.c_ulonglong(model), err, cap), err)
+        self._models.pop(model, None)
+
+    def stats(self):
+        a, b, c = C.c_size_t(0), C.c_size_t(0), C.c_size_t(0)
+        self._lib.fastpls_b200_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c))
+        return dict(bytes_in_use=a.value, queued=b.value, resident_models=c.value)
+
+    def close(self):
+        if self._h:
+            self._lib.fastpls_b200_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

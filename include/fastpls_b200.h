@@ -244,6 +244,41 @@ FASTPLS_B200_API int fastpls_b200_fastsvd(const void* x, int precision, int n, i
                                           double* d, double* v, char* error,
                                           size_t error_capacity);
 
+/* ---- serving loop (no counterpart in the reference) ---------------------
+ * A server owns `workers` threads, each driving resident handles on its own
+ * CUDA stream, and admits queued requests by their HBM footprint against
+ * `budget_bytes` (oldest admissible first, so requests arriving while others
+ * run start as soon as memory and a worker free up). Fit requests return a
+ * ticket that is also the model id; the model stays resident (training
+ * predictors released) until fastpls_b200_server_release. Predictions queued
+ * against one model are merged into one projection. Inputs are copied at
+ * submission. Results are deterministic: identical alone or in a mix. */
+FASTPLS_B200_API void* fastpls_b200_server_create(size_t budget_bytes, int workers,
+                                                  char* error, size_t error_capacity);
+FASTPLS_B200_API void fastpls_b200_server_destroy(void* server);
+/* method: 1 PLS-SVD, 3 SIMPLS, 4 OPLS (north), 5 kernel PLS (kernel, gamma,
+ * degree, coef0); y (n x q) or one-based labels (q classes). */
+FASTPLS_B200_API int fastpls_b200_server_submit_fit(
+    void* server, int method, const void* x, const void* y, const int* labels,
+    int precision, int n, int p, int q, int components, int scaling, int north,
+    int kernel, double gamma, int degree, double coef0,
+    unsigned long long* ticket, char* error, size_t error_capacity);
+FASTPLS_B200_API int fastpls_b200_server_submit_predict(
+    void* server, unsigned long long model, const void* x, int rows, int p,
+    int precision, const int* prefixes, int prefix_count, int lda,
+    unsigned long long* ticket, char* error, size_t error_capacity);
+/* Blocks (at most timeout_seconds) until the request completes; predictions
+ * are written to out (rows x q per prefix, request precision). queue_ms and
+ * service_ms: submission-to-start and start-to-finish times. */
+FASTPLS_B200_API int fastpls_b200_server_wait(
+    void* server, unsigned long long ticket, double timeout_seconds, void* out,
+    size_t capacity_bytes, double* queue_ms, double* service_ms, char* error,
+    size_t error_capacity);
+FASTPLS_B200_API int fastpls_b200_server_release(void* server, unsigned long long model,
+                                                 char* error, size_t error_capacity);
+FASTPLS_B200_API int fastpls_b200_server_stats(void* server, size_t* bytes_in_use,
+                                               size_t* queued, size_t* resident_models);
+
 /* out (p x nb, FP64) = X^T V for device-resident X (n x p, leading
  * dimension ldx, FP32 or FP64 by `precision`), V (n x nb FP64, ldv) and out
  * (ldo), without any memory allocation by the library: for callers whose
