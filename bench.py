@@ -46,6 +46,8 @@ def args_parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--perms", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--served-requests", type=int, default=120,
+                    help="requests in the served mixed-workload leg (0 = skip)")
     ap.add_argument("--plain-perms", type=int, default=3,
                     help="permutations sampled for the one-fit-at-a-time path")
     return ap.parse_args()
@@ -176,6 +178,126 @@ def run_reference_arm(a):
     return 0
 
 
+def served_workload(count, seed=11):
+    """Mixed request stream (scaled-down served configuration): n log-uniform
+    in [200, 3000], p log-uniform in [500, 4000], m in 1..10, ncomp in 2..30;
+    SIMPLS 50%, PLS-SVD 20%, OPLS 15%, kernel PLS (RBF) 15%; 30%
+    classification (2-20 classes); 70% fits, 30% predictions against the
+    models fitted so far. Inputs are seeded per request id."""
+    from fastpls_b200 import workloads as W
+    g = np.random.default_rng(seed)
+    reqs = []
+    fitted = []
+    for rid in range(count):
+        if fitted and g.random() < 0.3:
+            src = fitted[int(g.integers(len(fitted)))]
+            rows = int(g.integers(50, 500))
+            xt, _ = W.latent_regression(rows, src["p"], 1, 3, 0.4, 5000 + rid)
+            reqs.append(dict(kind="predict", src=src, x=xt))
+            continue
+        n = int(np.exp(g.uniform(np.log(200), np.log(3000))))
+        p = int(np.exp(g.uniform(np.log(500), np.log(4000))))
+        m = int(g.integers(1, 11))
+        method = g.choice(["simpls", "plssvd", "opls", "kernelpls"], p=[0.5, 0.2, 0.15, 0.15])
+        cls = g.random() < 0.3
+        if cls:
+            m = int(g.integers(2, 21))
+            x, lab = W.latent_classification(n, p, m, 5, 0.4, rid)
+            # factor levels present only (R drops empty levels)
+            present, lab = np.unique(lab, return_inverse=True)
+            lab = (lab + 1).astype(np.int32)
+            m = int(present.size)
+            if m < 2:
+                continue
+            y = None
+        else:
+            x, y = W.latent_regression(n, p, m, 5, 0.4, rid)
+            lab = None
+        cap = min(n - 1, p) if method != "kernelpls" else n - 1
+        a = int(min(int(g.integers(2, 31)), cap))
+        if method == "plssvd":
+            a = max(1, min(a, m - 1 if cls else m))
+            if cls and a < 1:
+                continue
+        r = dict(kind="fit", method=str(method), x=x, y=y, labels=lab,
+                 classes=m if cls else None, ncomp=a, p=p, q=m)
+        reqs.append(r)
+        fitted.append(r)
+    return reqs
+
+
+def _kw(r):
+    return dict(kernel="rbf", gamma=1.0 / r["p"]) if r["method"] == "kernelpls" else {}
+
+
+def run_plain(lib_api, reqs):
+    """Each request through the drop-in entry points, one at a time."""
+    kw = _kw
+    models = {}
+    plain_lat = []
+    t0 = time.perf_counter()
+    for i, r in enumerate(reqs):
+        s = time.perf_counter()
+        if r["kind"] == "fit":
+            models[id(r)] = lib_api.fit_resident(
+                r["x"], r["y"], labels=r["labels"], classes=r["classes"],
+                ncomp=r["ncomp"], method=r["method"], precision=32, **kw(r))
+        else:
+            src = r["src"]
+            models[id(src)].predict_path(r["x"], [src["ncomp"]])
+        plain_lat.append(1000 * (time.perf_counter() - s))
+    plain_time = time.perf_counter() - t0
+    for mdl in models.values():
+        mdl.close()
+    fits = sum(1 for r in reqs if r["kind"] == "fit")
+    return {"plain_fits_per_s": fits / plain_time,
+            "plain_p50_ms": float(np.percentile(plain_lat, 50)),
+            "plain_p99_ms": float(np.percentile(plain_lat, 99))}
+
+
+def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
+    """Served (continuous batching): Poisson arrivals into the server."""
+    kw = _kw
+    g = np.random.default_rng(3)
+    gaps = g.exponential(mean_gap_ms / 1000.0, size=len(reqs))
+    srv = lib_api.Server(budget_bytes=150 * 10**9, workers=workers)
+    tickets = []
+    fit_tickets = {}
+    waited = {}
+    submit_t = []
+    t0 = time.perf_counter()
+    next_t = t0
+    for i, r in enumerate(reqs):
+        next_t += gaps[i]
+        delay = next_t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        if r["kind"] == "fit":
+            t = srv.submit_fit(r["x"], r["y"], labels=r["labels"], classes=r["classes"],
+                               ncomp=r["ncomp"], method=r["method"], precision=32, **kw(r))
+            fit_tickets[id(r)] = t
+        else:
+            src = r["src"]
+            ft = fit_tickets[id(src)]
+            if ft not in waited:  # a prediction needs its model: wait for that fit
+                waited[ft] = srv.wait(ft)
+            t = srv.submit_predict(ft, r["x"], [src["ncomp"]])
+        tickets.append(t)
+        submit_t.append(time.perf_counter())
+    lat = []
+    for t in tickets:
+        _, qms, sms = waited[t] if t in waited else srv.wait(t)
+        lat.append(qms + sms)
+    served_time = time.perf_counter() - t0
+    for t in fit_tickets.values():
+        srv.release(t)
+    srv.close()
+    fits = sum(1 for r in reqs if r["kind"] == "fit")
+    return {"mean_gap_ms": mean_gap_ms, "fits_per_s": fits / served_time,
+            "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99))}
+
+
 def workload_config(perms):
     return {"workload": f"cv{FOLDS}_perm{perms}_ncomp{NCOMP}_{N}x{P}_f32",
             "n": N, "p": P, "q": Q, "folds": FOLDS, "fold_sizes": "480-520",
@@ -262,11 +384,11 @@ def main():
     _lib.check(lib.fastpls_b200_fp64_peak(C.byref(pk), err, cap), err)
     fp64_peak = pk.value
 
+    clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
+    clk = clock_sampler_start(clk_path)
     for _ in range(max(a.warmup, 3)):
         step_device()
     barrier()
-    clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
-    clk = clock_sampler_start(clk_path)
     launches0 = lib.fastpls_b200_launch_count()
     lib.fastpls_b200_profile_gemm(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
@@ -368,6 +490,17 @@ def main():
         if plain else None,
         "clocks": clocks,
     }
+    if rank == 0 and a.served_requests > 0:
+        from fastpls_b200 import api as fapi
+        reqs = served_workload(a.served_requests)
+        run_served(fapi, reqs[:20], mean_gap_ms=0.0)  # warm-up
+        plain = run_plain(fapi, reqs)
+        sweep = [run_served(fapi, reqs, mean_gap_ms=g_) for g_ in (2.0, 0.5, 0.0)]
+        line["served"] = dict(
+            requests=len(reqs), fits=sum(1 for r in reqs if r["kind"] == "fit"),
+            workers=4, arrivals="Poisson; mean gap swept (0 = all at once)",
+            sweep=sweep, **plain,
+            saturated_served_over_plain=sweep[-1]["fits_per_s"] / plain["plain_fits_per_s"])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu, ref_out = cpu_reference_sample(x, y, folds, prefixes)
         line["cpu_baseline"] = cpu
