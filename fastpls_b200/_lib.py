@@ -73,6 +73,12 @@ SIGNATURES = {
     "fastpls_b200_fp64_peak": (_i, [_dp, _cp, _sz]),
     "fastpls_b200_profile_gemm": (None, [_i]),
     "fastpls_b200_profile_gemm_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
+    "fastpls_b200_set_product_digits": (None, [_i]),
+    "fastpls_b200_product_digits": (_i, []),
+    "fastpls_b200_profile_int8": (None, [_i]),
+    "fastpls_b200_profile_int8_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
+    "fastpls_b200_int8_crossprod": (
+        _i, [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _vp, _i, _cp, _sz]),
     "fastpls_b200_simpls_cv_permutation": (
         _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp,
              _vp, _vp, _vp, _cp, _sz]),

@@ -303,11 +303,50 @@ def cv_classification(X, labels, classes, folds, prefixes, scaling="centering",
     return out
 
 
+def set_product_digits(digits: int) -> None:
+    """int8 digits per FP64 value in the batched engine's products with the
+    shared Gram (0 = FP64 DMMA GEMMs); process-wide."""
+    _lib.load().fastpls_b200_set_product_digits(int(digits))
+
+
+def product_digits() -> int:
+    return int(_lib.load().fastpls_b200_product_digits())
+
+
+def int8_crossprod(a, b=None, digits=6):
+    """a^T b (b = None: a^T a, symmetric) by the int8 split product on the
+    tensor cores; a is k x m, b is k x n (FP64)."""
+    A = _mat(a, np.float64)
+    sym = b is None
+    B = A if sym else _mat(b, np.float64)
+    if A.shape[0] != B.shape[0]:
+        raise ValueError("a and b need the same number of rows")
+    k, m = A.shape
+    n = B.shape[1]
+    out = np.zeros((m, n), order="F")
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_b200_int8_crossprod(
+        _p(A), max(k, 1), _p(B), max(k, 1), m, n, k, int(digits), 1 if sym else 0,
+        _p(out), m, err, cap)
+    _lib.check(rc, err)
+    return out
+
+
 def cv_permutation(X, Y, folds, permutations, prefixes, scaling="centering",
-                   metric="q2", precision=32):
+                   metric="q2", precision=32, digits=None):
     """Batched CV over the observed responses and their row permutations
     (``fastpls_b200_simpls_cv_permutation``). Returns arrays of shape
-    (permutations + 1, prefixes), row 0 the observed responses."""
+    (permutations + 1, prefixes), row 0 the observed responses. digits
+    selects the product precision for this call (None: the process setting,
+    see set_product_digits)."""
+    if digits is not None:
+        old = product_digits()
+        set_product_digits(digits)
+        try:
+            return cv_permutation(X, Y, folds, permutations, prefixes, scaling,
+                                  metric, precision, None)
+        finally:
+            set_product_digits(old)
     dt = _dtype(precision)
     x = _mat(X, dt)
     y = _mat(Y, dt)

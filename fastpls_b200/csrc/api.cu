@@ -8,6 +8,7 @@
 #include "../../include/fastpls_b200.h"
 
 #include "batched.cuh"
+#include "ozaki.cuh"
 #include "cv.cuh"
 #include "handle.cuh"
 
@@ -488,6 +489,66 @@ int fastpls_b200_fp64_peak(double* tflops, char* error, size_t error_capacity) {
 void fastpls_b200_profile_gemm_read(double* milliseconds, double* flops,
                                     unsigned long long* launches) {
   gemm_profile_read(milliseconds, flops, launches);
+}
+
+void fastpls_b200_set_product_digits(int digits) {
+  ozaki_slices() = std::max(0, std::min(digits, kOzakiMaxSlices));
+}
+
+int fastpls_b200_product_digits(void) { return ozaki_slices(); }
+
+void fastpls_b200_profile_int8(int enable) { ozaki_profile_enable(enable != 0); }
+
+void fastpls_b200_profile_int8_read(double* milliseconds, double* int8_ops,
+                                    unsigned long long* launches) {
+  ozaki_profile_read(milliseconds, int8_ops, launches);
+}
+
+int fastpls_b200_int8_crossprod(const double* a, int lda, const double* b, int ldb, int m,
+                                int n, int k, int digits, int symmetric, double* c, int ldc,
+                                char* error, size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown int8 split product error", [&] {
+    if (!a || !b || !c || m < 1 || n < 1 || k < 0 || lda < std::max(k, 1) ||
+        ldb < std::max(k, 1) || ldc < m || digits < 1 || digits > kOzakiMaxSlices)
+      throw std::invalid_argument("invalid int8 split product input");
+    if (symmetric && (a != b || m != n || lda != ldb))
+      throw std::invalid_argument("symmetric int8 split product needs one operand");
+    if (k == 0) {
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) c[i + (size_t)j * ldc] = 0.0;
+      return;
+    }
+    cudaStream_t s = nullptr;
+    FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct Guard {
+      cudaStream_t s;
+      ~Guard() {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    } guard{s};
+    DeviceArray<double> da((size_t)lda * m, s), db, dc((size_t)m * n, s);
+    DeviceArray<int> flag(1, s);
+    flag.zero(s);
+    FPLS_CHECK(cudaMemcpyAsync(da.get(), a, sizeof(double) * lda * m, cudaMemcpyHostToDevice, s));
+    OzakiOperand oa, ob;
+    ozaki_split_rows(da.get(), lda, m, k, digits, oa, flag.get(), s);
+    if (symmetric) {
+      ozaki_gemm(oa, oa, dc.get(), m, true, flag.get(), s);
+    } else {
+      db.allocate((size_t)ldb * n, s);
+      FPLS_CHECK(cudaMemcpyAsync(db.get(), b, sizeof(double) * ldb * n, cudaMemcpyHostToDevice, s));
+      ozaki_split_rows(db.get(), ldb, n, k, digits, ob, flag.get(), s);
+      ozaki_gemm(oa, ob, dc.get(), m, false, flag.get(), s);
+    }
+    int bad = 0;
+    FPLS_CHECK(cudaMemcpyAsync(&bad, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    FPLS_CHECK(cudaMemcpy2DAsync(c, sizeof(double) * ldc, dc.get(), sizeof(double) * m,
+                                 sizeof(double) * m, n, cudaMemcpyDeviceToHost, s));
+    FPLS_CHECK(cudaStreamSynchronize(s));
+    if (bad == 4) throw std::runtime_error("int8 split product: tensor-core pipeline wait timed out");
+    if (bad) throw std::runtime_error("int8 split product: non-finite input");
+  });
 }
 
 int fastpls_b200_simpls_cv_permutation(

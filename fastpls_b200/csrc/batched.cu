@@ -413,9 +413,18 @@ __global__ void response_moments(const double* __restrict__ Y, int n, double* ou
 // ---------------------------------------------------------------------------
 template <class T>
 void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
+  gram.reserve((size_t)n * n, s);
+  if (digits > 0) {
+    // int8 digits of the rows of X D^1/2, the symmetric product on the int8
+    // tensor cores (lower tiles + mirror), then the digits of K's rows for
+    // every later product with K
+    ozaki_split_colmajor<T>(X, n, p, n, kscale, digits, x_split, flag.get(), s);
+    ozaki_gemm(x_split, x_split, gram.get(), n, true, flag.get(), s);
+    ozaki_split_rows(gram.get(), n, n, n, digits, gram_split, flag.get(), s);
+    return;
+  }
   // FP64 copy of X with the scaling folded in (X D^1/2), then the symmetric
   // product on the FP64 tensor-core path (lower tiles + mirror).
-  gram.reserve((size_t)n * n, s);
   x64.reserve((size_t)n * p, s);
   const long total = (long)n * p;
   scale_columns_f64<T><<<(unsigned)std::min<long>((total + 255) / 256, 16L * num_sms()), 256, 0, s>>>(
@@ -434,6 +443,27 @@ void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
   g.C = gram.get();
   g.ldc = n;
   g.lower = gemm_mma_supported(g);
+  gemm_f64(g, s);
+}
+
+template <class T>
+void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out, cudaStream_t s) {
+  if (digits > 0) {
+    // K is symmetric: its rows are its columns (contiguous, ld n)
+    ozaki_split_rows(rhs, n, cols, n, digits, rhs_split, flag.get(), s);
+    ozaki_gemm(gram_split, rhs_split, out, n, false, flag.get(), s);
+    return;
+  }
+  GemmArgs g;
+  g.M = n;
+  g.N = cols;
+  g.K = n;
+  g.A = gram.get();
+  g.lda = n;
+  g.B = rhs;
+  g.ldb = n;
+  g.C = out;
+  g.ldc = n;
   gemm_f64(g, s);
 }
 
@@ -473,18 +503,8 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
                                   yhat.get(), max_test, sse.get(), prefix_count);
   count_launch();
   FPLS_LAUNCH("init_instances");
-  // G0 = C0^T K C0 via one GEMM over all instances' C0 columns
-  GemmArgs g;
-  g.M = n;
-  g.N = q * I;
-  g.K = n;
-  g.A = gram.get();
-  g.lda = n;
-  g.B = C0.get();
-  g.ldb = n;
-  g.C = KC0.get();
-  g.ldc = n;
-  gemm_f64(g, s);
+  // G0 = C0^T K C0 via one product over all instances' C0 columns
+  gram_product(C0.get(), q * I, KC0.get(), s);
   initial_gram<<<I, BT, 0, s>>>(v, C0.get(), KC0.get(), G.get());
   count_launch();
   FPLS_LAUNCH("initial_gram");
@@ -496,24 +516,14 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   FPLS_LAUNCH("direction_batched");
   KC0.release();
   for (int a = 0; a < kmax; ++a) {
-    GemmArgs k1;
-    k1.M = n;
-    k1.N = I;
-    k1.K = n;
-    k1.A = gram.get();
-    k1.lda = n;
-    k1.B = U.get();
-    k1.ldb = n;
-    k1.C = Y1.get();
-    k1.ldc = n;
-    if (a > 0) gemm_f64(k1, s);  // Y1 = K u (a = 0: formed from K C0)
+    if (a > 0) gram_product(U.get(), I, Y1.get(), s);  // Y1 = K u (a = 0: from K C0)
     scores_batched<<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(),
                                     yhat.get(), max_test, a, d_slot.get(),
                                     prefix_count, sse.get(), nullptr, flag.get());
     count_launch();
     FPLS_LAUNCH("scores_batched");
     if (a + 1 == kmax) break;  // the last deflation is never used
-    gemm_f64(k1, s);  // Y1 = K t~ (U now holds the masked training scores)
+    gram_product(U.get(), I, Y1.get(), s);  // Y1 = K t~ (U holds the masked training scores)
     deflate_batched<<<I, BT, (kmax + q + 2 * q * q) * sizeof(double), s>>>(
         v, Y1.get(), U.get(), Wb.get(), KWb.get(), C.get(), G.get(), a, flag.get());
     count_launch();
@@ -547,6 +557,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   prefix_count = count;
   scaling = scaling_;
   center = scaling != 3;
+  digits = ozaki_slices();
   require(q >= 1 && q <= kBatchMaxResponses, "batched CV supports 1..32 responses");
   kmax = 0;
   for (int j = 0; j < count; ++j) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "ozaki.cuh"
 
 #include <vector>
 
@@ -32,12 +33,18 @@ struct BatchedCv {
   void form_gram(const double* kscale, cudaStream_t s);
   void run_group(const std::vector<int>& inst_fold,
                  const std::vector<int>& inst_perm, cudaStream_t s);
+  // out (n x cols) = K rhs, rhs n x cols column-major (ld n): FP64 DMMA or,
+  // when digits > 0, the int8 split product with the digits of K prepared by
+  // form_gram.
+  void gram_product(const double* rhs, int cols, double* out, cudaStream_t s);
 
   const T* X = nullptr;
   const int* perms = nullptr;
   int n = 0, p = 0, q = 0, P = 0, prefix_count = 0, scaling = 1, kmax = 0;
   int folds = 0, max_test = 1;
   bool center = true;
+  int digits = 0;                 // int8 digits per FP64 value (0: FP64 DMMA)
+  OzakiOperand gram_split, rhs_split, x_split;
   DeviceArray<double> gram, Y64, x64;
   DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag;
 };

@@ -1,0 +1,652 @@
+// FP64-accurate GEMM on the int8 tensor cores (tcgen05.mma kind::i8, TMEM
+// accumulators, TMA-fed shared memory), by the digit split described in
+// ozaki.cuh.
+//
+// Kernel layout (one CTA per 128 x 128 output tile, 192 threads):
+//   warp 0, lane 0   TMA producer: per k-block of 64 bytes, the digit planes
+//                    0..ns-1 of the A rows and of the B rows of the tile
+//                    (8 KB each, 64-byte swizzle) into a ring of stages.
+//   warp 1, lane 0   MMA issuer: for every diagonal d of the pass and every
+//                    digit pair (s, d - s), two tcgen05.mma (K = 32 each)
+//                    into the TMEM accumulator of d (128 lanes x 128 int32
+//                    columns); tcgen05.commit releases the stage.
+//   warps 2..5       epilogue: tcgen05.ld of the accumulators (lane quarter
+//                    = warp % 4), exact int32 -> FP64, weighted sum over the
+//                    diagonals, power-of-two row scales, store to C.
+// TMEM holds four 128-column accumulators, so the S diagonals run in passes
+// of four (S = 6: diagonals 0-3, then 4-5); a later pass adds to C. Every
+// wait on an mbarrier is bounded: on expiry the kernel sets flag = 4, stops
+// issuing, waits (bounded) for its copies and MMAs in flight, frees TMEM and
+// returns.
+#include "ozaki.cuh"
+#include "kernels.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+
+namespace fpls {
+
+int& ozaki_slices() {
+  static int slices = 6;
+  return slices;
+}
+
+namespace {
+
+constexpr int OZ_BM = 128;                 // A rows per tile (TMEM lanes)
+constexpr int OZ_BN = 128;                 // B rows per tile (accumulator columns)
+constexpr int OZ_BK = 64;                  // k bytes per stage (64-byte swizzle span)
+constexpr int OZ_PLANE = OZ_BM * OZ_BK;    // one digit plane block: 8 KB
+constexpr int OZ_DATA = 2 * 2 * kOzakiMaxSlices * OZ_PLANE;  // 224 KB of stages
+constexpr int OZ_MAX_STAGES = 4;
+constexpr int OZ_THREADS = 192;
+constexpr int OZ_ACC = 4;                  // accumulators per pass (4 x 128 columns)
+constexpr int OZ_TMEM_COLS = 512;
+constexpr long long OZ_WAIT_CYCLES = 4000000000LL;  // about 2 s
+
+struct OzArgs {
+  int M, N;          // valid rows of A (output rows) and of B (output columns)
+  int tiles_n;       // column tiles (rectangular grid)
+  int kb0, kblocks;  // k-block range of this launch
+  int slices, stages, lower, accumulate;
+  long ldc;
+  double* C;
+  const double* scale_a;
+  const double* scale_b;
+  int* flag;
+  double weight[kOzakiMaxSlices];  // 1 / (127^2 254^d)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for the phase of the given parity. Gives up when another
+// thread of the CTA gave up (abort set, unless ignore_abort) or after
+// OZ_WAIT_CYCLES; a timeout sets the CTA abort flag and the error flag.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                          int* flag, bool ignore_abort = false) {
+  const long long start = clock64();
+  while (!mbar_test(bar, parity)) {
+    if (!ignore_abort && *abort) return false;
+    if (clock64() - start > OZ_WAIT_CYCLES) {
+      *abort = 1;
+      flag_error(flag, 4);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 bytes,
+// 8-row groups 512 bytes apart (descriptor version 1).
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
+         ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+// Instruction descriptor: s32 accumulator, signed int8 A and B, both K-major,
+// N = 128 (bits 17-22: N / 8), M = 128 (bits 24-28: M / 16).
+constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(OZ_IDESC), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
+                      const __grid_constant__ CUtensorMap map_b, const OzArgs args) {
+  extern __shared__ uint8_t oz_smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[OZ_MAX_STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[OZ_MAX_STAGES];
+  __shared__ __align__(8) uint64_t acc_full, acc_empty, drain_bar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int abort_s;
+  volatile int* abort = &abort_s;
+
+  uint8_t* smem = oz_smem_raw + ((1024 - (smem_u32(oz_smem_raw) & 1023)) & 1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int tm, tn;
+  if (args.lower) {
+    // blockIdx.x = tm (tm + 1) / 2 + tn, tn <= tm
+    const int t = blockIdx.x;
+    int r = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    while (r * (r + 1) / 2 > t) --r;
+    tm = r;
+    tn = t - r * (r + 1) / 2;
+  } else {
+    tm = blockIdx.x / args.tiles_n;
+    tn = blockIdx.x % args.tiles_n;
+  }
+  const int S = args.slices;
+  const int stages = args.stages;
+  const int stage_bytes = 2 * S * OZ_PLANE;
+  const int npass = (S + OZ_ACC - 1) / OZ_ACC;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < stages; ++i) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], 1);
+    }
+    mbar_init(&acc_full, 1);
+    mbar_init(&acc_empty, 4 * 32);
+    mbar_init(&drain_bar, 1);
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(OZ_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------------------------------------------------- producer
+      uint32_t it = 0;
+      bool ok = true;
+      for (int pass = 0; pass < npass && ok; ++pass) {
+        const int dhi = min(S - 1, pass * OZ_ACC + OZ_ACC - 1);
+        const int ns = min(S, dhi + 1);
+        const uint32_t bytes = 2u * ns * OZ_PLANE;
+        for (int kb = 0; kb < args.kblocks; ++kb) {
+          const int st = it % stages;
+          if (it >= (uint32_t)stages &&
+              !mbar_wait(&empty_bar[st], ((it / stages) - 1) & 1, abort, args.flag)) {
+            ok = false;
+            break;
+          }
+          uint8_t* a_dst = smem + st * stage_bytes;
+          uint8_t* b_dst = a_dst + S * OZ_PLANE;
+          mbar_expect_tx(&full_bar[st], bytes);
+          const int kx = (args.kb0 + kb) * OZ_BK;
+          for (int j = 0; j < ns; ++j) {
+            tma_load_3d(a_dst + j * OZ_PLANE, &map_a, kx, tm * OZ_BM, j, &full_bar[st]);
+            tma_load_3d(b_dst + j * OZ_PLANE, &map_b, kx, tn * OZ_BN, j, &full_bar[st]);
+          }
+          ++it;
+        }
+      }
+      // copies still in flight land before the CTA leaves (no-op when every
+      // stage was consumed)
+      for (uint32_t j = it > (uint32_t)stages ? it - stages : 0; j < it; ++j)
+        mbar_wait(&full_bar[j % stages], (j / stages) & 1, abort, args.flag, true);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // -------------------------------------------------------- MMA issuer
+      uint32_t it = 0;
+      bool ok = true;
+      for (int pass = 0; pass < npass && ok; ++pass) {
+        const int dlo = pass * OZ_ACC, dhi = min(S - 1, dlo + OZ_ACC - 1);
+        if (pass > 0) {
+          if (!mbar_wait(&acc_empty, (pass - 1) & 1, abort, args.flag)) break;
+          tc_fence_after();
+        }
+        for (int kb = 0; kb < args.kblocks; ++kb) {
+          const int st = it % stages;
+          if (!mbar_wait(&full_bar[st], (it / stages) & 1, abort, args.flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + st * stage_bytes);
+          const uint32_t b0 = a0 + S * OZ_PLANE;
+#pragma unroll
+          for (int ks = 0; ks < OZ_BK / 32; ++ks)
+            for (int d = dlo; d <= dhi; ++d)
+              for (int s = 0; s <= d; ++s) {
+                const uint64_t ad = sw64_desc(a0 + s * OZ_PLANE + ks * 32);
+                const uint64_t bd = sw64_desc(b0 + (d - s) * OZ_PLANE + ks * 32);
+                const uint32_t acc = (kb > 0 || ks > 0 || s > 0) ? 1u : 0u;
+                tc_mma_i8(tmem + (uint32_t)((d - dlo) * OZ_BN), ad, bd, acc);
+              }
+          tc_commit(&empty_bar[st]);
+          ++it;
+        }
+        if (ok) tc_commit(&acc_full);
+      }
+      // every MMA issued has completed before TMEM is freed
+      tc_commit(&drain_bar);
+      mbar_wait(&drain_bar, 0, abort, args.flag, true);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int quarter = warp & 3;
+    const int row = tm * OZ_BM + quarter * 32 + lane;
+    const bool row_ok = row < args.M;
+    const double sa = row_ok ? args.scale_a[row] : 0.0;
+    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+    for (int pass = 0; pass < npass; ++pass) {
+      const int dlo = pass * OZ_ACC, dhi = min(S - 1, dlo + OZ_ACC - 1);
+      const int nd = dhi - dlo + 1;
+      int ready = 0;
+      if (lane == 0) ready = mbar_wait(&acc_full, pass & 1, abort, args.flag) ? 1 : 0;
+      ready = __shfl_sync(0xffffffffu, ready, 0);
+      if (!ready) break;
+      tc_fence_after();
+      double w[OZ_ACC];
+#pragma unroll
+      for (int a = 0; a < OZ_ACC; ++a) w[a] = a < nd ? args.weight[dlo + a] : 0.0;
+      const bool add = pass > 0 || args.accumulate;
+      for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
+        uint32_t r[OZ_ACC][16];
+#pragma unroll
+        for (int a = 0; a < OZ_ACC; ++a)
+          if (a < nd) tmem_ld16(lane_addr + (uint32_t)(a * OZ_BN + c0), r[a]);
+        tmem_wait_ld();
+        double v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = 0.0;
+#pragma unroll
+        for (int a = OZ_ACC - 1; a >= 0; --a)
+          if (a < nd) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              v[j] = __dadd_rn(v[j], __dmul_rn(w[a], (double)(int)r[a][j]));
+          }
+        if (row_ok) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = tn * OZ_BN + c0 + j;
+            if (col < args.N) {
+              const double val = __dmul_rn(__dmul_rn(v[j], sa), args.scale_b[col]);
+              double* dst = args.C + row + (long)col * args.ldc;
+              *dst = add ? __dadd_rn(*dst, val) : val;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      if (pass + 1 < npass) mbar_arrive(&acc_empty);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(OZ_TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// ------------------------------------------------------------------ split
+// x = 2^e (d0 + d1/254 + ...)/127: scaled by 2^-e (exact) and 127, then
+// rounded to nearest digit by digit.
+__device__ __forceinline__ void split_value(double x, double inv, int slices, int (&d)[kOzakiMaxSlices]) {
+  double v = __dmul_rn(__dmul_rn(x, inv), 127.0);
+#pragma unroll
+  for (int s = 0; s < kOzakiMaxSlices; ++s) {
+    if (s < slices) {
+      const double r = rint(v);
+      d[s] = (int)r;
+      v = __dmul_rn(__dsub_rn(v, r), 254.0);
+    } else {
+      d[s] = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void row_exponent(double mx, double* inv, double* scale) {
+  if (mx > 0.0 && isfinite(mx)) {
+    int e = 0;
+    frexp(mx, &e);  // mx = f 2^e, f in [0.5, 1): 2^e > mx
+    *inv = ldexp(1.0, -e);
+    *scale = ldexp(1.0, e);
+  } else {
+    *inv = 0.0;
+    *scale = 1.0;
+  }
+}
+
+// Warp per row; rows stored contiguously (row r at src + r * ld).
+__global__ void split_rows_kernel(const double* __restrict__ src, long ld, int rows, int k,
+                                  int rows_p, int k_p, int slices, int8_t* __restrict__ digits,
+                                  double* __restrict__ scale, int* flag) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (row >= rows_p) return;
+  const bool live = row < rows;
+  const double* x = src + (long)row * ld;
+  double mx = 0.0;
+  bool bad = false;
+  if (live)
+    for (int c = lane; c < k; c += 32) {
+      const double v = x[c];
+      bad |= !isfinite(v);
+      mx = fmax(mx, fabs(v));
+    }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (__any_sync(0xffffffffu, bad) && lane == 0) flag_error(flag, 1);
+  double inv, sc;
+  row_exponent(mx, &inv, &sc);
+  if (lane == 0) scale[row] = sc;
+  const size_t plane = (size_t)rows_p * k_p;
+  for (int c4 = lane * 4; c4 < k_p; c4 += 128) {
+    int d[4][kOzakiMaxSlices];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c4 + j;
+      const double v = (live && c < k) ? x[c] : 0.0;
+      split_value(isfinite(v) ? v : 0.0, inv, slices, d[j]);
+    }
+    for (int s = 0; s < slices; ++s) {
+      char4 out = make_char4((signed char)d[0][s], (signed char)d[1][s], (signed char)d[2][s],
+                             (signed char)d[3][s]);
+      *reinterpret_cast<char4*>(digits + s * plane + (size_t)row * k_p + c4) = out;
+    }
+  }
+}
+
+// Row maxima of a scaled column-major matrix (non-negative doubles order as
+// their bit patterns, so an integer atomic max is exact and deterministic).
+template <class T>
+__global__ void colmajor_rowmax(const T* __restrict__ X, int n, int p, long ld,
+                                const double* __restrict__ kscale, int cols_per_block,
+                                unsigned long long* rowmax, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j0 = blockIdx.y * cols_per_block, j1 = min(p, j0 + cols_per_block);
+  double mx = 0.0;
+  bool bad = false;
+  for (int j = j0; j < j1; ++j) {
+    double v = as_f64(X[i + (long)j * ld]);
+    if (kscale) v = v * sqrt(kscale[j]);
+    bad |= !isfinite(v);
+    mx = fmax(mx, fabs(v));
+  }
+  if (bad) flag_error(flag, 1);
+  atomicMax(rowmax + i, (unsigned long long)__double_as_longlong(mx));
+}
+
+// 64 x 64 tile: read along rows (coalesced in the column-major source),
+// write each row's 64 digits per plane contiguously.
+template <class T>
+__global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
+                               const double* __restrict__ kscale,
+                               const unsigned long long* __restrict__ rowmax, int rows_p,
+                               int k_p, int slices, int8_t* __restrict__ digits,
+                               double* __restrict__ scale) {
+  __shared__ double tile[64][65];
+  const int i0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
+  {
+    const int ii = threadIdx.x & 63;
+    const int i = i0 + ii;
+    for (int kk = threadIdx.x >> 6; kk < 64; kk += 4) {
+      const int c = k0 + kk;
+      double v = 0.0;
+      if (i < n && c < p) {
+        v = as_f64(X[i + (long)c * ld]);
+        if (kscale) v = v * sqrt(kscale[c]);
+        if (!isfinite(v)) v = 0.0;
+      }
+      tile[kk][ii] = v;
+    }
+  }
+  __syncthreads();
+  const int ii = threadIdx.x >> 2, kg = (threadIdx.x & 3) * 16;
+  const int i = i0 + ii;
+  double inv = 0.0, sc = 1.0;
+  if (i < n) row_exponent(__longlong_as_double((long long)rowmax[i]), &inv, &sc);
+  if (blockIdx.y == 0 && (threadIdx.x & 3) == 0) scale[i] = sc;
+  const size_t plane = (size_t)rows_p * k_p;
+  alignas(16) signed char out[kOzakiMaxSlices][16];
+#pragma unroll 4
+  for (int j = 0; j < 16; ++j) {
+    int d[kOzakiMaxSlices];
+    split_value(tile[kg + j][ii], inv, slices, d);
+#pragma unroll
+    for (int s = 0; s < kOzakiMaxSlices; ++s) out[s][j] = (signed char)d[s];
+  }
+  for (int s = 0; s < slices; ++s)
+    *reinterpret_cast<int4*>(digits + s * plane + (size_t)i * k_p + k0 + kg) =
+        *reinterpret_cast<const int4*>(out[s]);
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+void prepare(OzakiOperand& out, int rows, int k, int slices, cudaStream_t s) {
+  require(slices >= 1 && slices <= kOzakiMaxSlices, "int8 split: 1..7 digits");
+  require(rows >= 0 && k >= 0, "int8 split: invalid shape");
+  out.rows = rows;
+  out.k = k;
+  out.rows_p = std::max(OZ_BM, round_up(rows, OZ_BM));
+  out.k_p = std::max(OZ_BK, round_up(k, OZ_BK));
+  out.slices = slices;
+  out.digits.reserve((size_t)slices * out.rows_p * out.k_p, s);
+  out.scale.reserve((size_t)out.rows_p, s);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    FPLS_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p)
+      throw std::runtime_error("cuTensorMapEncodeTiled is not available from the driver");
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+CUtensorMap digit_map(const OzakiOperand& op) {
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {(cuuint64_t)op.k_p, (cuuint64_t)op.rows_p, (cuuint64_t)op.slices};
+  const cuuint64_t strides[2] = {(cuuint64_t)op.k_p, (cuuint64_t)op.k_p * op.rows_p};
+  const cuuint32_t box[3] = {OZ_BK, OZ_BM, 1};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  const CUresult r = encode_tiled()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                                    (void*)op.digits.get(), dims, strides, box, elem,
+                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed for the digit planes");
+  return map;
+}
+
+struct OzTiming {
+  bool enabled = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+  std::vector<double> ops;
+};
+OzTiming& oz_timing() {
+  static OzTiming t;
+  return t;
+}
+
+}  // namespace
+
+void ozaki_profile_enable(bool on) { oz_timing().enabled = on; }
+
+void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launches) {
+  OzTiming& t = oz_timing();
+  double total_ms = 0.0, total_ops = 0.0;
+  for (size_t k = 0; k < t.events.size(); ++k) {
+    float e = 0.f;
+    cudaEventSynchronize(t.events[k].second);
+    cudaEventElapsedTime(&e, t.events[k].first, t.events[k].second);
+    total_ms += e;
+    total_ops += t.ops[k];
+    cudaEventDestroy(t.events[k].first);
+    cudaEventDestroy(t.events[k].second);
+  }
+  if (ms) *ms = total_ms;
+  if (int8_ops) *int8_ops = total_ops;
+  if (launches) *launches = t.events.size();
+  t.events.clear();
+  t.ops.clear();
+}
+
+void ozaki_split_rows(const double* src, long ld, int rows, int k, int slices,
+                      OzakiOperand& out, int* flag, cudaStream_t stream) {
+  prepare(out, rows, k, slices, stream);
+  const int warps = 8;
+  split_rows_kernel<<<ceil_div(out.rows_p, warps), 32 * warps, 0, stream>>>(
+      src, ld, rows, k, out.rows_p, out.k_p, slices, out.digits.get(), out.scale.get(), flag);
+  count_launch();
+  FPLS_LAUNCH("split_rows_kernel");
+}
+
+template <class T>
+void ozaki_split_colmajor(const T* X, int n, int p, long ld, const double* kscale,
+                          int slices, OzakiOperand& out, int* flag, cudaStream_t stream) {
+  prepare(out, n, p, slices, stream);
+  DeviceArray<unsigned long long> rowmax((size_t)out.rows_p, stream);
+  rowmax.zero(stream);
+  const int cols_per_block = 128;
+  dim3 g1(ceil_div(std::max(n, 1), 256), ceil_div(std::max(p, 1), cols_per_block));
+  colmajor_rowmax<T><<<g1, 256, 0, stream>>>(X, n, p, ld, kscale, cols_per_block, rowmax.get(), flag);
+  dim3 g2(out.rows_p / 64, out.k_p / 64);
+  colmajor_split<T><<<g2, 256, 0, stream>>>(X, n, p, ld, kscale, rowmax.get(), out.rows_p,
+                                           out.k_p, slices, out.digits.get(), out.scale.get());
+  count_launch(2);
+  FPLS_LAUNCH("colmajor_split");
+}
+
+template void ozaki_split_colmajor<float>(const float*, int, int, long, const double*, int,
+                                          OzakiOperand&, int*, cudaStream_t);
+template void ozaki_split_colmajor<double>(const double*, int, int, long, const double*, int,
+                                           OzakiOperand&, int*, cudaStream_t);
+
+void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ldc, bool lower,
+                int* flag, cudaStream_t stream) {
+  require(a.slices == b.slices && a.slices >= 1 && a.slices <= kOzakiMaxSlices,
+          "int8 split product: operands need the same digit count (1..7)");
+  require(a.k == b.k && a.k_p == b.k_p, "int8 split product: operands need the same k");
+  require(!lower || (&a == &b), "symmetric int8 split product needs one operand");
+  require(ldc >= std::max(a.rows, 1), "int8 split product: ldc < rows");
+  if (a.rows == 0 || b.rows == 0) return;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (oz_timing().enabled) {
+    FPLS_CHECK(cudaEventCreate(&ev0));
+    FPLS_CHECK(cudaEventCreate(&ev1));
+    FPLS_CHECK(cudaEventRecord(ev0, stream));
+  }
+  const int S = a.slices;
+  const int stage_bytes = 2 * S * OZ_PLANE;
+  const int stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
+  const size_t smem = (size_t)stages * stage_bytes + 1024;
+  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  OZ_DATA + 1024));
+  const CUtensorMap map_a = digit_map(a);
+  const CUtensorMap map_b = digit_map(b);
+  OzArgs args{};
+  args.M = a.rows;
+  args.N = b.rows;
+  args.slices = S;
+  args.stages = stages;
+  args.lower = lower ? 1 : 0;
+  args.ldc = ldc;
+  args.C = C;
+  args.scale_a = a.scale.get();
+  args.scale_b = b.scale.get();
+  args.flag = flag;
+  for (int d = 0; d < kOzakiMaxSlices; ++d) args.weight[d] = 1.0 / (16129.0 * std::pow(254.0, d));
+  const int tiles_m = a.rows_p / OZ_BM, tiles_n = b.rows_p / OZ_BN;
+  args.tiles_n = tiles_n;
+  const long tiles = lower ? (long)tiles_m * (tiles_m + 1) / 2 : (long)tiles_m * tiles_n;
+  // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
+  const int kb_total = a.k_p / OZ_BK;
+  const int kb_seg = std::max(1, (int)((2147483647LL / (16129LL * S)) / OZ_BK));
+  for (int kb0 = 0; kb0 < kb_total; kb0 += kb_seg) {
+    args.kb0 = kb0;
+    args.kblocks = std::min(kb_seg, kb_total - kb0);
+    args.accumulate = kb0 > 0 ? 1 : 0;
+    ozaki_gemm_kernel<<<(unsigned)tiles, OZ_THREADS, smem, stream>>>(map_a, map_b, args);
+    count_launch();
+    FPLS_LAUNCH("ozaki_gemm_kernel");
+  }
+  if (lower) mirror_lower_triangle(C, a.rows, ldc, stream);
+  if (ev0) {
+    FPLS_CHECK(cudaEventRecord(ev1, stream));
+    oz_timing().events.emplace_back(ev0, ev1);
+    const double pairs = S * (S + 1) / 2.0;
+    oz_timing().ops.push_back(pairs * (lower ? (double)a.rows * (a.rows + 1.0) * a.k
+                                             : 2.0 * a.rows * (double)b.rows * a.k));
+  }
+}
+
+}  // namespace fpls

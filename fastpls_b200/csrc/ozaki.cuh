@@ -1,0 +1,58 @@
+// FP64-accurate products on the int8 tensor cores (tcgen05, kind::i8).
+//
+// Each FP64 operand row is scaled by a power of two 2^e >= max|row| and
+// written as S signed 8-bit digits with round-to-nearest:
+//     v0 = x 2^-e 127,  d_s = rint(v_s),  v_{s+1} = (v_s - d_s) 254
+// so x = 2^e (d_0 + d_1/254 + ... + d_{S-1}/254^{S-1} + r) / 127 with
+// |r| <= 1/(2 254^{S-1}). The product of two such rows is the sum over digit
+// pairs (s, t); pairs on the same diagonal d = s + t share the weight
+// 1 / (127^2 254^d) and are accumulated exactly in int32 by the tensor core
+// (|sum| <= (d+1) K 127^2 < 2^31 for K below 2^17). Diagonals d <= S - 1 are
+// kept (S (S + 1) / 2 int8 products); the FP64 epilogue combines the exact
+// integer sums of the diagonals, smallest weight first, and applies the two
+// power-of-two row scales. With S = 6 the product error is below 2^-47 of
+// max|a_i| max|b_j| K, which keeps the batched SIMPLS path within 1e-5 of the
+// FP64 path at 20 components.
+#pragma once
+
+#include "common.cuh"
+
+namespace fpls {
+
+constexpr int kOzakiMaxSlices = 7;
+
+// One operand of the split product: digit planes int8 [slices][rows_p][k_p]
+// (row-major, k contiguous, zero padded to rows_p = 128-multiple rows and
+// k_p = 64-multiple columns) and one power-of-two scale per row.
+struct OzakiOperand {
+  DeviceArray<int8_t> digits;
+  DeviceArray<double> scale;
+  int rows = 0, rows_p = 0, k = 0, k_p = 0, slices = 0;
+};
+
+// Rows stored contiguously: row r is src[r * ld + 0 .. k).
+void ozaki_split_rows(const double* src, long ld, int rows, int k, int slices,
+                      OzakiOperand& out, int* flag, cudaStream_t stream);
+
+// Rows of a column-major n x p matrix X (leading dimension ld), each element
+// scaled as X[i, j] * sqrt(kscale[j]) when kscale is given.
+template <class T>
+void ozaki_split_colmajor(const T* X, int n, int p, long ld,
+                          const double* kscale, int slices, OzakiOperand& out,
+                          int* flag, cudaStream_t stream);
+
+// C (a.rows x b.rows, column-major, ldc) = A B^T over the split rows of a
+// and b (same k, same slices). lower: only tiles on or below the diagonal
+// are computed (a and b must be the same operand) and mirrored.
+void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C,
+                long ldc, bool lower, int* flag, cudaStream_t stream);
+
+// Digit count used by the batched CV engine for its products with the
+// shared Gram (0 selects the FP64 DMMA path). Process-wide setting.
+int& ozaki_slices();
+
+// Timing of the last ozaki_gemm launches (CUDA events), for benchmarks.
+void ozaki_profile_enable(bool on);
+void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launches);
+
+}  // namespace fpls

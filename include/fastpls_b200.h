@@ -195,6 +195,33 @@ FASTPLS_B200_API void fastpls_b200_profile_gemm_read(
 FASTPLS_B200_API int fastpls_b200_fp64_peak(double* tflops, char* error,
                                             size_t error_capacity);
 
+/* Products with the shared Gram in the batched CV engine (no reference
+ * counterpart; the reference forms them in FP64 BLAS): digits = 0 runs them
+ * as FP64 DMMA GEMMs; digits = 1..7 splits every FP64 value into that many
+ * int8 digits (power-of-two row scale, base 254, round to nearest) and runs
+ * the digit-pair products on the int8 tensor cores (tcgen05.mma kind::i8)
+ * with exact int32 accumulation. Default 6: product error below 2^-47 of
+ * max|a_i| max|b_j| k. Process-wide; read back with _product_digits. */
+FASTPLS_B200_API void fastpls_b200_set_product_digits(int digits);
+FASTPLS_B200_API int fastpls_b200_product_digits(void);
+
+/* Benchmark instrumentation of the int8 split products, as for
+ * fastpls_b200_profile_gemm; the operation count is the int8 multiply-adds
+ * issued (2 M N k per digit pair, M (M + 1) k for a symmetric product). */
+FASTPLS_B200_API void fastpls_b200_profile_int8(int enable);
+FASTPLS_B200_API void fastpls_b200_profile_int8_read(
+    double* milliseconds, double* int8_ops, unsigned long long* launches);
+
+/* c (m x n, column-major, ldc) = a^T b by the int8 split product above, for
+ * a (k x m, lda) and b (k x n, ldb) column-major FP64 host arrays. With
+ * symmetric = 1 (a == b, m == n) only the lower tiles are computed and
+ * mirrored. No reference counterpart (test and integration entry for the
+ * split product). */
+FASTPLS_B200_API int fastpls_b200_int8_crossprod(
+    const double* a, int lda, const double* b, int ldb, int m, int n, int k,
+    int digits, int symmetric, double* c, int ldc, char* error,
+    size_t error_capacity);
+
 /* Batched SIMPLS regression CV over the observed responses and
  * `permutation_count` row permutations of them (pls.single.cv /
  * pls.double.cv with perm.test; R/main.R:9419-9450, 12048-12080), all
