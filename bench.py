@@ -5,13 +5,18 @@ Workload (the cross-validation x permutation configuration): X 5000 x 10000
 FP32 from the latent-factor generator (k = 10, noise 0.3), Y with 3
 continuous responses, 10 uneven folds (480-520 rows), the ncomp path 1..20
 and 200 seeded row permutations of Y -> (1 + 200) x 10 = 2010 SIMPLS fits per
-step, all sharing one device-resident X. Arithmetic is FP64 on the device.
+step, all sharing one device-resident X. Arithmetic is FP64 on the device;
+the products with the shared n x n Gram run as int8 digit-split products on
+the tensor cores (6 digits: error below 2^-47 of the row/column scale, the
+path within 1e-5 of FP64), or as FP64 DMMA GEMMs with --digits 0.
 
 One JSON line on rank 0 with
   value    fits/s with X, Y, folds and permutations resident in HBM,
   e2e      fits/s through the host-pointer C ABI call (H2D of every input and
            D2H of every result inside the timed region, pinned host buffers),
-  roofline the dominant kernel (FP64 GEMM) against the measured FP64 FMA rate,
+  roofline the dominant kernel (the int8 split product) against the measured
+           int8 tensor throughput of a library GEMM (FP64 DMMA GEMM against
+           the measured FP64 FMA rate with --digits 0),
   cpu_baseline the reference's own FP64 C++ core (oracle/_ref, OpenBLAS on all
            host cores) on a bounded sample of the same workload.
 `--impl reference` times that CPU reference alone (the reference arm).
@@ -50,6 +55,11 @@ def args_parse():
                     help="requests in the served mixed-workload leg (0 = skip)")
     ap.add_argument("--plain-perms", type=int, default=3,
                     help="permutations sampled for the one-fit-at-a-time path")
+    ap.add_argument("--digits", type=int, default=6,
+                    help="int8 digits per FP64 value in the products with the "
+                         "shared Gram (0 = FP64 DMMA GEMMs)")
+    ap.add_argument("--fp64-steps", type=int, default=2,
+                    help="timed steps with FP64 DMMA products, for comparison")
     return ap.parse_args()
 
 
@@ -298,12 +308,37 @@ def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
             "p99_ms": float(np.percentile(lat, 99))}
 
 
-def workload_config(perms):
+def int8_peak_tops(torch, dev):
+    """Dense int8 tensor-core throughput of this device, measured with the
+    library GEMM torch._int_mm (cuBLAS) on 8192^3 int8 operands."""
+    try:
+        a = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device=dev)
+        for _ in range(3):
+            torch._int_mm(a, b)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record()
+        for _ in range(reps):
+            torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return 2.0 * 8192 ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12, \
+            "measured in this run (cuBLAS int8 GEMM via torch._int_mm, 8192^3)"
+    except Exception as exc:  # no int8 library GEMM: nominal dense figure
+        return 4500.0, f"nominal B200 dense int8 (library GEMM unavailable: {exc})"
+
+
+def workload_config(perms, digits=6):
     return {"workload": f"cv{FOLDS}_perm{perms}_ncomp{NCOMP}_{N}x{P}_f32",
             "n": N, "p": P, "q": Q, "folds": FOLDS, "fold_sizes": "480-520",
             "permutations": perms, "ncomp_path": f"1..{NCOMP}",
             "fits_per_step": (perms + 1) * FOLDS, "storage": "f32",
             "arithmetic": "f64", "method": "simpls", "scaling": "centering",
+            "gram_products": (f"int8 split, {digits} digits per FP64 value "
+                              "(tcgen05.mma kind::i8, exact int32 accumulation)"
+                              if digits > 0 else "FP64 DMMA"),
             "l2": "inputs larger than L2 (X 200 MB FP32, Gram 200 MB FP64)",
             "parallelism": "replicas"}
 
@@ -379,10 +414,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # measured FP64 FMA peak (roofline denominator)
+    # measured FP64 FMA peak and int8 tensor peak (roofline denominators)
     pk = C.c_double(0)
     _lib.check(lib.fastpls_b200_fp64_peak(C.byref(pk), err, cap), err)
     fp64_peak = pk.value
+    i8_peak, i8_source = int8_peak_tops(torch, dev)
+    lib.fastpls_b200_set_product_digits(a.digits)
+    digits = lib.fastpls_b200_product_digits()
 
     clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
     clk = clock_sampler_start(clk_path)
@@ -391,6 +429,7 @@ def main():
     barrier()
     launches0 = lib.fastpls_b200_launch_count()
     lib.fastpls_b200_profile_gemm(1)
+    lib.fastpls_b200_profile_int8(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
     barrier()
     ev[0].record(stream)
@@ -399,13 +438,39 @@ def main():
         ev[s + 1].record(stream)
     barrier()
     lib.fastpls_b200_profile_gemm(0)
+    lib.fastpls_b200_profile_int8(0)
     launches = lib.fastpls_b200_launch_count() - launches0
     clocks = clock_sampler_stop(clk, clk_path, local)
     step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(a.steps)]
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     gms, gfl, gl = C.c_double(0), C.c_double(0), C.c_ulonglong(0)
     lib.fastpls_b200_profile_gemm_read(C.byref(gms), C.byref(gfl), C.byref(gl))
+    ims, iops, il = C.c_double(0), C.c_double(0), C.c_ulonglong(0)
+    lib.fastpls_b200_profile_int8_read(C.byref(ims), C.byref(iops), C.byref(il))
     observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
+    all_q2 = outs[1].reshape(Pn + 1, k).copy()
+
+    # the same step with FP64 DMMA products, for comparison (and the distance
+    # of the int8 split path to it over every instance)
+    fp64_leg = None
+    if digits > 0 and a.fp64_steps > 0:
+        lib.fastpls_b200_set_product_digits(0)
+        step_device()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(a.fp64_steps):
+            step_device()
+        f1.record(stream)
+        barrier()
+        fms = max_over_ranks(f0.elapsed_time(f1)) / a.fp64_steps
+        q2_fp64 = outs[1].reshape(Pn + 1, k).copy()
+        lib.fastpls_b200_set_product_digits(digits)
+        fp64_leg = {"value": world * fits_per_step / (fms / 1000.0), "unit": "fits/s",
+                    "ms_per_step": fms, "steps": a.fp64_steps,
+                    "q2_max_rel_diff_int8_vs_fp64_products": float(
+                        np.max(np.abs(all_q2 - q2_fp64) / np.maximum(np.abs(q2_fp64), 1e-300)))}
 
     # end to end through the host-pointer ABI
     for _ in range(2):
@@ -457,11 +522,14 @@ def main():
     ms_per_step = total_ms / a.steps
     value = world * fits_per_step / (ms_per_step / 1000.0)
     achieved = gfl.value / (gms.value * 1e-3) / 1e12 if gms.value > 0 else None
+    i8_achieved = iops.value / (ims.value * 1e-3) / 1e12 if ims.value > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("dgemm_traffic_bytes_per_launch")
+            traffic = json.load(open(tpath)).get(
+                "int8_split_traffic_bytes_per_launch" if digits > 0
+                else "dgemm_traffic_bytes_per_launch")
         except Exception:
             traffic = None
     h2d = Xh.numel() * 4 + Yh.numel() * 4 + Ph.numel() * 4 + folds32.nbytes
@@ -470,20 +538,33 @@ def main():
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world,
         "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": workload_config(Pn),
+        "dtype": "f64", "data": "synthetic", "config": workload_config(Pn, digits),
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                        "p99": float(np.percentile(step_ms, 99))},
         "e2e": {"value": world * fits_per_step / (e2e_ms / 1000.0), "unit": "fits/s",
                 "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "fp64", "kernel": "dgemm_mma (FP64 DMMA tensor path)",
-                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": (achieved / fp64_peak) if achieved else None,
-                     "peak_source": "measured in this run (FP64 FMA-chain probe); "
-                                    "MEASURED_PEAKS.json has no FP64 figure",
-                     "launches": int(gl.value),
-                     "gemm_share_of_step": (gms.value / a.steps) / ms_per_step,
-                     "traffic": traffic},
+        "roofline": ({"bound": "tensor", "kernel": "ozaki_gemm_kernel (int8 split "
+                      "products, tcgen05.mma kind::i8, TMEM accumulators, TMA loads)",
+                      "achieved": i8_achieved, "peak": i8_peak, "unit": "TOP/s (int8)",
+                      "frac": (i8_achieved / i8_peak) if i8_achieved else None,
+                      "peak_source": i8_source,
+                      "launches": int(il.value),
+                      "share_of_step": (ims.value / a.steps) / ms_per_step,
+                      "fp64_equivalent_tflops": (i8_achieved / (digits * (digits + 1) / 2.0))
+                      if i8_achieved else None,
+                      "fp64_fma_peak_tflops": fp64_peak,
+                      "traffic": traffic}
+                     if digits > 0 else
+                     {"bound": "fp64", "kernel": "dgemm_mma (FP64 DMMA tensor path)",
+                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                      "frac": (achieved / fp64_peak) if achieved else None,
+                      "peak_source": "measured in this run (FP64 FMA-chain probe); "
+                                     "MEASURED_PEAKS.json has no FP64 figure",
+                      "launches": int(gl.value),
+                      "share_of_step": (gms.value / a.steps) / ms_per_step,
+                      "traffic": traffic}),
+        "fp64_products": fp64_leg,
         "gpu_launches": int(launches),
         "plain": plain,
         "batched_over_plain_e2e": (world * fits_per_step / (e2e_ms / 1000.0)) / plain["value"]

@@ -2,27 +2,29 @@
 // accumulators, TMA-fed shared memory), by the digit split described in
 // ozaki.cuh.
 //
-// Kernel layout (one CTA per 128 x 128 output tile, 192 threads):
-//   warp 0, lane 0   TMA producer: per k-block of 64 bytes, the digit planes
-//                    0..ns-1 of the A rows and of the B rows of the tile
-//                    (8 KB each, 64-byte swizzle) into a ring of stages.
+// Kernel layout (one CTA per 128 x 128 output tile, 320 threads):
+//   warp 0, lane 0   bulk-copy producer: per k-block of 32 bytes, the digit
+//                    planes 0..ns-1 of the A rows and of the B rows of the
+//                    tile (4 KB each, stored pre-tiled so that they are one
+//                    contiguous run per operand) by two cp.async.bulk copies
+//                    (TMA engine) into a ring of stages.
 //   warp 1, lane 0   MMA issuer: for every diagonal d of the pass and every
-//                    digit pair (s, d - s), two tcgen05.mma (K = 32 each)
-//                    into the TMEM accumulator of d (128 lanes x 128 int32
-//                    columns); tcgen05.commit releases the stage.
-//   warps 2..5       epilogue: tcgen05.ld of the accumulators (lane quarter
-//                    = warp % 4), exact int32 -> FP64, weighted sum over the
-//                    diagonals, power-of-two row scales, store to C.
+//                    digit pair (s, d - s), one tcgen05.mma (K = 32) into the
+//                    TMEM accumulator of d (128 lanes x 128 int32 columns);
+//                    tcgen05.commit releases the stage.
+//   warps 2..9       epilogue: tcgen05.ld of the accumulators (lane quarter
+//                    = warp % 4, column half = (warp - 2) / 4), exact int32 ->
+//                    FP64, weighted sum over the diagonals, power-of-two row
+//                    scales, one store to C.
 // TMEM holds four 128-column accumulators, so the S diagonals run in passes
-// of four (S = 6: diagonals 0-3, then 4-5); a later pass adds to C. Every
-// wait on an mbarrier is bounded: on expiry the kernel sets flag = 4, stops
-// issuing, waits (bounded) for its copies and MMAs in flight, frees TMEM and
-// returns.
+// of four (S = 6: diagonals 0-3, then 4-5); the epilogue keeps the first
+// pass's 64 partial sums per thread in registers while the second pass runs.
+// Every wait on an mbarrier is bounded: on expiry the kernel sets flag = 4,
+// stops issuing, waits (bounded) for its copies and MMAs in flight, frees TMEM
+// and returns.
 #include "ozaki.cuh"
 #include "kernels.cuh"
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -38,11 +40,13 @@ namespace {
 
 constexpr int OZ_BM = 128;                 // A rows per tile (TMEM lanes)
 constexpr int OZ_BN = 128;                 // B rows per tile (accumulator columns)
-constexpr int OZ_BK = 64;                  // k bytes per stage (64-byte swizzle span)
-constexpr int OZ_PLANE = OZ_BM * OZ_BK;    // one digit plane block: 8 KB
-constexpr int OZ_DATA = 2 * 2 * kOzakiMaxSlices * OZ_PLANE;  // 224 KB of stages
-constexpr int OZ_MAX_STAGES = 4;
-constexpr int OZ_THREADS = 192;
+constexpr int OZ_BK = 32;                  // k bytes per stage (32-byte swizzle span)
+constexpr int OZ_KPAD = 64;                // k padding of the digit planes
+constexpr int OZ_PLANE = OZ_BM * OZ_BK;    // one digit plane block: 4 KB
+constexpr int OZ_DATA = 196 * 1024;        // bytes of stages
+constexpr int OZ_MAX_STAGES = 8;
+constexpr int OZ_EPI_WARPS = 8;
+constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;
 constexpr int OZ_ACC = 4;                  // accumulators per pass (4 x 128 columns)
 constexpr int OZ_TMEM_COLS = 512;
 constexpr long long OZ_WAIT_CYCLES = 4000000000LL;  // about 2 s
@@ -51,13 +55,13 @@ struct OzArgs {
   int M, N;          // valid rows of A (output rows) and of B (output columns)
   int tiles_n;       // column tiles (rectangular grid)
   int kb0, kblocks;  // k-block range of this launch
+  int kb_total;      // k-blocks per row tile in the digit layout
   int slices, stages, lower, accumulate;
   long ldc;
   double* C;
   const double* scale_a;
   const double* scale_b;
   int* flag;
-  double weight[kOzakiMaxSlices];  // 1 / (127^2 254^d)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -106,12 +110,14 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
   return true;
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
-                                            int z, uint64_t* bar) {
+// One contiguous global -> shared copy on the TMA engine, completing on an
+// mbarrier (addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -122,11 +128,13 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, 64-byte swizzle, rows of 64 bytes,
-// 8-row groups 512 bytes apart (descriptor version 1).
-__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
-  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) |
-         ((uint64_t)(512 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+// Shared-memory matrix descriptor: K-major, no swizzle. A plane block holds
+// 16 row groups x 2 k-chunks of 8 x 16-byte core matrices: k-adjacent core
+// matrices 128 bytes apart (leading offset), row groups 256 bytes apart
+// (stride offset); descriptor version 1.
+__device__ __forceinline__ uint64_t core_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(256 >> 4) << 32) | ((uint64_t)1 << 46);
 }
 
 // Instruction descriptor: s32 accumulator, signed int8 A and B, both K-major,
@@ -150,23 +158,59 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
 }
+
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c,
+                                         uint32_t d) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
+               "r"(a), "r"(b), "r"(c), "r"(d)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// 1 / (127^2 254^d): the weight of diagonal d (254^d exact for d < 7)
+constexpr double oz_weight(int d) {
+  double p = 1.0;
+  for (int i = 0; i < d; ++i) p *= 254.0;
+  return 1.0 / (16129.0 * p);
+}
+__constant__ double kOzWeight[kOzakiMaxSlices] = {oz_weight(0), oz_weight(1), oz_weight(2),
+                                                  oz_weight(3), oz_weight(4), oz_weight(5),
+                                                  oz_weight(6)};
 
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Weighted sum over the nd accumulators of a pass for 4 columns of this
+// thread's TMEM lane, smallest weight first (exact int32 -> FP64).
+__device__ __forceinline__ void pass_sum4(uint32_t addr, int nd, const double (&w)[OZ_ACC],
+                                          double (&v)[4]) {
+  uint32_t r[OZ_ACC][4];
+#pragma unroll
+  for (int a = 0; a < OZ_ACC; ++a)
+    if (a < nd) tmem_ld4(addr + (uint32_t)(a * OZ_BN), r[a]);
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = 0.0;
+#pragma unroll
+  for (int a = OZ_ACC - 1; a >= 0; --a)
+    if (a < nd) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = __dadd_rn(v[j], __dmul_rn(w[a], (double)(int)r[a][j]));
+    }
+}
+
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-    ozaki_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
-                      const __grid_constant__ CUtensorMap map_b, const OzArgs args) {
+    ozaki_gemm_kernel(const int8_t* __restrict__ digits_a, const int8_t* __restrict__ digits_b,
+                      const OzArgs args) {
   extern __shared__ uint8_t oz_smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[OZ_MAX_STAGES];
   __shared__ __align__(8) uint64_t empty_bar[OZ_MAX_STAGES];
@@ -201,7 +245,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       mbar_init(&empty_bar[i], 1);
     }
     mbar_init(&acc_full, 1);
-    mbar_init(&acc_empty, 4 * 32);
+    mbar_init(&acc_empty, 32 * OZ_EPI_WARPS);
     mbar_init(&drain_bar, 1);
     abort_s = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -237,11 +281,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           uint8_t* a_dst = smem + st * stage_bytes;
           uint8_t* b_dst = a_dst + S * OZ_PLANE;
           mbar_expect_tx(&full_bar[st], bytes);
-          const int kx = (args.kb0 + kb) * OZ_BK;
-          for (int j = 0; j < ns; ++j) {
-            tma_load_3d(a_dst + j * OZ_PLANE, &map_a, kx, tm * OZ_BM, j, &full_bar[st]);
-            tma_load_3d(b_dst + j * OZ_PLANE, &map_b, kx, tn * OZ_BN, j, &full_bar[st]);
-          }
+          const long kbg = args.kb0 + kb;
+          bulk_load(a_dst, digits_a + ((long)tm * args.kb_total + kbg) * S * OZ_PLANE,
+                    (uint32_t)(ns * OZ_PLANE), &full_bar[st]);
+          bulk_load(b_dst, digits_b + ((long)tn * args.kb_total + kbg) * S * OZ_PLANE,
+                    (uint32_t)(ns * OZ_PLANE), &full_bar[st]);
           ++it;
         }
       }
@@ -271,15 +315,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           tc_fence_after();
           const uint32_t a0 = smem_u32(smem + st * stage_bytes);
           const uint32_t b0 = a0 + S * OZ_PLANE;
-#pragma unroll
-          for (int ks = 0; ks < OZ_BK / 32; ++ks)
-            for (int d = dlo; d <= dhi; ++d)
-              for (int s = 0; s <= d; ++s) {
-                const uint64_t ad = sw64_desc(a0 + s * OZ_PLANE + ks * 32);
-                const uint64_t bd = sw64_desc(b0 + (d - s) * OZ_PLANE + ks * 32);
-                const uint32_t acc = (kb > 0 || ks > 0 || s > 0) ? 1u : 0u;
-                tc_mma_i8(tmem + (uint32_t)((d - dlo) * OZ_BN), ad, bd, acc);
-              }
+          for (int d = dlo; d <= dhi; ++d)
+            for (int s = 0; s <= d; ++s) {
+              const uint64_t ad = core_desc(a0 + s * OZ_PLANE);
+              const uint64_t bd = core_desc(b0 + (d - s) * OZ_PLANE);
+              const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+              tc_mma_i8(tmem + (uint32_t)((d - dlo) * OZ_BN), ad, bd, acc);
+            }
           tc_commit(&empty_bar[st]);
           ++it;
         }
@@ -292,14 +334,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     __syncwarp();
   } else {
     // ------------------------------------------------------------ epilogue
+    // Two epilogue warps per TMEM lane quarter, each owning 64 of the 128
+    // columns of every accumulator. With two passes whose second pass needs
+    // at most two accumulators, the first pass's FP64 sums are parked in
+    // TMEM, in this thread's own (already read) columns of accumulators 2
+    // and 3; otherwise the first pass goes to C and the second adds to it.
     const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = tm * OZ_BM + quarter * 32 + lane;
     const bool row_ok = row < args.M;
     const double sa = row_ok ? args.scale_a[row] : 0.0;
-    const uint32_t lane_addr = tmem + ((uint32_t)(quarter * 32) << 16);
+    const uint32_t mine = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 64);
+    const int col0 = tn * OZ_BN + half * 64;
+    const int nd_last = S - (npass - 1) * OZ_ACC;
+    const bool park = npass == 2 && nd_last <= 2;
     for (int pass = 0; pass < npass; ++pass) {
       const int dlo = pass * OZ_ACC, dhi = min(S - 1, dlo + OZ_ACC - 1);
       const int nd = dhi - dlo + 1;
+      const bool last = pass + 1 == npass;
       int ready = 0;
       if (lane == 0) ready = mbar_wait(&acc_full, pass & 1, abort, args.flag) ? 1 : 0;
       ready = __shfl_sync(0xffffffffu, ready, 0);
@@ -307,38 +359,59 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       tc_fence_after();
       double w[OZ_ACC];
 #pragma unroll
-      for (int a = 0; a < OZ_ACC; ++a) w[a] = a < nd ? args.weight[dlo + a] : 0.0;
-      const bool add = pass > 0 || args.accumulate;
-      for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
-        uint32_t r[OZ_ACC][16];
+      for (int a = 0; a < OZ_ACC; ++a) w[a] = a < nd ? kOzWeight[dlo + a] : 0.0;
+#pragma unroll 2
+      for (int c = 0; c < 16; ++c) {
+        const uint32_t at = mine + (uint32_t)(c * 4);
+        double v[4];
+        if (last && park) {
+          uint32_t p0[4], p1[4];
+          tmem_ld4(at + 2 * OZ_BN, p0);
+          tmem_ld4(at + 3 * OZ_BN, p1);
+          pass_sum4(at, nd, w, v);  // waits for all loads of this thread
+          const double first[4] = {__hiloint2double((int)p0[1], (int)p0[0]),
+                                   __hiloint2double((int)p0[3], (int)p0[2]),
+                                   __hiloint2double((int)p1[1], (int)p1[0]),
+                                   __hiloint2double((int)p1[3], (int)p1[2])};
+          if (row_ok) {
 #pragma unroll
-        for (int a = 0; a < OZ_ACC; ++a)
-          if (a < nd) tmem_ld16(lane_addr + (uint32_t)(a * OZ_BN + c0), r[a]);
-        tmem_wait_ld();
-        double v[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.0;
-#pragma unroll
-        for (int a = OZ_ACC - 1; a >= 0; --a)
-          if (a < nd) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-              v[j] = __dadd_rn(v[j], __dmul_rn(w[a], (double)(int)r[a][j]));
+            for (int j = 0; j < 4; ++j) {
+              const int col = col0 + c * 4 + j;
+              if (col < args.N) {
+                const double sb = args.scale_b[col];
+                double* dst = args.C + row + (long)col * args.ldc;
+                const double f = __dmul_rn(__dmul_rn(first[j], sa), sb);
+                const double val = __dmul_rn(__dmul_rn(v[j], sa), sb);
+                *dst = args.accumulate ? __dadd_rn(__dadd_rn(*dst, f), val) : __dadd_rn(f, val);
+              }
+            }
           }
-        if (row_ok) {
+        } else {
+          pass_sum4(at, nd, w, v);
+          if (!last && park) {
+            tmem_st4(at + 2 * OZ_BN, (uint32_t)__double2loint(v[0]), (uint32_t)__double2hiint(v[0]),
+                     (uint32_t)__double2loint(v[1]), (uint32_t)__double2hiint(v[1]));
+            tmem_st4(at + 3 * OZ_BN, (uint32_t)__double2loint(v[2]), (uint32_t)__double2hiint(v[2]),
+                     (uint32_t)__double2loint(v[3]), (uint32_t)__double2hiint(v[3]));
+          } else if (row_ok) {
+            const bool add = pass > 0 || args.accumulate;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int col = tn * OZ_BN + c0 + j;
-            if (col < args.N) {
-              const double val = __dmul_rn(__dmul_rn(v[j], sa), args.scale_b[col]);
-              double* dst = args.C + row + (long)col * args.ldc;
-              *dst = add ? __dadd_rn(*dst, val) : val;
+            for (int j = 0; j < 4; ++j) {
+              const int col = col0 + c * 4 + j;
+              if (col < args.N) {
+                double* dst = args.C + row + (long)col * args.ldc;
+                const double val = __dmul_rn(__dmul_rn(v[j], sa), args.scale_b[col]);
+                *dst = add ? __dadd_rn(*dst, val) : val;
+              }
             }
           }
         }
       }
-      tc_fence_before();
-      if (pass + 1 < npass) mbar_arrive(&acc_empty);
+      if (!last) {
+        if (park) tmem_wait_st();
+        tc_fence_before();
+        mbar_arrive(&acc_empty);
+      }
     }
   }
 
@@ -353,6 +426,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 }
 
 // ------------------------------------------------------------------ split
+// Byte offset of (row, k) in plane s of the tiled digit layout (k % 4 == 0
+// keeps a 4-byte group, k % 16 == 0 a 16-byte group, inside one core row).
+__device__ __forceinline__ size_t digit_offset(int row, int k, int s, int slices, int kb_total) {
+  return ((size_t)((row >> 7) * kb_total + (k >> 5)) * slices + s) * 4096 +
+         (size_t)(((row & 127) >> 3) * 256 + ((k & 31) >> 4) * 128 + (row & 7) * 16 + (k & 15));
+}
 // x = 2^e (d0 + d1/254 + ...)/127: scaled by 2^-e (exact) and 127, then
 // rounded to nearest digit by digit.
 __device__ __forceinline__ void split_value(double x, double inv, int slices, int (&d)[kOzakiMaxSlices]) {
@@ -404,7 +483,7 @@ __global__ void split_rows_kernel(const double* __restrict__ src, long ld, int r
   double inv, sc;
   row_exponent(mx, &inv, &sc);
   if (lane == 0) scale[row] = sc;
-  const size_t plane = (size_t)rows_p * k_p;
+  const int kb_total = k_p / 32;
   for (int c4 = lane * 4; c4 < k_p; c4 += 128) {
     int d[4][kOzakiMaxSlices];
 #pragma unroll
@@ -416,7 +495,7 @@ __global__ void split_rows_kernel(const double* __restrict__ src, long ld, int r
     for (int s = 0; s < slices; ++s) {
       char4 out = make_char4((signed char)d[0][s], (signed char)d[1][s], (signed char)d[2][s],
                              (signed char)d[3][s]);
-      *reinterpret_cast<char4*>(digits + s * plane + (size_t)row * k_p + c4) = out;
+      *reinterpret_cast<char4*>(digits + digit_offset(row, c4, s, slices, kb_total)) = out;
     }
   }
 }
@@ -443,7 +522,7 @@ __global__ void colmajor_rowmax(const T* __restrict__ X, int n, int p, long ld,
 }
 
 // 64 x 64 tile: read along rows (coalesced in the column-major source),
-// write each row's 64 digits per plane contiguously.
+// write each row's 16-digit groups per plane into the tiled layout.
 template <class T>
 __global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
                                const double* __restrict__ kscale,
@@ -472,7 +551,7 @@ __global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
   double inv = 0.0, sc = 1.0;
   if (i < n) row_exponent(__longlong_as_double((long long)rowmax[i]), &inv, &sc);
   if (blockIdx.y == 0 && (threadIdx.x & 3) == 0) scale[i] = sc;
-  const size_t plane = (size_t)rows_p * k_p;
+  const int kb_total = k_p / 32;
   alignas(16) signed char out[kOzakiMaxSlices][16];
 #pragma unroll 4
   for (int j = 0; j < 16; ++j) {
@@ -482,7 +561,7 @@ __global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
     for (int s = 0; s < kOzakiMaxSlices; ++s) out[s][j] = (signed char)d[s];
   }
   for (int s = 0; s < slices; ++s)
-    *reinterpret_cast<int4*>(digits + s * plane + (size_t)i * k_p + k0 + kg) =
+    *reinterpret_cast<int4*>(digits + digit_offset(i, k0 + kg, s, slices, kb_total)) =
         *reinterpret_cast<const int4*>(out[s]);
 }
 
@@ -494,37 +573,10 @@ void prepare(OzakiOperand& out, int rows, int k, int slices, cudaStream_t s) {
   out.rows = rows;
   out.k = k;
   out.rows_p = std::max(OZ_BM, round_up(rows, OZ_BM));
-  out.k_p = std::max(OZ_BK, round_up(k, OZ_BK));
+  out.k_p = std::max(OZ_KPAD, round_up(k, OZ_KPAD));
   out.slices = slices;
   out.digits.reserve((size_t)slices * out.rows_p * out.k_p, s);
   out.scale.reserve((size_t)out.rows_p, s);
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    FPLS_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    if (q != cudaDriverEntryPointSuccess || !p)
-      throw std::runtime_error("cuTensorMapEncodeTiled is not available from the driver");
-    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }();
-  return fn;
-}
-
-CUtensorMap digit_map(const OzakiOperand& op) {
-  CUtensorMap map;
-  const cuuint64_t dims[3] = {(cuuint64_t)op.k_p, (cuuint64_t)op.rows_p, (cuuint64_t)op.slices};
-  const cuuint64_t strides[2] = {(cuuint64_t)op.k_p, (cuuint64_t)op.k_p * op.rows_p};
-  const cuuint32_t box[3] = {OZ_BK, OZ_BM, 1};
-  const cuuint32_t elem[3] = {1, 1, 1};
-  const CUresult r = encode_tiled()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
-                                    (void*)op.digits.get(), dims, strides, box, elem,
-                                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed for the digit planes");
-  return map;
 }
 
 struct OzTiming {
@@ -611,8 +663,6 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   const size_t smem = (size_t)stages * stage_bytes + 1024;
   FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   OZ_DATA + 1024));
-  const CUtensorMap map_a = digit_map(a);
-  const CUtensorMap map_b = digit_map(b);
   OzArgs args{};
   args.M = a.rows;
   args.N = b.rows;
@@ -624,18 +674,20 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   args.scale_a = a.scale.get();
   args.scale_b = b.scale.get();
   args.flag = flag;
-  for (int d = 0; d < kOzakiMaxSlices; ++d) args.weight[d] = 1.0 / (16129.0 * std::pow(254.0, d));
   const int tiles_m = a.rows_p / OZ_BM, tiles_n = b.rows_p / OZ_BN;
   args.tiles_n = tiles_n;
   const long tiles = lower ? (long)tiles_m * (tiles_m + 1) / 2 : (long)tiles_m * tiles_n;
   // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
   const int kb_total = a.k_p / OZ_BK;
-  const int kb_seg = std::max(1, (int)((2147483647LL / (16129LL * S)) / OZ_BK));
+  args.kb_total = kb_total;
+  const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
+  const int kb_seg = seg_bytes / OZ_BK;
   for (int kb0 = 0; kb0 < kb_total; kb0 += kb_seg) {
     args.kb0 = kb0;
     args.kblocks = std::min(kb_seg, kb_total - kb0);
     args.accumulate = kb0 > 0 ? 1 : 0;
-    ozaki_gemm_kernel<<<(unsigned)tiles, OZ_THREADS, smem, stream>>>(map_a, map_b, args);
+    ozaki_gemm_kernel<<<(unsigned)tiles, OZ_THREADS, smem, stream>>>(a.digits.get(),
+                                                                     b.digits.get(), args);
     count_launch();
     FPLS_LAUNCH("ozaki_gemm_kernel");
   }

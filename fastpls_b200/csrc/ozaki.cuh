@@ -21,9 +21,14 @@ namespace fpls {
 
 constexpr int kOzakiMaxSlices = 7;
 
-// One operand of the split product: digit planes int8 [slices][rows_p][k_p]
-// (row-major, k contiguous, zero padded to rows_p = 128-multiple rows and
-// k_p = 64-multiple columns) and one power-of-two scale per row.
+// One operand of the split product: int8 digits of rows_p (128-multiple) rows
+// x k_p (64-multiple) columns, zero padded, for each of `slices` digit
+// planes, plus one power-of-two scale per row. Layout, tiled for the tensor
+// cores: 4 KB blocks ordered [row tile (128 rows)][k-block (32)][plane], each
+// block 16 row groups x 2 k-chunks of 8 x 16-byte core matrices:
+//   byte (r, k, s) = ((r/128 * k_p/32 + k/32) * slices + s) * 4096
+//                    + (r%128)/8 * 256 + (k%32)/16 * 128 + (r%8) * 16 + k%16
+// so the planes of one k-block of one row tile are a single contiguous run.
 struct OzakiOperand {
   DeviceArray<int8_t> digits;
   DeviceArray<double> scale;
