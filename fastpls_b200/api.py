@@ -313,9 +313,10 @@ def product_digits() -> int:
     return int(_lib.load().fastpls_b200_product_digits())
 
 
-def int8_crossprod(a, b=None, digits=6):
+def int8_crossprod(a, b=None, digits=6, tile_n=0):
     """a^T b (b = None: a^T a, symmetric) by the int8 split product on the
-    tensor cores; a is k x m, b is k x n (FP64)."""
+    tensor cores; a is k x m, b is k x n (FP64). tile_n: 128, 192, 256 or 0
+    (chosen for the shape)."""
     A = _mat(a, np.float64)
     sym = b is None
     B = A if sym else _mat(b, np.float64)
@@ -327,7 +328,7 @@ def int8_crossprod(a, b=None, digits=6):
     err, cap = _lib.error_buffer()
     rc = _lib.load().fastpls_b200_int8_crossprod(
         _p(A), max(k, 1), _p(B), max(k, 1), m, n, k, int(digits), 1 if sym else 0,
-        _p(out), m, err, cap)
+        int(tile_n), _p(out), m, err, cap)
     _lib.check(rc, err)
     return out
 

@@ -337,6 +337,105 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
                  sm + kmax + q + q * q, zs, scratch);
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident form of the score step (n <= RPT * BT): each thread
+// keeps its rows r = threadIdx.x + j BT (j < RPT) of the instance's score
+// vector in registers across the phases, so that Y1 is read from HBM once.
+// Same arithmetic as scores_batched.
+
+// Totals of per-warp partials: part[w * count + c] -> out[c] (c < count).
+__device__ __forceinline__ void warp_partials_total(const double* part, int count, double* out) {
+  __syncthreads();
+  for (int c = threadIdx.x; c < count; c += blockDim.x) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += part[w * count + c];
+    out[c] = tot;
+  }
+  __syncthreads();
+}
+
+template <int RPT>
+__global__ void __launch_bounds__(BT)
+    scores_rows(InstanceView v, const double* Y1, double* Tm, const double* C0,
+                const double* ymean, double* yhat, int yhat_ld, int a,
+                const int* prefix_slot, int prefix_count, double* sse, int* flag) {
+  __shared__ double scratch[32];
+  __shared__ double part[(BT / 32) * kBatchMaxResponses];
+  __shared__ double qs[kBatchMaxResponses];
+  const int i = blockIdx.x;
+  const int f = v.inst_fold[i], b = v.inst_perm[i];
+  const int n = v.n, q = v.q;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double* y = Y1 + (long)i * n;
+  double* t = Tm + (long)i * n;
+  double val[RPT];
+  unsigned train = 0u;
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = threadIdx.x + j * BT;
+    val[j] = 0.0;
+    if (r < n && v.fold_of_row[r] != f + 1) {
+      val[j] = y[r];
+      train |= 1u << j;
+      s += val[j];
+    }
+  }
+  const double mu = v.center ? block_sum(s, scratch) / v.ntrain[f] : 0.0;
+  double ss = 0.0;
+#pragma unroll
+  for (int j = 0; j < RPT; ++j)
+    if (train >> j & 1u) {
+      const double tv = val[j] - mu;
+      ss = fma(tv, tv, ss);
+    }
+  ss = block_sum(ss, scratch);
+  const double tn = sqrt(ss);
+  const bool ok = tn > 0.0 && isfinite(tn);
+  if (!ok && threadIdx.x == 0) flag_error(flag, 1);
+  const double inv = ok ? 1.0 / tn : 0.0;
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = threadIdx.x + j * BT;
+    val[j] = (train >> j & 1u) ? (val[j] - mu) * inv : 0.0;
+    if (r < n) t[r] = val[j];
+  }
+  const double* c0 = C0 + (long)i * n * q;
+  for (int c = 0; c < q; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = threadIdx.x + j * BT;
+      if (r < n) acc = fma(c0[r + (long)c * n], val[j], acc);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) part[warp * q + c] = acc;
+  }
+  warp_partials_total(part, q, qs);
+  // held-out scores and predictions
+  const int* te = v.test_rows + v.test_off[f];
+  const int nte = v.test_off[f + 1] - v.test_off[f];
+  double* yh = yhat + (long)i * yhat_ld * q;
+  const int slot = prefix_slot[a];
+  double err = 0.0;
+  for (int k = threadIdx.x; k < nte; k += blockDim.x) {
+    const int r = te[k];
+    const double tt = (y[r] - mu) * inv;
+    for (int c = 0; c < q; ++c) {
+      const double pv = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
+      yh[k + (long)c * yhat_ld] = pv;
+      if (slot >= 0) {
+        const double e = v.Y[src_row(v, b, r) + (long)c * n] - (ymean[(long)i * q + c] + pv);
+        err = fma(e, e, err);
+      }
+    }
+  }
+  if (slot >= 0) {
+    err = block_sum(err, scratch);
+    if (threadIdx.x == 0) sse[(long)i * prefix_count + slot] = err;
+  }
+}
+
 template <class T>
 __global__ void to_f64(const T* __restrict__ in, long count, double* out) {
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < count;
@@ -406,6 +505,15 @@ __global__ void response_moments(const double* __restrict__ Y, int n, double* ou
     out[2 * blockIdx.x] = s;
     out[2 * blockIdx.x + 1] = ss;
   }
+}
+
+// Rows per thread of the register-resident score kernel for n rows (0: too
+// many, use the general kernel).
+int rows_per_thread(int n) {
+  const int need = (n + BT - 1) / BT;
+  for (int r : {8, 16, 20, 24, 32})
+    if (need <= r) return r;
+  return 0;
 }
 
 }  // namespace
@@ -510,6 +618,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   FPLS_LAUNCH("initial_gram");
 
   const size_t smem_dir = 2 * (size_t)q * q * sizeof(double);
+  const int rpt = rows_per_thread(n);
   // first direction; K u comes from K C0 (no GEMM)
   direction_batched<<<I, BT, smem_dir, s>>>(v, G.get(), C.get(), U.get(), KC0.get(), Y1.get(), flag.get());
   count_launch();
@@ -517,9 +626,24 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   KC0.release();
   for (int a = 0; a < kmax; ++a) {
     if (a > 0) gram_product(U.get(), I, Y1.get(), s);  // Y1 = K u (a = 0: from K C0)
-    scores_batched<<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(),
-                                    yhat.get(), max_test, a, d_slot.get(),
-                                    prefix_count, sse.get(), nullptr, flag.get());
+    switch (rpt) {
+#define FPLS_SCORES(R)                                                                         \
+  case R:                                                                                      \
+    scores_rows<R><<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(), yhat.get(),      \
+                                    max_test, a, d_slot.get(), prefix_count, sse.get(),       \
+                                    flag.get());                                               \
+    break;
+      FPLS_SCORES(8)
+      FPLS_SCORES(16)
+      FPLS_SCORES(20)
+      FPLS_SCORES(24)
+      FPLS_SCORES(32)
+#undef FPLS_SCORES
+      default:
+        scores_batched<<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(), yhat.get(),
+                                        max_test, a, d_slot.get(), prefix_count, sse.get(),
+                                        nullptr, flag.get());
+    }
     count_launch();
     FPLS_LAUNCH("scores_batched");
     if (a + 1 == kmax) break;  // the last deflation is never used

@@ -39,23 +39,37 @@ int& ozaki_slices() {
 namespace {
 
 constexpr int OZ_BM = 128;                 // A rows per tile (TMEM lanes)
-constexpr int OZ_BN = 128;                 // B rows per tile (accumulator columns)
-constexpr int OZ_BK = 32;                  // k bytes per stage (32-byte swizzle span)
+constexpr int OZ_BK = 32;                  // k bytes per stage
 constexpr int OZ_KPAD = 64;                // k padding of the digit planes
-constexpr int OZ_PLANE = OZ_BM * OZ_BK;    // one digit plane block: 4 KB
-constexpr int OZ_DATA = 196 * 1024;        // bytes of stages
+constexpr int OZ_ROWPAD = 64;              // row padding of the digit planes
+constexpr int OZ_TAIL = 256 * OZ_BK;       // bytes past the last plane a tile may read
+constexpr int OZ_A_PLANE = OZ_BM * OZ_BK;  // one A digit plane block: 4 KB
+constexpr int OZ_DATA = 222 * 1024;        // bytes of stages
 constexpr int OZ_MAX_STAGES = 8;
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;
-constexpr int OZ_ACC = 4;                  // accumulators per pass (4 x 128 columns)
 constexpr int OZ_TMEM_COLS = 512;
 constexpr long long OZ_WAIT_CYCLES = 4000000000LL;  // about 2 s
+
+// Tile shapes: BN output columns (B rows) per tile. TMEM holds 512 int32
+// columns: four 128-column accumulators (diagonals per pass) for BN = 128,
+// two for BN = 192 and 256.
+template <int BN>
+struct OzShape {
+  static constexpr int ACC = BN == 128 ? 4 : 2;
+  static constexpr int B_PLANE = BN * OZ_BK;
+  // s32 accumulator, signed int8 A and B, both K-major, N = BN (bits 17-22:
+  // N / 8), M = 128 (bits 24-28: M / 16)
+  static constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) |
+                                    ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256 && ACC * BN <= OZ_TMEM_COLS, "tile");
+};
 
 struct OzArgs {
   int M, N;          // valid rows of A (output rows) and of B (output columns)
   int tiles_n;       // column tiles (rectangular grid)
   int kb0, kblocks;  // k-block range of this launch
-  int kb_total;      // k-blocks per row tile in the digit layout
+  int rows_pa, rows_pb;  // padded rows of the digit layouts of A and B
   int slices, stages, lower, accumulate;
   long ldc;
   double* C;
@@ -129,7 +143,7 @@ __device__ __forceinline__ void tc_fence_after() {
 }
 
 // Shared-memory matrix descriptor: K-major, no swizzle. A plane block holds
-// 16 row groups x 2 k-chunks of 8 x 16-byte core matrices: k-adjacent core
+// row groups of 2 k-chunks x 8 x 16-byte core matrices: k-adjacent core
 // matrices 128 bytes apart (leading offset), row groups 256 bytes apart
 // (stride offset); descriptor version 1.
 __device__ __forceinline__ uint64_t core_desc(uint32_t saddr) {
@@ -137,18 +151,13 @@ __device__ __forceinline__ uint64_t core_desc(uint32_t saddr) {
          ((uint64_t)(256 >> 4) << 32) | ((uint64_t)1 << 46);
 }
 
-// Instruction descriptor: s32 accumulator, signed int8 A and B, both K-major,
-// N = 128 (bits 17-22: N / 8), M = 128 (bits 24-28: M / 16).
-constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) |
-                              ((uint32_t)(OZ_BN >> 3) << 17) | ((uint32_t)(OZ_BM >> 4) << 24);
-
 __device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
-                                          uint32_t accumulate) {
+                                          uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(OZ_IDESC), "r"(accumulate)
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -191,26 +200,30 @@ __device__ __forceinline__ void tmem_wait_ld() {
 
 // Weighted sum over the nd accumulators of a pass for 4 columns of this
 // thread's TMEM lane, smallest weight first (exact int32 -> FP64).
-__device__ __forceinline__ void pass_sum4(uint32_t addr, int nd, const double (&w)[OZ_ACC],
+template <int ACC, int BN>
+__device__ __forceinline__ void pass_sum4(uint32_t addr, int nd, const double (&w)[ACC],
                                           double (&v)[4]) {
-  uint32_t r[OZ_ACC][4];
+  uint32_t r[ACC][4];
 #pragma unroll
-  for (int a = 0; a < OZ_ACC; ++a)
-    if (a < nd) tmem_ld4(addr + (uint32_t)(a * OZ_BN), r[a]);
+  for (int a = 0; a < ACC; ++a)
+    if (a < nd) tmem_ld4(addr + (uint32_t)(a * BN), r[a]);
   tmem_wait_ld();
 #pragma unroll
   for (int j = 0; j < 4; ++j) v[j] = 0.0;
 #pragma unroll
-  for (int a = OZ_ACC - 1; a >= 0; --a)
+  for (int a = ACC - 1; a >= 0; --a)
     if (a < nd) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) v[j] = __dadd_rn(v[j], __dmul_rn(w[a], (double)(int)r[a][j]));
     }
 }
 
+template <int BN>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     ozaki_gemm_kernel(const int8_t* __restrict__ digits_a, const int8_t* __restrict__ digits_b,
                       const OzArgs args) {
+  using Shape = OzShape<BN>;
+  constexpr int ACC = Shape::ACC;
   extern __shared__ uint8_t oz_smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[OZ_MAX_STAGES];
   __shared__ __align__(8) uint64_t empty_bar[OZ_MAX_STAGES];
@@ -223,7 +236,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int tm, tn;
   if (args.lower) {
-    // blockIdx.x = tm (tm + 1) / 2 + tn, tn <= tm
+    // blockIdx.x = tm (tm + 1) / 2 + tn, tn <= tm (BN == OZ_BM)
     const int t = blockIdx.x;
     int r = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
     while ((r + 1) * (r + 2) / 2 <= t) ++r;
@@ -236,8 +249,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   }
   const int S = args.slices;
   const int stages = args.stages;
-  const int stage_bytes = 2 * S * OZ_PLANE;
-  const int npass = (S + OZ_ACC - 1) / OZ_ACC;
+  const int stage_bytes = S * (OZ_A_PLANE + Shape::B_PLANE);
+  const int npass = (S + ACC - 1) / ACC;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < stages; ++i) {
@@ -268,9 +281,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       uint32_t it = 0;
       bool ok = true;
       for (int pass = 0; pass < npass && ok; ++pass) {
-        const int dhi = min(S - 1, pass * OZ_ACC + OZ_ACC - 1);
+        const int dhi = min(S - 1, pass * ACC + ACC - 1);
         const int ns = min(S, dhi + 1);
-        const uint32_t bytes = 2u * ns * OZ_PLANE;
+        const uint32_t bytes = (uint32_t)ns * (OZ_A_PLANE + Shape::B_PLANE);
         for (int kb = 0; kb < args.kblocks; ++kb) {
           const int st = it % stages;
           if (it >= (uint32_t)stages &&
@@ -279,13 +292,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             break;
           }
           uint8_t* a_dst = smem + st * stage_bytes;
-          uint8_t* b_dst = a_dst + S * OZ_PLANE;
+          uint8_t* b_dst = a_dst + S * OZ_A_PLANE;
           mbar_expect_tx(&full_bar[st], bytes);
-          const long kbg = args.kb0 + kb;
-          bulk_load(a_dst, digits_a + ((long)tm * args.kb_total + kbg) * S * OZ_PLANE,
-                    (uint32_t)(ns * OZ_PLANE), &full_bar[st]);
-          bulk_load(b_dst, digits_b + ((long)tn * args.kb_total + kbg) * S * OZ_PLANE,
-                    (uint32_t)(ns * OZ_PLANE), &full_bar[st]);
+          const long slab = (long)(args.kb0 + kb) * S;
+          for (int j = 0; j < ns; ++j) {
+            bulk_load(a_dst + j * OZ_A_PLANE,
+                      digits_a + ((slab + j) * args.rows_pa + (long)tm * OZ_BM) * OZ_BK,
+                      (uint32_t)OZ_A_PLANE, &full_bar[st]);
+            bulk_load(b_dst + j * Shape::B_PLANE,
+                      digits_b + ((slab + j) * args.rows_pb + (long)tn * BN) * OZ_BK,
+                      (uint32_t)Shape::B_PLANE, &full_bar[st]);
+          }
           ++it;
         }
       }
@@ -301,7 +318,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       uint32_t it = 0;
       bool ok = true;
       for (int pass = 0; pass < npass && ok; ++pass) {
-        const int dlo = pass * OZ_ACC, dhi = min(S - 1, dlo + OZ_ACC - 1);
+        const int dlo = pass * ACC, dhi = min(S - 1, dlo + ACC - 1);
         if (pass > 0) {
           if (!mbar_wait(&acc_empty, (pass - 1) & 1, abort, args.flag)) break;
           tc_fence_after();
@@ -314,13 +331,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           }
           tc_fence_after();
           const uint32_t a0 = smem_u32(smem + st * stage_bytes);
-          const uint32_t b0 = a0 + S * OZ_PLANE;
+          const uint32_t b0 = a0 + S * OZ_A_PLANE;
           for (int d = dlo; d <= dhi; ++d)
             for (int s = 0; s <= d; ++s) {
-              const uint64_t ad = core_desc(a0 + s * OZ_PLANE);
-              const uint64_t bd = core_desc(b0 + (d - s) * OZ_PLANE);
+              const uint64_t ad = core_desc(a0 + s * OZ_A_PLANE);
+              const uint64_t bd = core_desc(b0 + (d - s) * Shape::B_PLANE);
               const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
-              tc_mma_i8(tmem + (uint32_t)((d - dlo) * OZ_BN), ad, bd, acc);
+              tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
             }
           tc_commit(&empty_bar[st]);
           ++it;
@@ -334,22 +351,23 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     __syncwarp();
   } else {
     // ------------------------------------------------------------ epilogue
-    // Two epilogue warps per TMEM lane quarter, each owning 64 of the 128
-    // columns of every accumulator. With two passes whose second pass needs
+    // Two epilogue warps per TMEM lane quarter, each owning BN / 2 columns of
+    // every accumulator. For BN = 128 with two passes whose second pass needs
     // at most two accumulators, the first pass's FP64 sums are parked in
     // TMEM, in this thread's own (already read) columns of accumulators 2
-    // and 3; otherwise the first pass goes to C and the second adds to it.
+    // and 3; otherwise each pass after the first adds to C.
+    constexpr int HALF = BN / 2;
     const int quarter = warp & 3;
     const int half = (warp - 2) >> 2;
     const int row = tm * OZ_BM + quarter * 32 + lane;
     const bool row_ok = row < args.M;
     const double sa = row_ok ? args.scale_a[row] : 0.0;
-    const uint32_t mine = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 64);
-    const int col0 = tn * OZ_BN + half * 64;
-    const int nd_last = S - (npass - 1) * OZ_ACC;
-    const bool park = npass == 2 && nd_last <= 2;
+    const uint32_t mine = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * HALF);
+    const int col0 = tn * BN + half * HALF;
+    const int nd_last = S - (npass - 1) * ACC;
+    const bool park = ACC == 4 && npass == 2 && nd_last <= 2;
     for (int pass = 0; pass < npass; ++pass) {
-      const int dlo = pass * OZ_ACC, dhi = min(S - 1, dlo + OZ_ACC - 1);
+      const int dlo = pass * ACC, dhi = min(S - 1, dlo + ACC - 1);
       const int nd = dhi - dlo + 1;
       const bool last = pass + 1 == npass;
       int ready = 0;
@@ -357,18 +375,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       ready = __shfl_sync(0xffffffffu, ready, 0);
       if (!ready) break;
       tc_fence_after();
-      double w[OZ_ACC];
+      double w[ACC];
 #pragma unroll
-      for (int a = 0; a < OZ_ACC; ++a) w[a] = a < nd ? kOzWeight[dlo + a] : 0.0;
+      for (int a = 0; a < ACC; ++a) w[a] = a < nd ? kOzWeight[dlo + a] : 0.0;
 #pragma unroll 2
-      for (int c = 0; c < 16; ++c) {
+      for (int c = 0; c < HALF / 4; ++c) {
         const uint32_t at = mine + (uint32_t)(c * 4);
         double v[4];
         if (last && park) {
           uint32_t p0[4], p1[4];
-          tmem_ld4(at + 2 * OZ_BN, p0);
-          tmem_ld4(at + 3 * OZ_BN, p1);
-          pass_sum4(at, nd, w, v);  // waits for all loads of this thread
+          tmem_ld4(at + 2 * BN, p0);
+          tmem_ld4(at + 3 * BN, p1);
+          pass_sum4<ACC, BN>(at, nd, w, v);  // waits for all loads of this thread
           const double first[4] = {__hiloint2double((int)p0[1], (int)p0[0]),
                                    __hiloint2double((int)p0[3], (int)p0[2]),
                                    __hiloint2double((int)p1[1], (int)p1[0]),
@@ -387,11 +405,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             }
           }
         } else {
-          pass_sum4(at, nd, w, v);
+          pass_sum4<ACC, BN>(at, nd, w, v);
           if (!last && park) {
-            tmem_st4(at + 2 * OZ_BN, (uint32_t)__double2loint(v[0]), (uint32_t)__double2hiint(v[0]),
+            tmem_st4(at + 2 * BN, (uint32_t)__double2loint(v[0]), (uint32_t)__double2hiint(v[0]),
                      (uint32_t)__double2loint(v[1]), (uint32_t)__double2hiint(v[1]));
-            tmem_st4(at + 3 * OZ_BN, (uint32_t)__double2loint(v[2]), (uint32_t)__double2hiint(v[2]),
+            tmem_st4(at + 3 * BN, (uint32_t)__double2loint(v[2]), (uint32_t)__double2hiint(v[2]),
                      (uint32_t)__double2loint(v[3]), (uint32_t)__double2hiint(v[3]));
           } else if (row_ok) {
             const bool add = pass > 0 || args.accumulate;
@@ -428,9 +446,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 // ------------------------------------------------------------------ split
 // Byte offset of (row, k) in plane s of the tiled digit layout (k % 4 == 0
 // keeps a 4-byte group, k % 16 == 0 a 16-byte group, inside one core row).
-__device__ __forceinline__ size_t digit_offset(int row, int k, int s, int slices, int kb_total) {
-  return ((size_t)((row >> 7) * kb_total + (k >> 5)) * slices + s) * 4096 +
-         (size_t)(((row & 127) >> 3) * 256 + ((k & 31) >> 4) * 128 + (row & 7) * 16 + (k & 15));
+__device__ __forceinline__ size_t digit_offset(int row, int k, int s, int slices, int rows_p) {
+  return ((size_t)((k >> 5) * slices + s) * rows_p + (row & ~7)) * OZ_BK +
+         (size_t)(((k & 31) >> 4) * 128 + (row & 7) * 16 + (k & 15));
 }
 // x = 2^e (d0 + d1/254 + ...)/127: scaled by 2^-e (exact) and 127, then
 // rounded to nearest digit by digit.
@@ -460,43 +478,58 @@ __device__ __forceinline__ void row_exponent(double mx, double* inv, double* sca
   }
 }
 
-// Warp per row; rows stored contiguously (row r at src + r * ld).
-__global__ void split_rows_kernel(const double* __restrict__ src, long ld, int rows, int k,
-                                  int rows_p, int k_p, int slices, int8_t* __restrict__ digits,
-                                  double* __restrict__ scale, int* flag) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (row >= rows_p) return;
+// Block per row; rows stored contiguously (row r at src + r * ld). Each
+// thread digitises 16 consecutive values per step and stores one 16-byte
+// core-matrix row per digit plane.
+constexpr int OZ_SPLIT_THREADS = 128;
+
+__global__ void __launch_bounds__(OZ_SPLIT_THREADS)
+    split_rows_kernel(const double* __restrict__ src, long ld, int rows, int k, int k_p,
+                      int slices, int8_t* __restrict__ digits, double* __restrict__ scale,
+                      int* flag) {
+  __shared__ double red[OZ_SPLIT_THREADS / 32];
+  const int row = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool live = row < rows;
   const double* x = src + (long)row * ld;
   double mx = 0.0;
   bool bad = false;
   if (live)
-    for (int c = lane; c < k; c += 32) {
+    for (int c = threadIdx.x; c < k; c += OZ_SPLIT_THREADS) {
       const double v = x[c];
       bad |= !isfinite(v);
       mx = fmax(mx, fabs(v));
     }
 #pragma unroll
   for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (__any_sync(0xffffffffu, bad) && lane == 0) flag_error(flag, 1);
+  if (lane == 0) red[warp] = mx;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) flag_error(flag, 1);
+  mx = red[0];
+#pragma unroll
+  for (int w = 1; w < OZ_SPLIT_THREADS / 32; ++w) mx = fmax(mx, red[w]);
   double inv, sc;
   row_exponent(mx, &inv, &sc);
-  if (lane == 0) scale[row] = sc;
-  const int kb_total = k_p / 32;
-  for (int c4 = lane * 4; c4 < k_p; c4 += 128) {
-    int d[4][kOzakiMaxSlices];
+  if (threadIdx.x == 0) scale[row] = sc;
+  const int rows_p = gridDim.x;
+  for (int c16 = threadIdx.x * 16; c16 < k_p; c16 += OZ_SPLIT_THREADS * 16) {
+    uint32_t pk[kOzakiMaxSlices][4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = c4 + j;
+    for (int s = 0; s < kOzakiMaxSlices; ++s) pk[s][0] = pk[s][1] = pk[s][2] = pk[s][3] = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int c = c16 + j;
       const double v = (live && c < k) ? x[c] : 0.0;
-      split_value(isfinite(v) ? v : 0.0, inv, slices, d[j]);
+      int d[kOzakiMaxSlices];
+      split_value(isfinite(v) ? v : 0.0, inv, slices, d);
+#pragma unroll
+      for (int s = 0; s < kOzakiMaxSlices; ++s)
+        pk[s][j >> 2] |= (uint32_t)(uint8_t)(int8_t)d[s] << (8 * (j & 3));
     }
-    for (int s = 0; s < slices; ++s) {
-      char4 out = make_char4((signed char)d[0][s], (signed char)d[1][s], (signed char)d[2][s],
-                             (signed char)d[3][s]);
-      *reinterpret_cast<char4*>(digits + digit_offset(row, c4, s, slices, kb_total)) = out;
-    }
+#pragma unroll
+    for (int s = 0; s < kOzakiMaxSlices; ++s)
+      if (s < slices)
+        *reinterpret_cast<int4*>(digits + digit_offset(row, c16, s, slices, rows_p)) =
+            make_int4((int)pk[s][0], (int)pk[s][1], (int)pk[s][2], (int)pk[s][3]);
   }
 }
 
@@ -551,7 +584,6 @@ __global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
   double inv = 0.0, sc = 1.0;
   if (i < n) row_exponent(__longlong_as_double((long long)rowmax[i]), &inv, &sc);
   if (blockIdx.y == 0 && (threadIdx.x & 3) == 0) scale[i] = sc;
-  const int kb_total = k_p / 32;
   alignas(16) signed char out[kOzakiMaxSlices][16];
 #pragma unroll 4
   for (int j = 0; j < 16; ++j) {
@@ -561,7 +593,7 @@ __global__ void colmajor_split(const T* __restrict__ X, int n, int p, long ld,
     for (int s = 0; s < kOzakiMaxSlices; ++s) out[s][j] = (signed char)d[s];
   }
   for (int s = 0; s < slices; ++s)
-    *reinterpret_cast<int4*>(digits + digit_offset(i, k0 + kg, s, slices, kb_total)) =
+    *reinterpret_cast<int4*>(digits + digit_offset(i, k0 + kg, s, slices, rows_p)) =
         *reinterpret_cast<const int4*>(out[s]);
 }
 
@@ -572,12 +604,60 @@ void prepare(OzakiOperand& out, int rows, int k, int slices, cudaStream_t s) {
   require(rows >= 0 && k >= 0, "int8 split: invalid shape");
   out.rows = rows;
   out.k = k;
-  out.rows_p = std::max(OZ_BM, round_up(rows, OZ_BM));
+  out.rows_p = std::max(OZ_ROWPAD, round_up(rows, OZ_ROWPAD));
   out.k_p = std::max(OZ_KPAD, round_up(k, OZ_KPAD));
   out.slices = slices;
-  out.digits.reserve((size_t)slices * out.rows_p * out.k_p, s);
+  // a tile may run up to OZ_TAIL bytes past the last plane (rows beyond the
+  // padded ones only feed outputs that are never stored)
+  const size_t body = (size_t)slices * out.rows_p * out.k_p;
+  out.digits.reserve(body + OZ_TAIL, s);
+  FPLS_CHECK(cudaMemsetAsync(out.digits.get() + body, 0, OZ_TAIL, s));
   out.scale.reserve((size_t)out.rows_p, s);
 }
+
+// Tile width for a rectangular product: the tensor core reads A (4 KB) and
+// B (BN * 32 bytes) from shared memory per 128 x BN x 32 step, so a step
+// costs about 128 + BN; the tile count sets the number of waves over the SMs.
+int pick_tile_n(int M, int N) {
+  int best = 128;
+  double best_cost = 0.0;
+  for (int bn : {128, 192, 256}) {
+    const long tiles = (long)ceil_div(M, OZ_BM) * ceil_div(N, bn);
+    const long waves = (tiles + num_sms() - 1) / num_sms();
+    const double cost = (double)waves * (128 + bn) * (bn == 128 ? 1.0 : 1.05);
+    if (bn == 128 || cost < best_cost) {
+      best = bn;
+      best_cost = cost;
+    }
+  }
+  return best;
+}
+
+template <int BN>
+void launch_gemm(const OzakiOperand& a, const OzakiOperand& b, OzArgs args, long tiles,
+                 cudaStream_t stream) {
+  const int S = a.slices;
+  const int stage_bytes = S * (OZ_A_PLANE + OzShape<BN>::B_PLANE);
+  args.stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
+  require(args.stages >= 2, "int8 split product: stages do not fit shared memory");
+  const size_t smem = (size_t)args.stages * stage_bytes + 1024;
+  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel<BN>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+  // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
+  const int kb_total = a.k_p / OZ_BK;
+  const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
+  const int kb_seg = seg_bytes / OZ_BK;
+  for (int kb0 = 0; kb0 < kb_total; kb0 += kb_seg) {
+    args.kb0 = kb0;
+    args.kblocks = std::min(kb_seg, kb_total - kb0);
+    args.accumulate = kb0 > 0 ? 1 : 0;
+    ozaki_gemm_kernel<BN><<<(unsigned)tiles, OZ_THREADS, smem, stream>>>(a.digits.get(),
+                                                                         b.digits.get(), args);
+    count_launch();
+    FPLS_LAUNCH("ozaki_gemm_kernel");
+  }
+}
+
 
 struct OzTiming {
   bool enabled = false;
@@ -615,9 +695,8 @@ void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launch
 void ozaki_split_rows(const double* src, long ld, int rows, int k, int slices,
                       OzakiOperand& out, int* flag, cudaStream_t stream) {
   prepare(out, rows, k, slices, stream);
-  const int warps = 8;
-  split_rows_kernel<<<ceil_div(out.rows_p, warps), 32 * warps, 0, stream>>>(
-      src, ld, rows, k, out.rows_p, out.k_p, slices, out.digits.get(), out.scale.get(), flag);
+  split_rows_kernel<<<out.rows_p, OZ_SPLIT_THREADS, 0, stream>>>(
+      src, ld, rows, k, out.k_p, slices, out.digits.get(), out.scale.get(), flag);
   count_launch();
   FPLS_LAUNCH("split_rows_kernel");
 }
@@ -644,7 +723,7 @@ template void ozaki_split_colmajor<double>(const double*, int, int, long, const 
                                            OzakiOperand&, int*, cudaStream_t);
 
 void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ldc, bool lower,
-                int* flag, cudaStream_t stream) {
+                int* flag, cudaStream_t stream, int tile_n) {
   require(a.slices == b.slices && a.slices >= 1 && a.slices <= kOzakiMaxSlices,
           "int8 split product: operands need the same digit count (1..7)");
   require(a.k == b.k && a.k_p == b.k_p, "int8 split product: operands need the same k");
@@ -658,39 +737,29 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
     FPLS_CHECK(cudaEventRecord(ev0, stream));
   }
   const int S = a.slices;
-  const int stage_bytes = 2 * S * OZ_PLANE;
-  const int stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
-  const size_t smem = (size_t)stages * stage_bytes + 1024;
-  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  OZ_DATA + 1024));
+  const int bn = lower ? 128 : tile_n > 0 ? tile_n : pick_tile_n(a.rows, b.rows);
+  require(bn == 128 || bn == 192 || bn == 256, "int8 split product: tile width 128, 192 or 256");
   OzArgs args{};
   args.M = a.rows;
   args.N = b.rows;
   args.slices = S;
-  args.stages = stages;
   args.lower = lower ? 1 : 0;
   args.ldc = ldc;
   args.C = C;
   args.scale_a = a.scale.get();
   args.scale_b = b.scale.get();
   args.flag = flag;
-  const int tiles_m = a.rows_p / OZ_BM, tiles_n = b.rows_p / OZ_BN;
+  args.rows_pa = a.rows_p;
+  args.rows_pb = b.rows_p;
+  const int tiles_m = ceil_div(a.rows, OZ_BM), tiles_n = ceil_div(b.rows, bn);
   args.tiles_n = tiles_n;
   const long tiles = lower ? (long)tiles_m * (tiles_m + 1) / 2 : (long)tiles_m * tiles_n;
-  // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
-  const int kb_total = a.k_p / OZ_BK;
-  args.kb_total = kb_total;
-  const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
-  const int kb_seg = seg_bytes / OZ_BK;
-  for (int kb0 = 0; kb0 < kb_total; kb0 += kb_seg) {
-    args.kb0 = kb0;
-    args.kblocks = std::min(kb_seg, kb_total - kb0);
-    args.accumulate = kb0 > 0 ? 1 : 0;
-    ozaki_gemm_kernel<<<(unsigned)tiles, OZ_THREADS, smem, stream>>>(a.digits.get(),
-                                                                     b.digits.get(), args);
-    count_launch();
-    FPLS_LAUNCH("ozaki_gemm_kernel");
-  }
+  if (bn == 128)
+    launch_gemm<128>(a, b, args, tiles, stream);
+  else if (bn == 192)
+    launch_gemm<192>(a, b, args, tiles, stream);
+  else
+    launch_gemm<256>(a, b, args, tiles, stream);
   if (lower) mirror_lower_triangle(C, a.rows, ldc, stream);
   if (ev0) {
     FPLS_CHECK(cudaEventRecord(ev1, stream));

@@ -21,14 +21,15 @@ namespace fpls {
 
 constexpr int kOzakiMaxSlices = 7;
 
-// One operand of the split product: int8 digits of rows_p (128-multiple) rows
+// One operand of the split product: int8 digits of rows_p (64-multiple) rows
 // x k_p (64-multiple) columns, zero padded, for each of `slices` digit
 // planes, plus one power-of-two scale per row. Layout, tiled for the tensor
-// cores: 4 KB blocks ordered [row tile (128 rows)][k-block (32)][plane], each
-// block 16 row groups x 2 k-chunks of 8 x 16-byte core matrices:
-//   byte (r, k, s) = ((r/128 * k_p/32 + k/32) * slices + s) * 4096
-//                    + (r%128)/8 * 256 + (k%32)/16 * 128 + (r%8) * 16 + k%16
-// so the planes of one k-block of one row tile are a single contiguous run.
+// cores: slabs ordered [k-block (32 columns)][plane], each slab the rows_p / 8
+// row groups of 2 k-chunks x 8 rows x 16 bytes (core matrices):
+//   byte (r, k, s) = ((k/32 * slices + s) * rows_p + r - r%8) * 32
+//                    + (k%32)/16 * 128 + (r%8) * 16 + k%16
+// so any run of consecutive rows (from a multiple of 8) of one plane and
+// k-block is one contiguous block of 32 bytes per row.
 struct OzakiOperand {
   DeviceArray<int8_t> digits;
   DeviceArray<double> scale;
@@ -48,9 +49,12 @@ void ozaki_split_colmajor(const T* X, int n, int p, long ld,
 
 // C (a.rows x b.rows, column-major, ldc) = A B^T over the split rows of a
 // and b (same k, same slices). lower: only tiles on or below the diagonal
-// are computed (a and b must be the same operand) and mirrored.
+// are computed (a and b must be the same operand) and mirrored. tile_n: the
+// tile width in columns of C (128, 192, 256; 0 picks one for the shape).
+// The FP64 summation order of the epilogue depends on the width (diagonals
+// are combined in passes of four for 128, of two otherwise).
 void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C,
-                long ldc, bool lower, int* flag, cudaStream_t stream);
+                long ldc, bool lower, int* flag, cudaStream_t stream, int tile_n = 0);
 
 // Digit count used by the batched CV engine for its products with the
 // shared Gram (0 selects the FP64 DMMA path). Process-wide setting.

@@ -18,9 +18,12 @@
  *   - a handle owns one CUDA stream; calls are synchronous and a handle is
  *     not safe for concurrent calls. Every handle, whatever the method, is
  *     released with fastpls_resident_simpls_destroy.
- * Arithmetic: all products and reductions are FP64 on the device whatever
- * the storage precision, so results agree with the reference's FP64 CPU
- * path to ~1e-10 relative.
+ * Arithmetic: products and reductions are FP64 on the device whatever the
+ * storage precision, so results agree with the reference's FP64 CPU path to
+ * ~1e-10 relative. The one exception is the batched CV x permutation engine,
+ * whose products with its shared n x n Gram run by default as int8 digit
+ * products on the tensor cores (fastpls_b200_set_product_digits; results
+ * within 1e-5 relative of FP64, ~1e-9 observed; digits = 0 restores FP64).
  */
 #ifndef FASTPLS_B200_H
 #define FASTPLS_B200_H
@@ -215,11 +218,13 @@ FASTPLS_B200_API void fastpls_b200_profile_int8_read(
 /* c (m x n, column-major, ldc) = a^T b by the int8 split product above, for
  * a (k x m, lda) and b (k x n, ldb) column-major FP64 host arrays. With
  * symmetric = 1 (a == b, m == n) only the lower tiles are computed and
- * mirrored. No reference counterpart (test and integration entry for the
- * split product). */
+ * mirrored. tile_n: tile width in columns of c (128, 192 or 256; 0 = chosen
+ * for the shape); the diagonals are combined in FP64 in passes of four for
+ * 128 and of two otherwise. No reference counterpart (test and integration
+ * entry for the split product). */
 FASTPLS_B200_API int fastpls_b200_int8_crossprod(
     const double* a, int lda, const double* b, int ldb, int m, int n, int k,
-    int digits, int symmetric, double* c, int ldc, char* error,
+    int digits, int symmetric, int tile_n, double* c, int ldc, char* error,
     size_t error_capacity);
 
 /* Batched SIMPLS regression CV over the observed responses and

@@ -11,9 +11,10 @@ sides; the FP64 epilogue is reproduced in the same order):
 
   * row scale 2^e with e from frexp(max |row|) (2^e > max |row|);
   * v0 = (x 2^-e) 127, d_s = rint(v_s), v_{s+1} = (v_s - d_s) 254;
-  * diagonals d = s + t <= digits - 1, in passes of four diagonals; within a
-    pass v = sum over d from high to low of w_d acc_d, w_d = 1/(127^2 254^d),
-    acc_d the exact integer sum of the digit-pair products;
+  * diagonals d = s + t <= digits - 1, in passes of four diagonals (tile
+    width 128) or two (widths 192 and 256); within a pass v = sum over d
+    from high to low of w_d acc_d, w_d = 1/(127^2 254^d), acc_d the exact
+    integer sum of the digit-pair products;
   * each pass adds (v 2^e_a) 2^e_b to the result; k is split into segments of
     at most floor((2^31 - 1) / (127^2 digits) / 64) * 64 so that int32 sums
     stay exact.
@@ -53,8 +54,13 @@ def weights(digits):
     return [1.0 / (16129.0 * 254.0 ** d) for d in range(digits)]
 
 
-def product(a_rows, b_rows, digits):
-    """C = A B^T for A (M x K), B (N x K), as the device computes it."""
+def pass_diagonals(tile_n):
+    return 4 if tile_n == 128 else 2
+
+
+def product(a_rows, b_rows, digits, per_pass=PASS):
+    """C = A B^T for A (M x K), B (N x K), as the device computes it with
+    `per_pass` diagonals combined per pass."""
     A, sa = split(a_rows, digits)
     B, sb = split(b_rows, digits)
     M, K = np.shape(a_rows)
@@ -65,8 +71,8 @@ def product(a_rows, b_rows, digits):
     C = None
     for k0 in range(0, kp, seg):
         k1 = min(K, k0 + seg)
-        for lo in range(0, digits, PASS):
-            hi = min(digits - 1, lo + PASS - 1)
+        for lo in range(0, digits, per_pass):
+            hi = min(digits - 1, lo + per_pass - 1)
             v = np.zeros((M, N))
             for d in range(hi, lo - 1, -1):
                 acc = np.zeros((M, N))

@@ -66,3 +66,20 @@ def test_batched_matches_plain_cv():
     plain = api.cv_regression(x, y, folds, pre)
     batched = api.cv_permutation(x, y, folds, None, pre, precision=64, digits=0)
     assert np.allclose(batched["q2"][0], plain["q2"], rtol=1e-10, atol=1e-12)
+
+
+# the register-resident score kernel holds ceil(n / 256) rows per thread in
+# 8/16/20/24/32-row variants; larger n uses the general kernel
+@pytest.mark.parametrize("n", [1500, 4600, 7000, 9000])
+def test_batched_row_variants(n):
+    p = 120
+    x, y = W.latent_regression(n, p, 2, 4, 0.3, 43, dtype=np.float64)
+    folds = W.uneven_folds(n, 4, 43)
+    perms = W.permutations(n, 1, 43)
+    pre = [1, 2, 4, 7]
+    got = api.cv_permutation(x, y, folds, perms, pre, precision=64, digits=0)
+    for b in range(2):
+        yb = y if b == 0 else y[perms[b - 1]]
+        ref = O.cv_regression(x, yb, folds, pre, family=3)
+        for key in ("q2", "rmsd", "observed_r2"):
+            assert np.allclose(got[key][b], ref[key], rtol=1e-9, atol=1e-11), (b, key)

@@ -20,21 +20,30 @@ def _operands(k, m, n, seed):
     return a, b
 
 
+@pytest.mark.parametrize("tile_n", [128, 192, 256])
 @pytest.mark.parametrize("digits", [1, 2, 3, 4, 5, 6, 7])
-def test_bit_exact_against_emulation(digits):
-    a, b = _operands(300, 200, 77, 1 + digits)
-    got = api.int8_crossprod(a, b, digits=digits)
-    ref = Z.product(a.T, b.T, digits)
+def test_bit_exact_against_emulation(digits, tile_n):
+    a, b = _operands(300, 200, 77 + tile_n, 1 + digits)
+    got = api.int8_crossprod(a, b, digits=digits, tile_n=tile_n)
+    ref = Z.product(a.T, b.T, digits, Z.pass_diagonals(tile_n))
     assert np.array_equal(got, ref)
     assert np.all(np.abs(got - a.T @ b) <= Z.error_bound(a.T, b.T, digits))
 
 
+@pytest.mark.parametrize("tile_n", [128, 192, 256])
 @pytest.mark.parametrize("k,m,n", [(1, 1, 1), (64, 128, 128), (65, 129, 257),
-                                   (1000, 3, 300), (0, 5, 6)])
-def test_shapes(k, m, n):
+                                   (1000, 3, 300), (0, 5, 6), (96, 200, 450)])
+def test_shapes(k, m, n, tile_n):
     a, b = _operands(k, m, n, 7)
+    got = api.int8_crossprod(a, b, digits=6, tile_n=tile_n)
+    assert np.array_equal(got, Z.product(a.T, b.T, 6, Z.pass_diagonals(tile_n)))
+
+
+def test_width_choice_stays_accurate():
+    # tile width chosen for the shape (2010 columns: 192); accuracy bound only
+    a, b = _operands(600, 500, 2010, 17)
     got = api.int8_crossprod(a, b, digits=6)
-    assert np.array_equal(got, Z.product(a.T, b.T, 6))
+    assert np.all(np.abs(got - a.T @ b) <= Z.error_bound(a.T, b.T, 6))
 
 
 def test_symmetric_lower_tiles_mirrored():
@@ -48,8 +57,9 @@ def test_symmetric_lower_tiles_mirrored():
 def test_k_segments_keep_int32_exact():
     # digits 7: segments of 19008 k; 20000 needs two launches accumulating C
     a, b = _operands(20000, 40, 24, 11)
-    got = api.int8_crossprod(a, b, digits=7)
-    assert np.array_equal(got, Z.product(a.T, b.T, 7))
+    for tile_n in (128, 192):
+        got = api.int8_crossprod(a, b, digits=7, tile_n=tile_n)
+        assert np.array_equal(got, Z.product(a.T, b.T, 7, Z.pass_diagonals(tile_n)))
 
 
 def test_zero_and_tiny_rows():
