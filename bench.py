@@ -58,6 +58,8 @@ def args_parse():
     ap.add_argument("--digits", type=int, default=6,
                     help="int8 digits per FP64 value in the products with the "
                          "shared Gram (0 = FP64 DMMA GEMMs)")
+    ap.add_argument("--lanes", type=int, default=3,
+                    help="stream lanes of the batched engine (1..4)")
     ap.add_argument("--fp64-steps", type=int, default=2,
                     help="timed steps with FP64 DMMA products, for comparison")
     return ap.parse_args()
@@ -330,7 +332,7 @@ def int8_peak_tops(torch, dev):
         return 4500.0, f"nominal B200 dense int8 (library GEMM unavailable: {exc})"
 
 
-def workload_config(perms, digits=6):
+def workload_config(perms, digits=6, lanes=3):
     return {"workload": f"cv{FOLDS}_perm{perms}_ncomp{NCOMP}_{N}x{P}_f32",
             "n": N, "p": P, "q": Q, "folds": FOLDS, "fold_sizes": "480-520",
             "permutations": perms, "ncomp_path": f"1..{NCOMP}",
@@ -340,7 +342,7 @@ def workload_config(perms, digits=6):
                               "(tcgen05.mma kind::i8, exact int32 accumulation)"
                               if digits > 0 else "FP64 DMMA"),
             "l2": "inputs larger than L2 (X 200 MB FP32, Gram 200 MB FP64)",
-            "parallelism": "replicas"}
+            "parallelism": "replicas", "stream_lanes": lanes}
 
 
 def main():
@@ -421,6 +423,8 @@ def main():
     i8_peak, i8_source = int8_peak_tops(torch, dev)
     lib.fastpls_b200_set_product_digits(a.digits)
     digits = lib.fastpls_b200_product_digits()
+    lib.fastpls_b200_set_batch_lanes(a.lanes)
+    lanes = lib.fastpls_b200_batch_lanes()
 
     clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
     clk = clock_sampler_start(clk_path)
@@ -428,8 +432,6 @@ def main():
         step_device()
     barrier()
     launches0 = lib.fastpls_b200_launch_count()
-    lib.fastpls_b200_profile_gemm(1)
-    lib.fastpls_b200_profile_int8(1)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
     barrier()
     ev[0].record(stream)
@@ -437,18 +439,33 @@ def main():
         step_device()
         ev[s + 1].record(stream)
     barrier()
-    lib.fastpls_b200_profile_gemm(0)
-    lib.fastpls_b200_profile_int8(0)
     launches = lib.fastpls_b200_launch_count() - launches0
     clocks = clock_sampler_stop(clk, clk_path, local)
     step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(a.steps)]
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
+    all_q2 = outs[1].reshape(Pn + 1, k).copy()
+
+    # roofline of the dominant kernel: one more step with a single lane (the
+    # products run alone, not overlapped with the other lane's kernels), each
+    # product bracketed by CUDA events on its stream
+    lib.fastpls_b200_set_batch_lanes(1)
+    lib.fastpls_b200_profile_gemm(1)
+    lib.fastpls_b200_profile_int8(1)
+    r0 = torch.cuda.Event(enable_timing=True)
+    r1 = torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    step_device()
+    r1.record(stream)
+    barrier()
+    lib.fastpls_b200_profile_gemm(0)
+    lib.fastpls_b200_profile_int8(0)
+    lib.fastpls_b200_set_batch_lanes(lanes)
+    roof_step_ms = r0.elapsed_time(r1)
     gms, gfl, gl = C.c_double(0), C.c_double(0), C.c_ulonglong(0)
     lib.fastpls_b200_profile_gemm_read(C.byref(gms), C.byref(gfl), C.byref(gl))
     ims, iops, il = C.c_double(0), C.c_double(0), C.c_ulonglong(0)
     lib.fastpls_b200_profile_int8_read(C.byref(ims), C.byref(iops), C.byref(il))
-    observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
-    all_q2 = outs[1].reshape(Pn + 1, k).copy()
 
     # the same step with FP64 DMMA products, for comparison (and the distance
     # of the int8 split path to it over every instance)
@@ -538,9 +555,10 @@ def main():
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world,
         "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": workload_config(Pn, digits),
+        "dtype": "f64", "data": "synthetic", "config": workload_config(Pn, digits, lanes),
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
-                       "p99": float(np.percentile(step_ms, 99))},
+                       "p99": float(np.percentile(step_ms, 99)),
+                       "steps": [round(v, 3) for v in step_ms]},
         "e2e": {"value": world * fits_per_step / (e2e_ms / 1000.0), "unit": "fits/s",
                 "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -550,7 +568,8 @@ def main():
                       "frac": (i8_achieved / i8_peak) if i8_achieved else None,
                       "peak_source": i8_source,
                       "launches": int(il.value),
-                      "share_of_step": (ims.value / a.steps) / ms_per_step,
+                      "measured_on": "one single-lane step after the timed region",
+                      "share_of_step": ims.value / roof_step_ms,
                       "fp64_equivalent_tflops": (i8_achieved / (digits * (digits + 1) / 2.0))
                       if i8_achieved else None,
                       "fp64_fma_peak_tflops": fp64_peak,
@@ -562,7 +581,8 @@ def main():
                       "peak_source": "measured in this run (FP64 FMA-chain probe); "
                                      "MEASURED_PEAKS.json has no FP64 figure",
                       "launches": int(gl.value),
-                      "share_of_step": (gms.value / a.steps) / ms_per_step,
+                      "measured_on": "one single-lane step after the timed region",
+                      "share_of_step": gms.value / roof_step_ms,
                       "traffic": traffic}),
         "fp64_products": fp64_leg,
         "gpu_launches": int(launches),

@@ -75,6 +75,8 @@ SIGNATURES = {
     "fastpls_b200_profile_gemm_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
     "fastpls_b200_set_product_digits": (None, [_i]),
     "fastpls_b200_product_digits": (_i, []),
+    "fastpls_b200_set_batch_lanes": (None, [_i]),
+    "fastpls_b200_batch_lanes": (_i, []),
     "fastpls_b200_profile_int8": (None, [_i]),
     "fastpls_b200_profile_int8_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
     "fastpls_b200_int8_crossprod": (

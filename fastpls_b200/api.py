@@ -313,6 +313,15 @@ def product_digits() -> int:
     return int(_lib.load().fastpls_b200_product_digits())
 
 
+def set_batch_lanes(lanes: int) -> None:
+    """Stream lanes of the batched engine (1..4); process-wide."""
+    _lib.load().fastpls_b200_set_batch_lanes(int(lanes))
+
+
+def batch_lanes() -> int:
+    return int(_lib.load().fastpls_b200_batch_lanes())
+
+
 def int8_crossprod(a, b=None, digits=6, tile_n=0):
     """a^T b (b = None: a^T a, symmetric) by the int8 split product on the
     tensor cores; a is k x m, b is k x n (FP64). tile_n: 128, 192, 256 or 0

@@ -497,6 +497,10 @@ void fastpls_b200_set_product_digits(int digits) {
 
 int fastpls_b200_product_digits(void) { return ozaki_slices(); }
 
+void fastpls_b200_set_batch_lanes(int lanes) { batch_lanes() = std::max(1, std::min(lanes, 4)); }
+
+int fastpls_b200_batch_lanes(void) { return batch_lanes(); }
+
 void fastpls_b200_profile_int8(int enable) { ozaki_profile_enable(enable != 0); }
 
 void fastpls_b200_profile_int8_read(double* milliseconds, double* int8_ops,

@@ -507,6 +507,15 @@ __global__ void response_moments(const double* __restrict__ Y, int n, double* ou
   }
 }
 
+}  // namespace
+
+int& batch_lanes() {
+  static int lanes = 3;
+  return lanes;
+}
+
+namespace {
+
 // Rows per thread of the register-resident score kernel for n rows (0: too
 // many, use the general kernel).
 int rows_per_thread(int n) {
@@ -555,7 +564,8 @@ void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
 }
 
 template <class T>
-void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out, cudaStream_t s) {
+void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out,
+                                OzakiOperand& rhs_split, cudaStream_t s) {
   if (digits > 0) {
     // K is symmetric: its rows are its columns (contiguous, ld n)
     ozaki_split_rows(rhs, n, cols, n, digits, rhs_split, flag.get(), s);
@@ -575,6 +585,10 @@ void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out, cudaSt
   gemm_f64(g, s);
 }
 
+// The instances of a group run in lanes of their own CUDA stream, enqueued
+// component by component in turn, so that the memory-bound score and
+// deflation kernels of one lane overlap the tensor-core products of the
+// other. Lanes share the Gram and its digits (read only).
 template <class T>
 void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
                              const std::vector<int>& inst_perm,
@@ -582,82 +596,154 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   const int I = (int)inst_fold.size();
   if (I == 0) return;
   const int q = this->q, kmax = this->kmax;
-  DeviceArray<int> d_if(I, s), d_ip(I, s);
-  FPLS_CHECK(cudaMemcpyAsync(d_if.get(), inst_fold.data(), sizeof(int) * I, cudaMemcpyHostToDevice, s));
-  FPLS_CHECK(cudaMemcpyAsync(d_ip.get(), inst_perm.data(), sizeof(int) * I, cudaMemcpyHostToDevice, s));
-  InstanceView v;
-  v.n = n;
-  v.q = q;
-  v.kmax = kmax;
-  v.B = 0;
-  v.center = center ? 1 : 0;
-  v.fold_of_row = d_fold.get();
-  v.inst_fold = d_if.get();
-  v.inst_perm = d_ip.get();
-  v.perms = perms;
-  v.ntrain = d_ntrain.get();
-  v.test_rows = d_test_rows.get();
-  v.test_off = d_test_off.get();
-  v.Y = Y64.get();
-
   const size_t nq = (size_t)n * q;
-  DeviceArray<double> C0(nq * I, s), C(nq * I, s), G((size_t)I * q * (q + 1) / 2, s);
-  DeviceArray<double> ym((size_t)I * q, s), sst(I, s), sse((size_t)I * prefix_count, s);
-  DeviceArray<double> yhat((size_t)I * max_test * q, s);
-  DeviceArray<double> Wb((size_t)I * n * kmax, s), KWb((size_t)I * n * kmax, s);
-  DeviceArray<double> U((size_t)n * I, s), Y1((size_t)n * I, s), KC0(nq * I, s);
-
-  init_instances<<<I, BT, 0, s>>>(v, C0.get(), C.get(), ym.get(), sst.get(),
-                                  yhat.get(), max_test, sse.get(), prefix_count);
-  count_launch();
-  FPLS_LAUNCH("init_instances");
-  // G0 = C0^T K C0 via one product over all instances' C0 columns
-  gram_product(C0.get(), q * I, KC0.get(), s);
-  initial_gram<<<I, BT, 0, s>>>(v, C0.get(), KC0.get(), G.get());
-  count_launch();
-  FPLS_LAUNCH("initial_gram");
+  const int nlanes = std::max(1, std::min(batch_lanes(), I / kLaneMinInstances));
+  struct OwnStream {
+    cudaStream_t st = nullptr;
+    bool own = false;
+    ~OwnStream() {
+      if (own) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
+    }
+  };
+  struct Lane {
+    OwnStream hold;  // destroyed last: every array below is freed on it first
+    int off = 0, cnt = 0;
+    InstanceView v;
+    DeviceArray<int> d_if, d_ip;
+    DeviceArray<double> C0, C, G, ym, sst, sse, yhat, Wb, KWb, U, Y1, KC0;
+    OzakiOperand rhs;
+  };
+  std::vector<Lane> lanes(nlanes);
+  cudaEvent_t ready = nullptr;
+  FPLS_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  struct EventGuard {
+    cudaEvent_t e;
+    ~EventGuard() { cudaEventDestroy(e); }
+  } ready_guard{ready};
+  FPLS_CHECK(cudaEventRecord(ready, s));
 
   const size_t smem_dir = 2 * (size_t)q * q * sizeof(double);
   const int rpt = rows_per_thread(n);
-  // first direction; K u comes from K C0 (no GEMM)
-  direction_batched<<<I, BT, smem_dir, s>>>(v, G.get(), C.get(), U.get(), KC0.get(), Y1.get(), flag.get());
-  count_launch();
-  FPLS_LAUNCH("direction_batched");
-  KC0.release();
+  for (int l = 0; l < nlanes; ++l) {
+    Lane& L = lanes[l];
+    L.off = l * (I / nlanes);
+    L.cnt = l + 1 == nlanes ? I - L.off : I / nlanes;
+    if (nlanes == 1) {
+      L.hold.st = s;
+    } else {
+      FPLS_CHECK(cudaStreamCreateWithFlags(&L.hold.st, cudaStreamNonBlocking));
+      L.hold.own = true;
+      FPLS_CHECK(cudaStreamWaitEvent(L.hold.st, ready, 0));
+    }
+    const cudaStream_t st = L.hold.st;
+    const int c = L.cnt;
+    L.d_if.allocate(c, st);
+    L.d_ip.allocate(c, st);
+    FPLS_CHECK(cudaMemcpyAsync(L.d_if.get(), inst_fold.data() + L.off, sizeof(int) * c,
+                               cudaMemcpyHostToDevice, st));
+    FPLS_CHECK(cudaMemcpyAsync(L.d_ip.get(), inst_perm.data() + L.off, sizeof(int) * c,
+                               cudaMemcpyHostToDevice, st));
+    InstanceView& v = L.v;
+    v.n = n;
+    v.q = q;
+    v.kmax = kmax;
+    v.B = 0;
+    v.center = center ? 1 : 0;
+    v.fold_of_row = d_fold.get();
+    v.inst_fold = L.d_if.get();
+    v.inst_perm = L.d_ip.get();
+    v.perms = perms;
+    v.ntrain = d_ntrain.get();
+    v.test_rows = d_test_rows.get();
+    v.test_off = d_test_off.get();
+    v.Y = Y64.get();
+    L.C0.allocate(nq * c, st);
+    L.C.allocate(nq * c, st);
+    L.G.allocate((size_t)c * q * (q + 1) / 2, st);
+    L.ym.allocate((size_t)c * q, st);
+    L.sst.allocate(c, st);
+    L.sse.allocate((size_t)c * prefix_count, st);
+    L.yhat.allocate((size_t)c * max_test * q, st);
+    L.Wb.allocate((size_t)c * n * kmax, st);
+    L.KWb.allocate((size_t)c * n * kmax, st);
+    L.U.allocate((size_t)n * c, st);
+    L.Y1.allocate((size_t)n * c, st);
+    L.KC0.allocate(nq * c, st);
+
+    init_instances<<<c, BT, 0, st>>>(v, L.C0.get(), L.C.get(), L.ym.get(), L.sst.get(),
+                                     L.yhat.get(), max_test, L.sse.get(), prefix_count);
+    count_launch();
+    FPLS_LAUNCH("init_instances");
+    // G0 = C0^T K C0 via one product over all instances' C0 columns
+    gram_product(L.C0.get(), q * c, L.KC0.get(), L.rhs, st);
+    initial_gram<<<c, BT, 0, st>>>(v, L.C0.get(), L.KC0.get(), L.G.get());
+    count_launch();
+    FPLS_LAUNCH("initial_gram");
+    // first direction; K u comes from K C0 (no GEMM)
+    direction_batched<<<c, BT, smem_dir, st>>>(v, L.G.get(), L.C.get(), L.U.get(), L.KC0.get(),
+                                               L.Y1.get(), flag.get());
+    count_launch();
+    FPLS_LAUNCH("direction_batched");
+    L.KC0.release();
+  }
   for (int a = 0; a < kmax; ++a) {
-    if (a > 0) gram_product(U.get(), I, Y1.get(), s);  // Y1 = K u (a = 0: from K C0)
-    switch (rpt) {
+    for (Lane& L : lanes) {
+      const cudaStream_t st = L.hold.st;
+      const int c = L.cnt;
+      const InstanceView& v = L.v;
+      if (a > 0) gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);  // Y1 = K u
+      switch (rpt) {
 #define FPLS_SCORES(R)                                                                         \
   case R:                                                                                      \
-    scores_rows<R><<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(), yhat.get(),      \
-                                    max_test, a, d_slot.get(), prefix_count, sse.get(),       \
-                                    flag.get());                                               \
+    scores_rows<R><<<c, BT, 0, st>>>(v, L.Y1.get(), L.U.get(), L.C0.get(), L.ym.get(),         \
+                                     L.yhat.get(), max_test, a, d_slot.get(), prefix_count,    \
+                                     L.sse.get(), flag.get());                                 \
     break;
-      FPLS_SCORES(8)
-      FPLS_SCORES(16)
-      FPLS_SCORES(20)
-      FPLS_SCORES(24)
-      FPLS_SCORES(32)
+        FPLS_SCORES(8)
+        FPLS_SCORES(16)
+        FPLS_SCORES(20)
+        FPLS_SCORES(24)
+        FPLS_SCORES(32)
 #undef FPLS_SCORES
-      default:
-        scores_batched<<<I, BT, 0, s>>>(v, Y1.get(), U.get(), C0.get(), ym.get(), yhat.get(),
-                                        max_test, a, d_slot.get(), prefix_count, sse.get(),
-                                        nullptr, flag.get());
+        default:
+          scores_batched<<<c, BT, 0, st>>>(v, L.Y1.get(), L.U.get(), L.C0.get(), L.ym.get(),
+                                           L.yhat.get(), max_test, a, d_slot.get(),
+                                           prefix_count, L.sse.get(), nullptr, flag.get());
+      }
+      count_launch();
+      FPLS_LAUNCH("scores_batched");
+      if (a + 1 == kmax) continue;  // the last deflation is never used
+      // Y1 = K t~ (U holds the masked training scores)
+      gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);
+      deflate_batched<<<c, BT, (kmax + q + 2 * q * q) * sizeof(double), st>>>(
+          v, L.Y1.get(), L.U.get(), L.Wb.get(), L.KWb.get(), L.C.get(), L.G.get(), a, flag.get());
+      count_launch();
+      FPLS_LAUNCH("deflate_batched");
     }
-    count_launch();
-    FPLS_LAUNCH("scores_batched");
-    if (a + 1 == kmax) break;  // the last deflation is never used
-    gram_product(U.get(), I, Y1.get(), s);  // Y1 = K t~ (U holds the masked training scores)
-    deflate_batched<<<I, BT, (kmax + q + 2 * q * q) * sizeof(double), s>>>(
-        v, Y1.get(), U.get(), Wb.get(), KWb.get(), C.get(), G.get(), a, flag.get());
-    count_launch();
-    FPLS_LAUNCH("deflate_batched");
   }
   // collect per-instance sums
   std::vector<double> h_sse((size_t)I * prefix_count), h_sst(I);
-  FPLS_CHECK(cudaMemcpyAsync(h_sse.data(), sse.get(), sizeof(double) * h_sse.size(), cudaMemcpyDeviceToHost, s));
-  FPLS_CHECK(cudaMemcpyAsync(h_sst.data(), sst.get(), sizeof(double) * I, cudaMemcpyDeviceToHost, s));
-  FPLS_CHECK(cudaStreamSynchronize(s));
+  for (Lane& L : lanes) {
+    FPLS_CHECK(cudaMemcpyAsync(h_sse.data() + (size_t)L.off * prefix_count, L.sse.get(),
+                               sizeof(double) * L.cnt * prefix_count, cudaMemcpyDeviceToHost,
+                               L.hold.st));
+    FPLS_CHECK(cudaMemcpyAsync(h_sst.data() + L.off, L.sst.get(), sizeof(double) * L.cnt,
+                               cudaMemcpyDeviceToHost, L.hold.st));
+  }
+  for (Lane& L : lanes) {
+    FPLS_CHECK(cudaStreamSynchronize(L.hold.st));
+    if (L.hold.own) {
+      // later work on the caller's stream follows this lane
+      cudaEvent_t done = nullptr;
+      FPLS_CHECK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+      FPLS_CHECK(cudaEventRecord(done, L.hold.st));
+      FPLS_CHECK(cudaStreamWaitEvent(s, done, 0));
+      cudaEventDestroy(done);
+    }
+  }
   for (int k = 0; k < I; ++k) {
     const int f = inst_fold[k];
     const int b = inst_perm[k] + 1;  // 0 = observed responses

@@ -10,6 +10,10 @@
 namespace fpls {
 
 constexpr int kBatchMaxResponses = 32;
+// Instance groups run as up to batch_lanes() interleaved stream lanes of at
+// least kLaneMinInstances instances each (process-wide setting, 1..4).
+constexpr int kLaneMinInstances = 32;
+int& batch_lanes();
 
 template <class T>
 struct BatchedCv {
@@ -35,8 +39,9 @@ struct BatchedCv {
                  const std::vector<int>& inst_perm, cudaStream_t s);
   // out (n x cols) = K rhs, rhs n x cols column-major (ld n): FP64 DMMA or,
   // when digits > 0, the int8 split product with the digits of K prepared by
-  // form_gram.
-  void gram_product(const double* rhs, int cols, double* out, cudaStream_t s);
+  // form_gram (rhs_split receives the digits of rhs).
+  void gram_product(const double* rhs, int cols, double* out, OzakiOperand& rhs_split,
+                    cudaStream_t s);
 
   const T* X = nullptr;
   const int* perms = nullptr;
@@ -44,7 +49,7 @@ struct BatchedCv {
   int folds = 0, max_test = 1;
   bool center = true;
   int digits = 0;                 // int8 digits per FP64 value (0: FP64 DMMA)
-  OzakiOperand gram_split, rhs_split, x_split;
+  OzakiOperand gram_split, x_split;
   DeviceArray<double> gram, Y64, x64;
   DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag;
 };

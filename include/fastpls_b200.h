@@ -208,6 +208,15 @@ FASTPLS_B200_API int fastpls_b200_fp64_peak(double* tflops, char* error,
 FASTPLS_B200_API void fastpls_b200_set_product_digits(int digits);
 FASTPLS_B200_API int fastpls_b200_product_digits(void);
 
+/* Stream lanes of the batched CV engine (no reference counterpart): the
+ * instances are split into `lanes` (1..4, default 3; each lane at least 32
+ * instances) that run on their own CUDA streams, enqueued component by
+ * component in turn so that one lane's memory-bound score and deflation
+ * kernels overlap another lane's tensor-core products. Results do not
+ * depend on it. Process-wide. */
+FASTPLS_B200_API void fastpls_b200_set_batch_lanes(int lanes);
+FASTPLS_B200_API int fastpls_b200_batch_lanes(void);
+
 /* Benchmark instrumentation of the int8 split products, as for
  * fastpls_b200_profile_gemm; the operation count is the int8 multiply-adds
  * issued (2 M N k per digit pair, M (M + 1) k for a symmetric product). */

@@ -83,3 +83,26 @@ def test_batched_row_variants(n):
         ref = O.cv_regression(x, yb, folds, pre, family=3)
         for key in ("q2", "rmsd", "observed_r2"):
             assert np.allclose(got[key][b], ref[key], rtol=1e-9, atol=1e-11), (b, key)
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 3])
+@pytest.mark.parametrize("digits,rtol", [(0, 1e-9), (6, 1e-5)])
+def test_batched_lanes(digits, rtol, lanes):
+    # 5 folds x (1 + 19) response orders = 100 instances: up to three stream
+    # lanes of >= 32 instances; results must not depend on the lane count
+    old = api.batch_lanes()
+    api.set_batch_lanes(lanes)
+    n, p = 260, 150
+    x, y = W.latent_regression(n, p, 2, 4, 0.3, 47, dtype=np.float64)
+    folds = W.uneven_folds(n, 5, 47)
+    perms = W.permutations(n, 19, 47)
+    pre = [1, 3, 6]
+    try:
+        got = api.cv_permutation(x, y, folds, perms, pre, precision=64, digits=digits)
+    finally:
+        api.set_batch_lanes(old)
+    for b in (0, 7, 19):
+        yb = y if b == 0 else y[perms[b - 1]]
+        ref = O.cv_regression(x, yb, folds, pre, family=3)
+        for key in ("q2", "rmsd", "observed_r2"):
+            assert np.allclose(got[key][b], ref[key], rtol=rtol, atol=rtol * 1e-2), (b, key)
