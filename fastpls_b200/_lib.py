@@ -80,7 +80,7 @@ SIGNATURES = {
     "fastpls_b200_profile_int8": (None, [_i]),
     "fastpls_b200_profile_int8_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
     "fastpls_b200_int8_crossprod": (
-        _i, [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _i, _cp, _sz]),
+        _i, [_vp, _i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _vp, _i, _cp, _sz]),
     "fastpls_b200_simpls_cv_permutation": (
         _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp,
              _vp, _vp, _vp, _cp, _sz]),

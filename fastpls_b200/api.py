@@ -322,10 +322,11 @@ def batch_lanes() -> int:
     return int(_lib.load().fastpls_b200_batch_lanes())
 
 
-def int8_crossprod(a, b=None, digits=6, tile_n=0):
+def int8_crossprod(a, b=None, digits=6, tile_n=0, pair=-1):
     """a^T b (b = None: a^T a, symmetric) by the int8 split product on the
     tensor cores; a is k x m, b is k x n (FP64). tile_n: 128, 192, 256 or 0
-    (chosen for the shape)."""
+    (chosen for the shape); pair: 1 = CTA-pair 256-row tiles, 0 or -1 =
+    single-CTA tiles (-1: automatic)."""
     A = _mat(a, np.float64)
     sym = b is None
     B = A if sym else _mat(b, np.float64)
@@ -337,7 +338,7 @@ def int8_crossprod(a, b=None, digits=6, tile_n=0):
     err, cap = _lib.error_buffer()
     rc = _lib.load().fastpls_b200_int8_crossprod(
         _p(A), max(k, 1), _p(B), max(k, 1), m, n, k, int(digits), 1 if sym else 0,
-        int(tile_n), _p(out), m, err, cap)
+        int(tile_n), int(pair), _p(out), m, err, cap)
     _lib.check(rc, err)
     return out
 

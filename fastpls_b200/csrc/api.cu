@@ -509,13 +509,14 @@ void fastpls_b200_profile_int8_read(double* milliseconds, double* int8_ops,
 }
 
 int fastpls_b200_int8_crossprod(const double* a, int lda, const double* b, int ldb, int m,
-                                int n, int k, int digits, int symmetric, int tile_n, double* c,
-                                int ldc, char* error, size_t error_capacity) {
+                                int n, int k, int digits, int symmetric, int tile_n, int pair,
+                                double* c, int ldc, char* error, size_t error_capacity) {
   return guarded(error, error_capacity, "unknown int8 split product error", [&] {
     if (!a || !b || !c || m < 1 || n < 1 || k < 0 || lda < std::max(k, 1) ||
         ldb < std::max(k, 1) || ldc < m || digits < 1 || digits > kOzakiMaxSlices ||
         (tile_n != 0 && tile_n != 128 && tile_n != 192 && tile_n != 256) ||
-        (symmetric && tile_n != 0 && tile_n != 128))
+        (symmetric && tile_n != 0 && tile_n != 128) || pair < -1 || pair > 1 ||
+        (pair == 1 && (symmetric || tile_n == 128)))
       throw std::invalid_argument("invalid int8 split product input");
     if (symmetric && (a != b || m != n || lda != ldb))
       throw std::invalid_argument("symmetric int8 split product needs one operand");
@@ -545,7 +546,7 @@ int fastpls_b200_int8_crossprod(const double* a, int lda, const double* b, int l
       db.allocate((size_t)ldb * n, s);
       FPLS_CHECK(cudaMemcpyAsync(db.get(), b, sizeof(double) * ldb * n, cudaMemcpyHostToDevice, s));
       ozaki_split_rows(db.get(), ldb, n, k, digits, ob, flag.get(), s);
-      ozaki_gemm(oa, ob, dc.get(), m, false, flag.get(), s, tile_n);
+      ozaki_gemm(oa, ob, dc.get(), m, false, flag.get(), s, tile_n, pair);
     }
     int bad = 0;
     FPLS_CHECK(cudaMemcpyAsync(&bad, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));

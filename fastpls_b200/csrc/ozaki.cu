@@ -443,6 +443,291 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
   }
 }
 
+// ---------------------------------------------------------- CTA-pair helpers
+__device__ __forceinline__ bool mbar_test_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait with cluster-scope acquire (for phases completed by arrivals
+// from the other CTA of the pair).
+__device__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, volatile int* abort, int* flag) {
+  const long long start = clock64();
+  while (!mbar_test_cluster(bar, parity)) {
+    if (*abort) return false;
+    if (clock64() - start > OZ_WAIT_CYCLES) {
+      *abort = 1;
+      flag_error(flag, 4);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// Shared::cluster address of the same shared variable in CTA `rank`.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+// Every thread of both CTAs of the pair.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
+__device__ __forceinline__ void tc_mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                               uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrives (once the pair's MMAs issued so far complete) on the barrier at
+// this address in both CTAs of the pair.
+__device__ __forceinline__ void tc_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+
+// CTA-pair form (tcgen05 cta_group::2): a cluster of two CTAs computes a
+// 256 x BN tile. CTA r of the pair holds A rows 128 r .. 128 r + 127 and
+// B rows (BN / 2) r .. (BN / 2) (r + 1) - 1 of the tile in its own shared
+// memory; the leader (r = 0) issues M = 256 MMAs that read both CTAs' halves
+// and accumulate each CTA's 128 rows x BN columns in that CTA's TMEM, so each
+// SM reads only half of B from shared memory per MMA. Each CTA's producer
+// completes its copies on its own full barrier; in the second CTA a relay
+// thread forwards each completed stage to the leader (peer_full). The
+// leader frees both CTAs' stages, and signals both epilogues, with
+// multicast commits; both epilogues release the accumulators to the
+// leader's acc_empty. Waits are bounded as in the single-CTA kernel; every
+// thread of both CTAs reaches the final cluster barrier.
+template <int BN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
+    ozaki_gemm_pair_kernel(const int8_t* __restrict__ digits_a,
+                           const int8_t* __restrict__ digits_b, const OzArgs args) {
+  using Shape = OzShape<BN>;
+  constexpr int ACC = Shape::ACC;
+  constexpr int B_HALF = (BN / 2) * OZ_BK;  // this CTA's B plane block
+  // s32 accumulator, signed int8 A and B, K-major, N = BN, M = 256
+  constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                             ((uint32_t)(256 >> 4) << 24);
+  static_assert(BN % 32 == 0, "each CTA holds a multiple of 16 B rows");
+  extern __shared__ uint8_t oz_smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[OZ_MAX_STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[OZ_MAX_STAGES];
+  __shared__ __align__(8) uint64_t peer_full[OZ_MAX_STAGES];
+  __shared__ __align__(8) uint64_t acc_full, acc_empty, drain_bar;
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int abort_s;
+  volatile int* abort = &abort_s;
+
+  uint8_t* smem = oz_smem_raw + ((1024 - (smem_u32(oz_smem_raw) & 1023)) & 1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int pair = blockIdx.x >> 1;
+  const int tm = pair / args.tiles_n, tn = pair % args.tiles_n;
+  const int S = args.slices;
+  const int stages = args.stages;
+  const int stage_bytes = S * (OZ_A_PLANE + B_HALF);
+  const int npass = (S + ACC - 1) / ACC;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < stages; ++i) {
+      mbar_init(&full_bar[i], 1);
+      mbar_init(&empty_bar[i], 1);
+      mbar_init(&peer_full[i], 1);
+    }
+    mbar_init(&acc_full, 1);
+    mbar_init(&acc_empty, 2 * 32 * OZ_EPI_WARPS);
+    mbar_init(&drain_bar, 1);
+    abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_s)),
+                 "r"(OZ_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  cluster_sync_all();  // barriers of both CTAs initialised before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------------------------------------------------- producer
+      uint32_t it = 0;
+      bool ok = true;
+      const long a_row = (long)tm * 256 + rank * OZ_BM;
+      const long b_row = (long)tn * BN + rank * (BN / 2);
+      for (int pass = 0; pass < npass && ok; ++pass) {
+        const int dhi = min(S - 1, pass * ACC + ACC - 1);
+        const int ns = min(S, dhi + 1);
+        const uint32_t bytes = (uint32_t)ns * (OZ_A_PLANE + B_HALF);
+        for (int kb = 0; kb < args.kblocks; ++kb) {
+          const int st = it % stages;
+          if (it >= (uint32_t)stages &&
+              !mbar_wait(&empty_bar[st], ((it / stages) - 1) & 1, abort, args.flag)) {
+            ok = false;
+            break;
+          }
+          uint8_t* a_dst = smem + st * stage_bytes;
+          uint8_t* b_dst = a_dst + S * OZ_A_PLANE;
+          mbar_expect_tx(&full_bar[st], bytes);
+          const long slab = (long)(args.kb0 + kb) * S;
+          for (int j = 0; j < ns; ++j) {
+            bulk_load(a_dst + j * OZ_A_PLANE, digits_a + ((slab + j) * args.rows_pa + a_row) * OZ_BK,
+                      (uint32_t)OZ_A_PLANE, &full_bar[st]);
+            bulk_load(b_dst + j * B_HALF, digits_b + ((slab + j) * args.rows_pb + b_row) * OZ_BK,
+                      (uint32_t)B_HALF, &full_bar[st]);
+          }
+          ++it;
+        }
+      }
+      for (uint32_t j = it > (uint32_t)stages ? it - stages : 0; j < it; ++j)
+        mbar_wait(&full_bar[j % stages], (j / stages) & 1, abort, args.flag, true);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0 && leader) {
+      // -------------------------------------------------- MMA issuer (leader)
+      uint32_t it = 0;
+      bool ok = true;
+      for (int pass = 0; pass < npass && ok; ++pass) {
+        const int dlo = pass * ACC, dhi = min(S - 1, dlo + ACC - 1);
+        if (pass > 0) {
+          if (!mbar_wait_cluster(&acc_empty, (pass - 1) & 1, abort, args.flag)) break;
+          tc_fence_after();
+        }
+        for (int kb = 0; kb < args.kblocks; ++kb) {
+          const int st = it % stages;
+          const uint32_t ph = (it / stages) & 1;
+          if (!mbar_wait(&full_bar[st], ph, abort, args.flag) ||
+              !mbar_wait_cluster(&peer_full[st], ph, abort, args.flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + st * stage_bytes);
+          const uint32_t b0 = a0 + S * OZ_A_PLANE;
+          for (int d = dlo; d <= dhi; ++d)
+            for (int s = 0; s <= d; ++s) {
+              const uint64_t ad = core_desc(a0 + s * OZ_A_PLANE);
+              const uint64_t bd = core_desc(b0 + (d - s) * B_HALF);
+              const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+              tc_mma_i8_pair(tmem + (uint32_t)((d - dlo) * BN), ad, bd, IDESC, acc);
+            }
+          tc_commit_pair(&empty_bar[st]);
+          ++it;
+        }
+        if (ok) tc_commit_pair(&acc_full);
+      }
+      tc_commit_pair(&drain_bar);
+      mbar_wait(&drain_bar, 0, abort, args.flag, true);
+    } else if (lane == 0) {
+      // ------------------------------------------ relay (second CTA of the pair)
+      const uint32_t leader_peer_full = cluster_addr(&peer_full[0], 0);
+      uint32_t it = 0;
+      bool ok = true;
+      for (int pass = 0; pass < npass && ok; ++pass)
+        for (int kb = 0; kb < args.kblocks; ++kb) {
+          const int st = it % stages;
+          if (!mbar_wait(&full_bar[st], (it / stages) & 1, abort, args.flag)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_remote(leader_peer_full + (uint32_t)(st * sizeof(uint64_t)));
+          ++it;
+        }
+      // the leader's MMAs write this CTA's TMEM: wait for them before it is freed
+      mbar_wait(&drain_bar, 0, abort, args.flag, true);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    constexpr int HALF = BN / 2;
+    const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int row = tm * 256 + (int)rank * OZ_BM + quarter * 32 + lane;
+    const bool row_ok = row < args.M;
+    const double sa = row_ok ? args.scale_a[row] : 0.0;
+    const uint32_t mine = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * HALF);
+    const int col0 = tn * BN + half * HALF;
+    const uint32_t leader_acc_empty = cluster_addr(&acc_empty, 0);
+    for (int pass = 0; pass < npass; ++pass) {
+      const int dlo = pass * ACC, dhi = min(S - 1, dlo + ACC - 1);
+      const int nd = dhi - dlo + 1;
+      const bool last = pass + 1 == npass;
+      int ready = 0;
+      if (lane == 0) ready = mbar_wait_cluster(&acc_full, pass & 1, abort, args.flag) ? 1 : 0;
+      ready = __shfl_sync(0xffffffffu, ready, 0);
+      if (!ready) break;
+      tc_fence_after();
+      double w[ACC];
+#pragma unroll
+      for (int a = 0; a < ACC; ++a) w[a] = a < nd ? kOzWeight[dlo + a] : 0.0;
+#pragma unroll 2
+      for (int c = 0; c < HALF / 4; ++c) {
+        double v[4];
+        pass_sum4<ACC, BN>(mine + (uint32_t)(c * 4), nd, w, v);
+        if (row_ok) {
+          const bool add = pass > 0 || args.accumulate;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int col = col0 + c * 4 + j;
+            if (col < args.N) {
+              double* dst = args.C + row + (long)col * args.ldc;
+              const double val = __dmul_rn(__dmul_rn(v[j], sa), args.scale_b[col]);
+              *dst = add ? __dadd_rn(*dst, val) : val;
+            }
+          }
+        }
+      }
+      if (!last) {
+        tc_fence_before();
+        mbar_arrive_remote(leader_acc_empty);
+      }
+    }
+  }
+
+  tc_fence_before();
+  cluster_sync_all();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(OZ_TMEM_COLS)
+                 : "memory");
+  }
+}
+
 // ------------------------------------------------------------------ split
 // Byte offset of (row, k) in plane s of the tiled digit layout (k % 4 == 0
 // keeps a 4-byte group, k % 16 == 0 a 16-byte group, inside one core row).
@@ -615,18 +900,35 @@ void prepare(OzakiOperand& out, int rows, int k, int slices, cudaStream_t s) {
   out.scale.reserve((size_t)out.rows_p, s);
 }
 
-// Tile width for a rectangular product: the tensor core reads A (4 KB) and
-// B (BN * 32 bytes) from shared memory per 128 x BN x 32 step, so a step
-// costs about 128 + BN; the tile count sets the number of waves over the SMs.
-int pick_tile_n(int M, int N) {
-  int best = 128;
-  double best_cost = 0.0;
-  for (int bn : {128, 192, 256}) {
-    const long tiles = (long)ceil_div(M, OZ_BM) * ceil_div(N, bn);
-    const long waves = (tiles + num_sms() - 1) / num_sms();
-    const double cost = (double)waves * (128 + bn) * (bn == 128 ? 1.0 : 1.05);
-    if (bn == 128 || cost < best_cost) {
-      best = bn;
+// Tile shape for a rectangular product: waves of tiles over the SMs (pairs
+// over SM pairs) times the measured time of one MMA step of the tile in this
+// kernel (B200, 6 digits, k = 5000; clocks per 128 x BN x 32 step, per pair
+// step for 256-row CTA-pair tiles). The CTA-pair form measured slower than
+// single-CTA tiles at every shape tried, so it runs only when asked for.
+struct TileChoice {
+  int bn;
+  bool pair;
+};
+
+TileChoice pick_tile(int M, int N, int tile_n, int pair) {
+  struct Cand {
+    int bn;
+    bool pair;
+    double step_clk;
+  };
+  const Cand cands[] = {{128, false, 177.0}, {192, false, 276.0}, {256, false, 288.0},
+                        {192, true, 327.0},  {256, true, 342.0}};
+  TileChoice best{128, false};
+  double best_cost = -1.0;
+  const int sms = num_sms();
+  for (const Cand& c : cands) {
+    if (c.pair != (pair == 1)) continue;  // pair < 0 (automatic): single-CTA tiles
+    if (tile_n > 0 && c.bn != tile_n) continue;
+    const long tiles = (long)ceil_div(M, c.pair ? 2 * OZ_BM : OZ_BM) * ceil_div(N, c.bn);
+    const long slots = c.pair ? sms / 2 : sms;
+    const double cost = (double)((tiles + slots - 1) / slots) * c.step_clk;
+    if (best_cost < 0.0 || cost < best_cost) {
+      best = {c.bn, c.pair};
       best_cost = cost;
     }
   }
@@ -667,6 +969,30 @@ struct OzTiming {
 OzTiming& oz_timing() {
   static OzTiming t;
   return t;
+}
+
+template <int BN>
+void launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, OzArgs args, long pairs,
+                      cudaStream_t stream) {
+  const int S = a.slices;
+  const int stage_bytes = S * (OZ_A_PLANE + (BN / 2) * OZ_BK);
+  args.stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
+  require(args.stages >= 2, "int8 split product: stages do not fit shared memory");
+  const size_t smem = (size_t)args.stages * stage_bytes + 1024;
+  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_pair_kernel<BN>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+  const int kb_total = a.k_p / OZ_BK;
+  const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
+  const int kb_seg = seg_bytes / OZ_BK;
+  for (int kb0 = 0; kb0 < kb_total; kb0 += kb_seg) {
+    args.kb0 = kb0;
+    args.kblocks = std::min(kb_seg, kb_total - kb0);
+    args.accumulate = kb0 > 0 ? 1 : 0;
+    ozaki_gemm_pair_kernel<BN><<<(unsigned)(2 * pairs), OZ_THREADS, smem, stream>>>(
+        a.digits.get(), b.digits.get(), args);
+    count_launch();
+    FPLS_LAUNCH("ozaki_gemm_pair_kernel");
+  }
 }
 
 }  // namespace
@@ -723,7 +1049,7 @@ template void ozaki_split_colmajor<double>(const double*, int, int, long, const 
                                            OzakiOperand&, int*, cudaStream_t);
 
 void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ldc, bool lower,
-                int* flag, cudaStream_t stream, int tile_n) {
+                int* flag, cudaStream_t stream, int tile_n, int pair) {
   require(a.slices == b.slices && a.slices >= 1 && a.slices <= kOzakiMaxSlices,
           "int8 split product: operands need the same digit count (1..7)");
   require(a.k == b.k && a.k_p == b.k_p, "int8 split product: operands need the same k");
@@ -737,8 +1063,12 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
     FPLS_CHECK(cudaEventRecord(ev0, stream));
   }
   const int S = a.slices;
-  const int bn = lower ? 128 : tile_n > 0 ? tile_n : pick_tile_n(a.rows, b.rows);
-  require(bn == 128 || bn == 192 || bn == 256, "int8 split product: tile width 128, 192 or 256");
+  require(tile_n == 0 || tile_n == 128 || tile_n == 192 || tile_n == 256,
+          "int8 split product: tile width 128, 192 or 256");
+  require(!(pair == 1 && (lower || tile_n == 128)),
+          "int8 split product: CTA pairs need a rectangular product with 192 or 256 columns");
+  const TileChoice tc = lower ? TileChoice{128, false} : pick_tile(a.rows, b.rows, tile_n, pair);
+  const int bn = tc.bn;
   OzArgs args{};
   args.M = a.rows;
   args.N = b.rows;
@@ -751,15 +1081,24 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   args.flag = flag;
   args.rows_pa = a.rows_p;
   args.rows_pb = b.rows_p;
-  const int tiles_m = ceil_div(a.rows, OZ_BM), tiles_n = ceil_div(b.rows, bn);
+  const int tiles_n = ceil_div(b.rows, bn);
   args.tiles_n = tiles_n;
-  const long tiles = lower ? (long)tiles_m * (tiles_m + 1) / 2 : (long)tiles_m * tiles_n;
-  if (bn == 128)
-    launch_gemm<128>(a, b, args, tiles, stream);
-  else if (bn == 192)
-    launch_gemm<192>(a, b, args, tiles, stream);
-  else
-    launch_gemm<256>(a, b, args, tiles, stream);
+  if (tc.pair) {
+    const long pairs = (long)ceil_div(a.rows, 2 * OZ_BM) * tiles_n;
+    if (bn == 192)
+      launch_gemm_pair<192>(a, b, args, pairs, stream);
+    else
+      launch_gemm_pair<256>(a, b, args, pairs, stream);
+  } else {
+    const int tiles_m = ceil_div(a.rows, OZ_BM);
+    const long tiles = lower ? (long)tiles_m * (tiles_m + 1) / 2 : (long)tiles_m * tiles_n;
+    if (bn == 128)
+      launch_gemm<128>(a, b, args, tiles, stream);
+    else if (bn == 192)
+      launch_gemm<192>(a, b, args, tiles, stream);
+    else
+      launch_gemm<256>(a, b, args, tiles, stream);
+  }
   if (lower) mirror_lower_triangle(C, a.rows, ldc, stream);
   if (ev0) {
     FPLS_CHECK(cudaEventRecord(ev1, stream));

@@ -50,11 +50,15 @@ void ozaki_split_colmajor(const T* X, int n, int p, long ld,
 // C (a.rows x b.rows, column-major, ldc) = A B^T over the split rows of a
 // and b (same k, same slices). lower: only tiles on or below the diagonal
 // are computed (a and b must be the same operand) and mirrored. tile_n: the
-// tile width in columns of C (128, 192, 256; 0 picks one for the shape).
-// The FP64 summation order of the epilogue depends on the width (diagonals
-// are combined in passes of four for 128, of two otherwise).
+// tile width in columns of C (128, 192, 256; 0 picks one for the shape);
+// pair: 1 runs 256-row tiles on CTA pairs (tcgen05 cta_group::2; widths 192
+// and 256), 0 or -1 single-CTA 128-row tiles (-1: the automatic choice; the
+// pair form measured slower, so it is never chosen automatically). The FP64
+// summation order of the epilogue depends only on the width (diagonals are
+// combined in passes of four for 128, of two otherwise).
 void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C,
-                long ldc, bool lower, int* flag, cudaStream_t stream, int tile_n = 0);
+                long ldc, bool lower, int* flag, cudaStream_t stream, int tile_n = 0,
+                int pair = -1);
 
 // Digit count used by the batched CV engine for its products with the
 // shared Gram (0 selects the FP64 DMMA path). Process-wide setting.

@@ -228,13 +228,16 @@ FASTPLS_B200_API void fastpls_b200_profile_int8_read(
  * a (k x m, lda) and b (k x n, ldb) column-major FP64 host arrays. With
  * symmetric = 1 (a == b, m == n) only the lower tiles are computed and
  * mirrored. tile_n: tile width in columns of c (128, 192 or 256; 0 = chosen
- * for the shape); the diagonals are combined in FP64 in passes of four for
- * 128 and of two otherwise. No reference counterpart (test and integration
- * entry for the split product). */
+ * for the shape); pair: 1 = 256-row tiles on CTA pairs (tcgen05
+ * cta_group::2; widths 192, 256; slower than single-CTA tiles on B200, kept
+ * selectable), 0 or -1 = single-CTA 128-row tiles. The diagonals are
+ * combined in FP64 in passes of four for
+ * width 128 and of two otherwise. No reference counterpart (test and
+ * integration entry for the split product). */
 FASTPLS_B200_API int fastpls_b200_int8_crossprod(
     const double* a, int lda, const double* b, int ldb, int m, int n, int k,
-    int digits, int symmetric, int tile_n, double* c, int ldc, char* error,
-    size_t error_capacity);
+    int digits, int symmetric, int tile_n, int pair, double* c, int ldc,
+    char* error, size_t error_capacity);
 
 /* Batched SIMPLS regression CV over the observed responses and
  * `permutation_count` row permutations of them (pls.single.cv /

@@ -20,30 +20,44 @@ def _operands(k, m, n, seed):
     return a, b
 
 
-@pytest.mark.parametrize("tile_n", [128, 192, 256])
+# (tile width, CTA pair): single-CTA 128-row tiles of width 128/192/256 and
+# CTA-pair 256-row tiles (tcgen05 cta_group::2) of width 192/256
+TILES = [(128, 0), (192, 0), (256, 0), (192, 1), (256, 1)]
+
+
+@pytest.mark.parametrize("tile_n,pair", TILES)
 @pytest.mark.parametrize("digits", [1, 2, 3, 4, 5, 6, 7])
-def test_bit_exact_against_emulation(digits, tile_n):
+def test_bit_exact_against_emulation(digits, tile_n, pair):
     a, b = _operands(300, 200, 77 + tile_n, 1 + digits)
-    got = api.int8_crossprod(a, b, digits=digits, tile_n=tile_n)
+    got = api.int8_crossprod(a, b, digits=digits, tile_n=tile_n, pair=pair)
     ref = Z.product(a.T, b.T, digits, Z.pass_diagonals(tile_n))
     assert np.array_equal(got, ref)
     assert np.all(np.abs(got - a.T @ b) <= Z.error_bound(a.T, b.T, digits))
 
 
-@pytest.mark.parametrize("tile_n", [128, 192, 256])
+@pytest.mark.parametrize("tile_n,pair", TILES)
 @pytest.mark.parametrize("k,m,n", [(1, 1, 1), (64, 128, 128), (65, 129, 257),
-                                   (1000, 3, 300), (0, 5, 6), (96, 200, 450)])
-def test_shapes(k, m, n, tile_n):
+                                   (1000, 3, 300), (0, 5, 6), (96, 200, 450),
+                                   (160, 513, 97)])
+def test_shapes(k, m, n, tile_n, pair):
     a, b = _operands(k, m, n, 7)
-    got = api.int8_crossprod(a, b, digits=6, tile_n=tile_n)
+    got = api.int8_crossprod(a, b, digits=6, tile_n=tile_n, pair=pair)
     assert np.array_equal(got, Z.product(a.T, b.T, 6, Z.pass_diagonals(tile_n)))
 
 
 def test_width_choice_stays_accurate():
-    # tile width chosen for the shape (2010 columns: 192); accuracy bound only
+    # tile shape chosen for the shape (2010 columns); accuracy bound only
     a, b = _operands(600, 500, 2010, 17)
     got = api.int8_crossprod(a, b, digits=6)
     assert np.all(np.abs(got - a.T @ b) <= Z.error_bound(a.T, b.T, 6))
+
+
+def test_pair_rejects_symmetric_and_narrow_tiles():
+    a, _ = _operands(64, 40, 1, 19)
+    with pytest.raises(RuntimeError):
+        api.int8_crossprod(a, None, digits=6, pair=1)
+    with pytest.raises(RuntimeError):
+        api.int8_crossprod(a, a, digits=6, tile_n=128, pair=1)
 
 
 def test_symmetric_lower_tiles_mirrored():
@@ -57,8 +71,8 @@ def test_symmetric_lower_tiles_mirrored():
 def test_k_segments_keep_int32_exact():
     # digits 7: segments of 19008 k; 20000 needs two launches accumulating C
     a, b = _operands(20000, 40, 24, 11)
-    for tile_n in (128, 192):
-        got = api.int8_crossprod(a, b, digits=7, tile_n=tile_n)
+    for tile_n, pair in ((128, 0), (192, 0), (256, 1)):
+        got = api.int8_crossprod(a, b, digits=7, tile_n=tile_n, pair=pair)
         assert np.array_equal(got, Z.product(a.T, b.T, 7, Z.pass_diagonals(tile_n)))
 
 
@@ -67,8 +81,9 @@ def test_zero_and_tiny_rows():
     a[:, 5] = 0.0
     a[:, 6] = 1e-300
     b[:, 3] = 0.0
-    got = api.int8_crossprod(a, b, digits=6)
-    assert np.array_equal(got, Z.product(a.T, b.T, 6))
+    for tile_n, pair in ((128, 0), (192, 1)):
+        got = api.int8_crossprod(a, b, digits=6, tile_n=tile_n, pair=pair)
+        assert np.array_equal(got, Z.product(a.T, b.T, 6, Z.pass_diagonals(tile_n)))
     assert np.all(got[5] == 0.0) and np.all(got[:, 3] == 0.0)
 
 
