@@ -117,16 +117,12 @@ __global__ void initial_gram(InstanceView v, const double* C0, const double* KC0
     }
 }
 
-// Dominant direction of instance i: u = C z / sqrt(lambda) (zero on held-out
-// rows, re-centred over the training rows), written to column i of U. When
-// KC0 is given (first component, C = C0) the product K u is formed directly
-// as (K C0) z / sqrt(lambda) into column i of Y1, replacing one GEMM.
-__device__ void direction_body(const InstanceView& v, int i, const double* G,
-                               const double* C, double* U, const double* KC0,
-                               double* Y1, int* flag, double* A, double* E,
-                               double* zs, double* scratch) {
-  const int f = v.inst_fold[i];
-  const int n = v.n, q = v.q;
+// zs = z / sqrt(lambda) for the dominant eigenpair of the instance's q x q
+// Gram (packed lower triangle), sign fixed so the largest |z| entry is
+// positive. A, E: 2 q^2 doubles of shared memory.
+__device__ void dominant_z(const InstanceView& v, int i, const double* G, int* flag,
+                           double* A, double* E, double* zs) {
+  const int q = v.q;
   const double* g = G + (long)i * q * (q + 1) / 2;
   for (int c = threadIdx.x; c < q; c += blockDim.x)
     for (int d = 0; d <= c; ++d) {
@@ -151,6 +147,19 @@ __device__ void direction_body(const InstanceView& v, int i, const double* G,
     for (int k = 0; k < q; ++k) zs[k] = sgn * E[k + best * q] * inv;
   }
   __syncthreads();
+}
+
+// Dominant direction of instance i: u = C z / sqrt(lambda) (zero on held-out
+// rows, re-centred over the training rows), written to column i of U. When
+// KC0 is given (first component, C = C0) the product K u is formed directly
+// as (K C0) z / sqrt(lambda) into column i of Y1, replacing one GEMM.
+__device__ void direction_body(const InstanceView& v, int i, const double* G,
+                               const double* C, double* U, const double* KC0,
+                               double* Y1, int* flag, double* A, double* E,
+                               double* zs, double* scratch) {
+  const int f = v.inst_fold[i];
+  const int n = v.n, q = v.q;
+  dominant_z(v, i, G, flag, A, E, zs);
   const double* c = C + (long)i * n * q;
   double* u = U + (long)i * n;
   double s = 0.0;
@@ -253,88 +262,123 @@ __global__ void scores_batched(InstanceView v, const double* Y1, double* Tm,
   }
 }
 
-// Deflation from Y2 = K t~: Kt = P_F Y2_F ; h = KW^T t ; w = t - W h ;
-// Kw = Kt - KW h ; normalise by sqrt(w^T Kw) ; row = Kw^T C ; C -= w row ;
-// G -= row row^T.
+// Deflation from Y2 = K t~ and the next direction, per instance:
+//   Kt = P_F Y2_F ; h = KW^T t ; w = t - W h ; Kw = Kt - KW h ;
+//   v = sqrt(w^T Kw) ; row = Kw^T C / v ; C -= (w / v) row ; G -= row row^T ;
+//   u = C z / sqrt(lambda) for the dominant eigenpair of G (next direction).
+// W and KW hold the columns unnormalised, with the scale 1/v of column k in
+// wscale[k] (applied where the columns are read), so no pass rewrites them;
+// Kw^T C is accumulated in the same sweep that forms w and Kw, and the C
+// update shares its sweep with u = C z. Dynamic shared memory:
+// 2 q^2 + 2 kmax + q doubles. QMAX >= q bounds the per-thread Kw^T C sums.
+template <int QMAX>
 __global__ void deflate_batched(InstanceView v, const double* Y2,
-                                double* Tm, double* W, double* KW,
+                                double* Tm, double* W, double* KW, double* wscale,
                                 double* C, double* G, int a, int* flag) {
-  extern __shared__ double sm[];  // h (kmax) + row (q) + 2 q^2 (direction)
+  extern __shared__ double sm[];
   __shared__ double scratch[32];
+  __shared__ double rowpart[(BT / 32) * kBatchMaxResponses];
+  __shared__ double zs[kBatchMaxResponses];
   const int i = blockIdx.x;
   const int f = v.inst_fold[i];
   const int n = v.n, q = v.q, kmax = v.kmax;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  double* A = sm;
+  double* E = A + q * q;
+  double* h = E + q * q;      // h_k * wscale_k (kmax)
+  double* hsc = h + kmax;     // scratch for the warp-per-column dots (kmax)
+  double* row = hsc + kmax;   // q
   const double* y = Y2 + (long)i * n;
-  const double* t = Tm + (long)i * n;
+  double* t = Tm + (long)i * n;
   double* w = W + (long)i * n * kmax;
   double* kw = KW + (long)i * n * kmax;
+  const double* ws = wscale + (long)i * kmax;
   double* c = C + (long)i * n * q;
-  double* h = sm;
-  double* row = sm + kmax;
   double s = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x)
     if (v.fold_of_row[r] != f + 1) s += y[r];
   const double mu = v.center ? block_sum(s, scratch) / v.ntrain[f] : 0.0;
-  // h = KW^T t (warp per column)
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  // h = KW^T t (warp per column), times the column scales
   for (int k = warp; k < a; k += warps) {
     double acc = 0.0;
 #pragma unroll 4
     for (int r = lane; r < n; r += 32) acc = fma(kw[r + (long)k * n], t[r], acc);
     acc = warp_sum(acc);
-    if (lane == 0) h[k] = acc;
+    if (lane == 0) hsc[k] = acc;
   }
   __syncthreads();
+  for (int k = threadIdx.x; k < a; k += blockDim.x) h[k] = hsc[k] * ws[k] * ws[k];
+  __syncthreads();
+  // w = t - W h, Kw = (Y2 - mu) - KW h (training rows), stored unscaled;
+  // w^T Kw and Kw^T C in the same sweep
   double* wa = w + (long)a * n;
   double* kwa = kw + (long)a * n;
   double vv = 0.0;
+  double rc[QMAX];
+#pragma unroll
+  for (int cc = 0; cc < QMAX; ++cc) rc[cc] = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double wr = 0.0, kr = 0.0;
     if (v.fold_of_row[r] != f + 1) {
-      double wr = t[r], kr = y[r] - mu;
+      wr = t[r];
+      kr = y[r] - mu;
 #pragma unroll 4
       for (int k = 0; k < a; ++k) {
         wr = fma(-w[r + (long)k * n], h[k], wr);
         kr = fma(-kw[r + (long)k * n], h[k], kr);
       }
-      wa[r] = wr;
-      kwa[r] = kr;
       vv = fma(wr, kr, vv);
-    } else {
-      wa[r] = 0.0;
-      kwa[r] = 0.0;
+#pragma unroll
+      for (int cc = 0; cc < QMAX; ++cc)
+        if (cc < q) rc[cc] = fma(kr, c[r + (long)cc * n], rc[cc]);
     }
+    wa[r] = wr;
+    kwa[r] = kr;
   }
   vv = block_sum(vv, scratch);
   const double vn = sqrt(vv);
   const bool ok = vn > 0.0 && isfinite(vn);
   if (!ok && threadIdx.x == 0) flag_error(flag, 1);
   const double inv = ok ? 1.0 / vn : 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    wa[r] *= inv;
-    kwa[r] *= inv;
-  }
+#pragma unroll
+  for (int cc = 0; cc < QMAX; ++cc)
+    if (cc < q) {
+      const double part = warp_sum(rc[cc]);
+      if (lane == 0) rowpart[warp * q + cc] = part;
+    }
   __syncthreads();
-  for (int k = warp; k < q; k += warps) {
-    double acc = 0.0;
-    for (int r = lane; r < n; r += 32) acc = fma(kwa[r], c[r + (long)k * n], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) row[k] = acc;
+  if (threadIdx.x < q) {
+    double tot = 0.0;
+    for (int ww = 0; ww < warps; ++ww) tot += rowpart[ww * q + threadIdx.x];
+    row[threadIdx.x] = tot * inv;
   }
+  if (threadIdx.x == 0) wscale[(long)i * kmax + a] = inv;
   __syncthreads();
-  for (int r = threadIdx.x; r < n; r += blockDim.x) {
-    const double wr = wa[r];
-    for (int k = 0; k < q; ++k) c[r + (long)k * n] = fma(-wr, row[k], c[r + (long)k * n]);
-  }
   if (threadIdx.x == 0) {
     double* g = G + (long)i * q * (q + 1) / 2;
     for (int cc = 0; cc < q; ++cc)
       for (int d = 0; d <= cc; ++d) g[cc * (cc + 1) / 2 + d] -= row[cc] * row[d];
   }
   __syncthreads();
-  // next component's direction, written over this instance's t~ column
-  __shared__ double zs[kBatchMaxResponses];
-  direction_body(v, i, G, C, Tm, nullptr, nullptr, flag, sm + kmax + q,
-                 sm + kmax + q + q * q, zs, scratch);
+  dominant_z(v, i, G, flag, A, E, zs);
+  // C -= (w / v) row^T and the next direction u = C z (over t~)
+  double su = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double wr = wa[r] * inv;
+    double u = 0.0;
+    for (int cc = 0; cc < q; ++cc) {
+      const double cv = fma(-wr, row[cc], c[r + (long)cc * n]);
+      c[r + (long)cc * n] = cv;
+      u = fma(cv, zs[cc], u);
+    }
+    t[r] = u;
+    su += u;
+  }
+  if (v.center) {
+    const double mu_u = block_sum(su, scratch) / v.ntrain[f];
+    for (int r = threadIdx.x; r < n; r += blockDim.x)
+      if (v.fold_of_row[r] != f + 1) t[r] -= mu_u;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -613,7 +657,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     int off = 0, cnt = 0;
     InstanceView v;
     DeviceArray<int> d_if, d_ip;
-    DeviceArray<double> C0, C, G, ym, sst, sse, yhat, Wb, KWb, U, Y1, KC0;
+    DeviceArray<double> C0, C, G, ym, sst, sse, yhat, Wb, KWb, Ws, U, Y1, KC0;
     OzakiOperand rhs;
   };
   std::vector<Lane> lanes(nlanes);
@@ -669,6 +713,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     L.yhat.allocate((size_t)c * max_test * q, st);
     L.Wb.allocate((size_t)c * n * kmax, st);
     L.KWb.allocate((size_t)c * n * kmax, st);
+    L.Ws.allocate((size_t)c * kmax, st);
     L.U.allocate((size_t)n * c, st);
     L.Y1.allocate((size_t)n * c, st);
     L.KC0.allocate(nq * c, st);
@@ -718,8 +763,15 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
       if (a + 1 == kmax) continue;  // the last deflation is never used
       // Y1 = K t~ (U holds the masked training scores)
       gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);
-      deflate_batched<<<c, BT, (kmax + q + 2 * q * q) * sizeof(double), st>>>(
-          v, L.Y1.get(), L.U.get(), L.Wb.get(), L.KWb.get(), L.C.get(), L.G.get(), a, flag.get());
+      const size_t smem_defl = (2 * (size_t)q * q + 2 * (size_t)kmax + q) * sizeof(double);
+      if (q <= 4)
+        deflate_batched<4><<<c, BT, smem_defl, st>>>(v, L.Y1.get(), L.U.get(), L.Wb.get(),
+                                                     L.KWb.get(), L.Ws.get(), L.C.get(),
+                                                     L.G.get(), a, flag.get());
+      else
+        deflate_batched<kBatchMaxResponses><<<c, BT, smem_defl, st>>>(
+            v, L.Y1.get(), L.U.get(), L.Wb.get(), L.KWb.get(), L.Ws.get(), L.C.get(), L.G.get(),
+            a, flag.get());
       count_launch();
       FPLS_LAUNCH("deflate_batched");
     }

@@ -106,3 +106,20 @@ def test_batched_lanes(digits, rtol, lanes):
         ref = O.cv_regression(x, yb, folds, pre, family=3)
         for key in ("q2", "rmsd", "observed_r2"):
             assert np.allclose(got[key][b], ref[key], rtol=rtol, atol=rtol * 1e-2), (b, key)
+
+
+@pytest.mark.parametrize("q", [1, 5])
+def test_batched_response_counts(q):
+    # the deflation keeps its Kw^T C sums in registers for q <= 4 and has a
+    # general form for larger q
+    n, p = 220, 130
+    x, y = W.latent_regression(n, p, q, 4, 0.3, 53, dtype=np.float64)
+    folds = W.uneven_folds(n, 4, 53)
+    perms = W.permutations(n, 2, 53)
+    pre = [1, 2, 5]
+    got = api.cv_permutation(x, y, folds, perms, pre, precision=64, digits=0)
+    for b in range(3):
+        yb = y if b == 0 else y[perms[b - 1]]
+        ref = O.cv_regression(x, yb, folds, pre, family=3)
+        for key in ("q2", "rmsd", "observed_r2"):
+            assert np.allclose(got[key][b], ref[key], rtol=1e-9, atol=1e-11), (b, key)
