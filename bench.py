@@ -275,7 +275,6 @@ def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
     srv = lib_api.Server(budget_bytes=150 * 10**9, workers=workers)
     tickets = []
     fit_tickets = {}
-    waited = {}
     submit_t = []
     t0 = time.perf_counter()
     next_t = t0
@@ -289,16 +288,14 @@ def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
                                ncomp=r["ncomp"], method=r["method"], precision=32, **kw(r))
             fit_tickets[id(r)] = t
         else:
+            # queued behind its model's fit if that is still running
             src = r["src"]
-            ft = fit_tickets[id(src)]
-            if ft not in waited:  # a prediction needs its model: wait for that fit
-                waited[ft] = srv.wait(ft)
-            t = srv.submit_predict(ft, r["x"], [src["ncomp"]])
+            t = srv.submit_predict(fit_tickets[id(src)], r["x"], [src["ncomp"]])
         tickets.append(t)
         submit_t.append(time.perf_counter())
     lat = []
     for t in tickets:
-        _, qms, sms = waited[t] if t in waited else srv.wait(t)
+        _, qms, sms = srv.wait(t)
         lat.append(qms + sms)
     served_time = time.perf_counter() - t0
     for t in fit_tickets.values():
@@ -594,12 +591,13 @@ def main():
     if rank == 0 and a.served_requests > 0:
         from fastpls_b200 import api as fapi
         reqs = served_workload(a.served_requests)
-        run_served(fapi, reqs[:20], mean_gap_ms=0.0)  # warm-up
+        run_served(fapi, reqs[:20], mean_gap_ms=0.0, workers=8)  # warm-up
         plain = run_plain(fapi, reqs)
-        sweep = [run_served(fapi, reqs, mean_gap_ms=g_) for g_ in (2.0, 0.5, 0.0)]
+        sweep = [run_served(fapi, reqs, mean_gap_ms=g_, workers=8) for g_ in (2.0, 0.5, 0.0)]
         line["served"] = dict(
             requests=len(reqs), fits=sum(1 for r in reqs if r["kind"] == "fit"),
-            workers=4, arrivals="Poisson; mean gap swept (0 = all at once)",
+            workers=8, arrivals="Poisson; mean gap swept (0 = all at once); predictions "
+                                "queue behind their model's fit in the server",
             sweep=sweep, **plain,
             saturated_served_over_plain=sweep[-1]["fits_per_s"] / plain["plain_fits_per_s"])
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

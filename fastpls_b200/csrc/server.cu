@@ -50,6 +50,7 @@ struct Request {
   int rows = 0;
   std::vector<int> prefixes;
   int lda = 0;
+  bool deferred = false;  // submitted before its model existed (fit still queued or running)
   // results
   bool done = false;
   int status = 0;  // 0 ok, 1 error
@@ -113,10 +114,20 @@ class Server {
     r->submitted = Clock::now();
     if (r->kind == kPredict) {
       auto it = models_.find(r->model);
-      if (it == models_.end()) throw std::invalid_argument("unknown model ticket");
-      if (it->second.p != r->fit.p || it->second.precision != r->precision)
-        throw std::invalid_argument("prediction rows do not match the model's columns or precision");
-      r->footprint = predict_footprint(r->rows, it->second);
+      if (it != models_.end()) {
+        if (it->second.p != r->fit.p || it->second.precision != r->precision)
+          throw std::invalid_argument("prediction rows do not match the model's columns or precision");
+        r->footprint = predict_footprint(r->rows, it->second);
+      } else {
+        // a prediction may be queued behind the fit of its model: it is
+        // admitted once that fit has produced the model
+        auto ft = all_.find(r->model);
+        if (ft == all_.end() || ft->second->kind != kFit || ft->second->done)
+          throw std::invalid_argument("unknown model ticket");
+        if (ft->second->fit.p != r->fit.p || ft->second->precision != r->precision)
+          throw std::invalid_argument("prediction rows do not match the model's columns or precision");
+        r->deferred = true;
+      }
     } else {
       r->footprint = fit_footprint(*r);
       if (r->footprint + resident_footprint(*r) > budget_)
@@ -180,9 +191,17 @@ class Server {
       Model* model = nullptr;
       if (r->kind == kPredict) {
         auto mit = models_.find(r->model);
-        if (mit == models_.end()) {  // released while queued
+        if (mit == models_.end()) {
+          auto ft = all_.find(r->model);
+          if (ft != all_.end() && ft->second->kind == kFit && !ft->second->done) {
+            ++it;  // its fit is still queued or running
+            continue;
+          }
+          // the fit failed, or the model was released while this waited
           r->status = 1;
-          r->error = "unknown model ticket";
+          r->error = ft != all_.end() && ft->second->status != 0
+                         ? "the model's fit failed: " + ft->second->error
+                         : "unknown model ticket";
           r->started = r->finished = Clock::now();
           r->done = true;
           it = pending_.erase(it);
@@ -190,6 +209,10 @@ class Server {
           continue;
         }
         model = &mit->second;
+        if (r->deferred) {
+          r->footprint = predict_footprint(r->rows, *model);
+          r->deferred = false;
+        }
         // one batch per model at a time: requests arriving meanwhile queue
         // up and join the next batch
         if (model->busy > 0) {
@@ -207,6 +230,10 @@ class Server {
       if (model) {
         for (auto jt = pending_.begin(); jt != pending_.end();) {
           Request* o = *jt;
+          if (o->kind == kPredict && o->model == r->model && o->deferred) {
+            o->footprint = predict_footprint(o->rows, *model);
+            o->deferred = false;
+          }
           if (o->kind == kPredict && o->model == r->model && o->lda == r->lda &&
               o->prefixes == r->prefixes && in_use_ + fp + o->footprint <= budget_) {
             batch.push_back(o);

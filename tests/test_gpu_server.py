@@ -83,3 +83,42 @@ def test_server_rejects_oversized_and_unknown():
     with pytest.raises(Exception):
         srv.submit_predict(12345, x, [1])
     srv.close()
+
+
+def test_predictions_queued_behind_their_fits():
+    # predictions submitted before their model exists wait in the server's
+    # queue (not on the client) and give the standalone results
+    srv = api.Server(budget_bytes=150 * 10**9, workers=3)
+    fits, preds = {}, {}
+    for i, (method, n, p, q, a, cls) in enumerate(SPECS):
+        x, y, lab = _data(i, method, n, p, q, cls)
+        fits[i] = srv.submit_fit(x, y, labels=lab, classes=q if cls else None, ncomp=a,
+                                 method=method, precision=32, **_kw(method, p))
+        xt, _, _ = _data(70 + i, method, 29, p, q, False)
+        preds[i] = srv.submit_predict(fits[i], xt, [a])
+    for i, t in preds.items():
+        got, _, _ = srv.wait(t)
+        method, n, p, q, a, cls = SPECS[i]
+        x, y, lab = _data(i, method, n, p, q, cls)
+        xt, _, _ = _data(70 + i, method, 29, p, q, False)
+        alone = api.fit_resident(x, y, labels=lab, classes=q if cls else None, ncomp=a,
+                                 method=method, precision=32, **_kw(method, p))
+        assert np.array_equal(got, alone.predict_path(xt, [a])), i
+        alone.close()
+    for t in fits.values():
+        srv.wait(t)
+        srv.release(t)
+    srv.close()
+
+
+def test_prediction_behind_a_failing_fit_reports_it():
+    srv = api.Server(budget_bytes=150 * 10**9, workers=1)
+    x = np.zeros((60, 12), dtype=np.float32)  # no spread: the fit fails on the device
+    y = np.ones((60, 1), dtype=np.float32)
+    t = srv.submit_fit(x, y, ncomp=2, method="simpls", precision=32)
+    pt = srv.submit_predict(t, np.zeros((5, 12), dtype=np.float32), [1])
+    with pytest.raises(Exception):
+        srv.wait(t)
+    with pytest.raises(Exception, match="fit failed|unknown model"):
+        srv.wait(pt)
+    srv.close()
