@@ -113,8 +113,12 @@ __global__ void finish_moments(const double* __restrict__ sum,
 }
 
 // Unpack the packed lower-triangular Gram, diagonalise, emit z / sqrt(lambda).
+// The `count` dominant eigenpairs of the m x m right Gram (packed lower
+// triangle), by decreasing eigenvalue (ties: lower index first):
+// zs[k + j m] = z_j / sqrt(lambda_j), sign fixed so the largest-magnitude
+// entry of z_j is positive; lambda_out = lambda_0.
 __global__ void direction_kernel(const double* __restrict__ gpk, int m,
-                                 double* zs, double* lambda_out, int* flag) {
+                                 double* zs, double* lambda_out, int* flag, int count) {
   extern __shared__ double sm[];
   double* A = sm;
   double* E = sm + m * m;
@@ -128,19 +132,23 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
   jacobi_eigen_warp(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
-    int best = 0;
-    for (int k = 1; k < m; ++k)
-      if (A[k + k * m] > A[best + best * m]) best = k;
-    const double lam = A[best + best * m];
-    if (!(lam > 0.0) || !isfinite(lam)) flag_error(flag, 1);
-    const double inv = (lam > 0.0 && isfinite(lam)) ? 1.0 / sqrt(lam) : 0.0;
-    // deterministic sign: largest-magnitude entry of z positive
-    int arg = 0;
-    for (int k = 1; k < m; ++k)
-      if (fabs(E[k + best * m]) > fabs(E[arg + best * m])) arg = k;
-    const double sgn = E[arg + best * m] < 0.0 ? -1.0 : 1.0;
-    for (int k = 0; k < m; ++k) zs[k] = sgn * E[k + best * m] * inv;
-    if (lambda_out) *lambda_out = lam;
+    unsigned long long taken = 0ull;  // m <= 64
+    for (int j = 0; j < count; ++j) {
+      int best = -1;
+      for (int k = 0; k < m; ++k)
+        if (!((taken >> k) & 1ull) && (best < 0 || A[k + k * m] > A[best + best * m])) best = k;
+      taken |= 1ull << best;
+      const double lam = A[best + best * m];
+      if (!(lam > 0.0) || !isfinite(lam)) flag_error(flag, 1);
+      const double inv = (lam > 0.0 && isfinite(lam)) ? 1.0 / sqrt(lam) : 0.0;
+      // deterministic sign: largest-magnitude entry of z positive
+      int arg = 0;
+      for (int k = 1; k < m; ++k)
+        if (fabs(E[k + best * m]) > fabs(E[arg + best * m])) arg = k;
+      const double sgn = E[arg + best * m] < 0.0 ? -1.0 : 1.0;
+      for (int k = 0; k < m; ++k) zs[k + j * m] = sgn * E[k + best * m] * inv;
+      if (lambda_out && j == 0) *lambda_out = lam;
+    }
   }
 }
 
@@ -422,7 +430,7 @@ void dominant_direction(const double* S, int p, int m, const double* gpk,
   const size_t smem_dir = 2 * (size_t)m * m * sizeof(double);
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
-  direction_kernel<<<1, 64, smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get());
+  direction_kernel<<<1, 64, smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get(), 1);
   s_times_z<<<std::min<unsigned>(ceil_div(p, TB), 4 * num_sms()), TB, 0, s>>>(S, p, m, zs, w);
   count_launch(2);
   FPLS_LAUNCH("dominant_direction");
@@ -468,7 +476,7 @@ void gram_of_columns(double* S, int p, int m, double* gpk, Workspace& ws,
 template <class T>
 void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
-                DeviceModel& model, Workspace& ws, cudaStream_t stream) {
+                DeviceModel& model, Workspace& ws, cudaStream_t stream, int block) {
   require(m >= 1 && m <= kMaxResponses, "SIMPLS supports 1..64 responses or classes");
   const int a_max = components;
   ws.ensure(n, p, m, a_max, stream);
@@ -510,14 +518,36 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
   gram_of_columns(S.get(), p, m, gpk, ws, stream);
 
+  // Candidate blocks (the reference's block refresh): the directions of
+  // `use` consecutive components are the leading left singular vectors of S
+  // at the start of the block, r_j = S_block z_j / sqrt(lambda_j), not
+  // recomputed from the deflated S in between.
+  block = std::max(1, std::min(block, std::min(a_max, std::min(p, m))));
+  DeviceArray<double> zblk, Sblk;
+  if (block > 1) {
+    zblk.allocate((size_t)m * block, stream);
+    Sblk.allocate((size_t)p * m, stream);
+  }
+  int use = 0, jb = 0;
   for (int a = 0; a < a_max; ++a) {
-    direction_kernel<<<1, 64, smem_dir, stream>>>(
-        gpk, m, zs, scal + 3, ws.flag.get());
-    rvec_kernel<<<g1, TB, 0, stream>>>(S.get(), p, m, zs, model.mean.get(),
-                                       model.scale.get(), r, rt, part, ctr + 0,
-                                       scal);
-    count_launch(2);
-    FPLS_LAUNCH("direction/rvec");
+    if (jb == use) {
+      use = std::min(block, a_max - a);
+      jb = 0;
+      direction_kernel<<<1, 64, smem_dir, stream>>>(gpk, m, use > 1 ? zblk.get() : zs, scal + 3,
+                                                    ws.flag.get(), use);
+      count_launch();
+      FPLS_LAUNCH("direction_kernel");
+      if (use > 1)
+        FPLS_CHECK(cudaMemcpyAsync(Sblk.get(), S.get(), sizeof(double) * p * m,
+                                   cudaMemcpyDeviceToDevice, stream));
+    }
+    rvec_kernel<<<g1, TB, 0, stream>>>(use > 1 ? Sblk.get() : S.get(), p, m,
+                                       use > 1 ? zblk.get() + (size_t)jb * m : zs,
+                                       model.mean.get(), model.scale.get(), r, rt, part,
+                                       ctr + 0, scal);
+    ++jb;
+    count_launch();
+    FPLS_LAUNCH("rvec_kernel");
     double* tcol = model.T.get() + (size_t)a * n;
     xr_product<T>(X, n, p, ld, rt, p, 1, scal, tcol, n, ws.stream_partial, stream);
     tstats_kernel<<<std::min<unsigned>(ceil_div(n, TB), 2 * num_sms()), TB, 0, stream>>>(
@@ -595,7 +625,7 @@ void predict_from_scores(const DeviceModel& model, const double* scores,
                                      double*, double*, int*, cudaStream_t);   \
   template void fit_simpls<T>(const T*, int, int, long, const double*,        \
                               const double*, int, int, int, DeviceModel&,     \
-                              Workspace&, cudaStream_t);                      \
+                              Workspace&, cudaStream_t, int);                 \
   template void project_rows<T>(const DeviceModel&, const T*, int, long, int, \
                                 double*, long, Workspace&, cudaStream_t);   \
   template void compute_crossprod<T>(const T*, int, int, long, const double*, \

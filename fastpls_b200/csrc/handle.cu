@@ -366,7 +366,8 @@ class TypedHandle final : public ResidentHandle {
       fit_kernelpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, rq_.kernel,
                        rq_.gamma, rq_.degree, rq_.coef0, model_, ws_, design_, stream_);
     else
-      fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
+      fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_,
+                    simpls_block_size(n, p, q, a, cls, std::is_same<T, float>::value));
     raise_on_flag(ws_, stream_, rq_.method == kPlssvd
         ? "resident PLS-SVD failed: invalid labels, decomposition or score Gram"
         : rq_.method == kOpls ? "resident CUDA OPLS filtering failed"

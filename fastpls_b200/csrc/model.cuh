@@ -3,6 +3,9 @@
 
 #include "common.cuh"
 
+#include <algorithm>
+#include <type_traits>
+
 namespace fpls {
 
 constexpr int kMaxResponses = 64;  // m x m direction eigenproblem in one block
@@ -56,7 +59,26 @@ void prepare_responses(const T* Y, const int* labels, int n, int m,
 template <class T>
 void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
-                DeviceModel& model, Workspace& ws, cudaStream_t stream);
+                DeviceModel& model, Workspace& ws, cudaStream_t stream,
+                int block = 1);
+
+// Candidate block size of a SIMPLS fit (src/cuda_resident_simpls.cuh:144-153):
+// a classification fit with q <= 2048 classes, at least 4 components and
+// n p q >= 5e8 takes min(64, components, p, q) directions from one
+// decomposition; an FP32 regression fit whose p x q cross-covariance exceeds
+// 512 MiB in FP32 and has at least 4 components takes min(8, components, p, q);
+// every other fit refreshes the direction once per component.
+inline int simpls_block_size(int n, int p, int q, int components,
+                             bool classification, bool fp32) {
+  const double work = (double)n * (double)p * (double)q;
+  const int cap = std::min(components, std::min(p, q));
+  if (classification && q <= 2048 && components >= 4 && work >= 5.0e8)
+    return std::max(1, std::min(64, cap));
+  if (!classification && fp32 && components >= 4 &&
+      (double)p * (double)q * 4.0 > 512.0 * 1024.0 * 1024.0)
+    return std::max(1, std::min(8, cap));
+  return 1;
+}
 
 // PLS-SVD fit (exact SVD of the m-column cross-product).
 template <class T>

@@ -270,7 +270,9 @@ void fit_opls(const T* X, int n, int p, long ld, const double* Yc,
     FPLS_LAUNCH("opls filter deflation");
   }
   // predictive SIMPLS on the filtered, already standardised predictors
-  fit_simpls<double>(xf, n, p, n, Yc, ycsum, m, components, 3, model, ws, s);
+  fit_simpls<double>(xf, n, p, n, Yc, ycsum, m, components, 3, model, ws, s,
+                     simpls_block_size(n, p, m, components, model.classification,
+                                       std::is_same<T, float>::value));
   for (int c = f - 1; c >= 0; --c) {
     fold_filter<<<std::min(components, 4 * num_sms()), TB, 0, s>>>(
         model.R.get(), p, components, Wo.get() + (size_t)c * p, Po.get() + (size_t)c * p);
@@ -326,7 +328,9 @@ void fit_kernelpls(const T* X, int n, int p, long ld, const double* Yc,
                                                       model.kcol_means.get(), model.kcol_means.get() + n);
   count_launch(4);
   FPLS_LAUNCH("kernel gram");
-  fit_simpls<double>(design.get(), n, n, n, Yc, ycsum, m, components, 3, model, ws, s);
+  fit_simpls<double>(design.get(), n, n, n, Yc, ycsum, m, components, 3, model, ws, s,
+                     simpls_block_size(n, n, m, components, model.classification,
+                                       std::is_same<T, float>::value));
   model.in_mean = std::move(mean);
   model.in_scale = std::move(scale);
   model.kernel_kind = kind;

@@ -305,9 +305,17 @@ template <class T>
 void column_moments(const T* X, int n, int p, long ld, const double* Yc, int m,
                     double* sum, double* sumsq, double* cross,
                     DeviceArray<double>& scratch, cudaStream_t stream) {
-  require(m <= 32, "column_moments supports at most 32 response columns");
-  xtv_dispatch<T, true>(X, n, p, ld, Yc, n, m, cross, p, sum, sumsq, scratch,
+  // the first pass carries the column sums and sums of squares with up to 32
+  // response columns; further columns go in passes of 32 without them
+  const int w0 = std::min(m, 32);
+  xtv_dispatch<T, true>(X, n, p, ld, Yc, n, w0, cross, p, sum, sumsq, scratch,
                         stream);
+  for (int c0 = 32; c0 < m; c0 += 32) {
+    const int w = std::min(32, m - c0);
+    xtv_dispatch<T, false>(X, n, p, ld, Yc + (long)c0 * n, n, w,
+                           cross + (long)c0 * p, p, nullptr, nullptr, scratch,
+                           stream);
+  }
 }
 
 template <class T>

@@ -31,7 +31,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = [
-    "column_statistics", "simpls_fit", "simpls_predict", "simpls_project",
+    "column_statistics", "simpls_fit", "simpls_block_size", "simpls_predict", "simpls_project",
     "plssvd_fit", "plssvd_predict", "lda_train", "lda_discriminants",
     "row_argmax", "topk", "response_sums", "cv_regression", "opls_fit",
     "opls_predict", "kernelpls_fit", "kernelpls_predict",
@@ -106,13 +106,39 @@ def _dominant_left(s: np.ndarray) -> np.ndarray:
     return u[:, 0].copy()
 
 
+def simpls_block_size(n, p, q, components, classification, fp32=False):
+    """Candidate directions taken from one decomposition of S.
+
+    Rule of the CUDA resident SIMPLS (src/cuda_resident_simpls.cuh:144-153):
+    classification with q <= 2048 classes, components >= 4 and n p q >= 5e8
+    -> min(64, components, p, q); FP32 regression whose p x q cross-covariance
+    exceeds 512 MiB and components >= 4 -> min(8, components, p, q); else 1.
+    The R/CPU path (simpls_candidate_block_size, simpls.hpp:43-62, called with
+    a maximum of 64 at src/r_api.cpp:1155) gives the same classification
+    blocks; its regression blocks start at p q > 64 Mi elements instead.
+    """
+    work = float(n) * float(p) * float(q)
+    cap = min(int(components), int(p), int(q))
+    if classification and q <= 2048 and components >= 4 and work >= 5.0e8:
+        return max(1, min(64, cap))
+    if (not classification and fp32 and components >= 4
+            and float(p) * float(q) * 4.0 > 512.0 * 1024.0 * 1024.0):
+        return max(1, min(8, cap))
+    return 1
+
+
 def simpls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1,
-               reorthogonalize=False):
+               reorthogonalize=False, block=None, classification=None):
     """Sequential SIMPLS (fit_simpls_preprocessed, simpls.hpp:479-763).
 
-    Per component (simpls.hpp:547-756): r = dominant left singular vector of
-    the deflated cross-product S; t = Xs r; r, t /= ||t||; p = Xs^T t;
-    q = S0^T r; v = p - V (V^T p) (twice when reorthogonalize);
+    Directions come in candidate blocks (simpls.hpp:547-567): at the start of
+    a block of ``use`` components the leading ``use`` left singular vectors of
+    the deflated cross-product S are computed once, and component j of the
+    block takes candidate j as its r (simpls.hpp:588-595). ``block`` defaults
+    to ``simpls_block_size`` (1 outside large classification fits, which is
+    the per-component dominant direction).
+    Per component (simpls.hpp:588-756): t = Xs r; r, t /= ||t||;
+    p = Xs^T t; q = S0^T r; v = p - V (V^T p) (twice when reorthogonalize);
     v /= ||v||; S -= v (v^T S). The FP64 CPU path runs with
     reorthogonalize = False (src/r_api.cpp:1179 and :1408-1411).
     Returns a dict with R (p x a), Q (m x a), V (p x a), T (n x a),
@@ -122,38 +148,51 @@ def simpls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1,
     n, p = xs.shape
     m = s0.shape[1]
     a = min(int(ncomp), p, max(n - 1, 1))
+    if classification is None:
+        classification = labels is not None
+    if block is None:
+        block = simpls_block_size(n, p, m, a, classification)
     R = np.zeros((p, a))
     Q = np.zeros((m, a))
     V = np.zeros((p, a))
     T = np.zeros((n, a))
     s = s0.copy()
     done = 0
-    for k in range(a):
-        r = _dominant_left(s)
-        t = xs @ r
-        if reorthogonalize and k > 0:
-            for _ in range(2):
-                proj = T[:, :k].T @ t
-                t = t - T[:, :k] @ proj
-                r = r - R[:, :k] @ proj
-        tn = np.linalg.norm(t)
-        if not np.isfinite(tn) or tn <= 0:
-            break
-        t = t / tn
-        r = r / tn
-        ld = xs.T @ t
-        q = s0.T @ r
-        v = ld.copy()
-        for _ in range(2 if reorthogonalize else 1):
-            if k:
-                v = v - V[:, :k] @ (V[:, :k].T @ v)
-        vn = np.linalg.norm(v)
-        if not np.isfinite(vn) or vn <= 0:
-            break
-        v = v / vn
-        s = s - np.outer(v, v @ s)
-        R[:, k], Q[:, k], V[:, k], T[:, k] = r, q, v, t
-        done = k + 1
+    k = 0
+    stopped = False
+    while k < a and not stopped:
+        use = max(1, min(int(block), a - k, p, m))
+        u, _, _ = np.linalg.svd(s, full_matrices=False)
+        candidates = u[:, :use].copy()
+        for j in range(use):
+            r = candidates[:, j].copy()
+            t = xs @ r
+            if reorthogonalize and k > 0:
+                for _ in range(2):
+                    proj = T[:, :k].T @ t
+                    t = t - T[:, :k] @ proj
+                    r = r - R[:, :k] @ proj
+            tn = np.linalg.norm(t)
+            if not np.isfinite(tn) or tn <= 0:
+                stopped = True
+                break
+            t = t / tn
+            r = r / tn
+            ld = xs.T @ t
+            q = s0.T @ r
+            v = ld.copy()
+            for _ in range(2 if reorthogonalize else 1):
+                if k:
+                    v = v - V[:, :k] @ (V[:, :k].T @ v)
+            vn = np.linalg.norm(v)
+            if not np.isfinite(vn) or vn <= 0:
+                stopped = True
+                break
+            v = v / vn
+            s = s - np.outer(v, v @ s)
+            R[:, k], Q[:, k], V[:, k], T[:, k] = r, q, v, t
+            k += 1
+            done = k
     return dict(R=R[:, :done], Q=Q[:, :done], V=V[:, :done], T=T[:, :done],
                 centre=centre, scale=scale, ymean=ymean)
 
@@ -237,7 +276,8 @@ def opls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1, north=1):
         xf = xf - np.outer(to, po)
         Wo.append(wo)
         Po.append(po)
-    inner = simpls_fit(xf, yd, ncomp=ncomp, scaling=3)
+    inner = simpls_fit(xf, yd, ncomp=ncomp, scaling=3,
+                       classification=labels is not None)
     R = inner["R"].copy()
     for wo, po in zip(reversed(Wo), reversed(Po)):
         R = R - np.outer(wo, R.T @ po)
@@ -269,7 +309,8 @@ def kernelpls_fit(x, y=None, labels=None, classes=None, ncomp=2, scaling=1,
     cm = K.mean(axis=0)
     g = cm.mean()
     Kc = K - cm[:, None] - cm[None, :] + g
-    inner = simpls_fit(Kc, yd, ncomp=ncomp, scaling=3)
+    inner = simpls_fit(Kc, yd, ncomp=ncomp, scaling=3,
+                       classification=labels is not None)
     inner.update(reference=xs, kcol=cm, kgrand=g, kind=kind, gamma=gamma,
                  degree=degree, coef0=coef0, centre=centre, scale=scale)
     return inner

@@ -1,0 +1,84 @@
+"""Candidate blocks of SIMPLS directions on the device vs the FP64 oracle.
+
+Classification fits with n p q >= 5e8, q <= 2048 and at least 4 components take
+min(64, components, p, q) directions from one decomposition of the
+cross-product (src/cuda_resident_simpls.cuh:144-190): the single fit, each
+CV fold fit, and the inner SIMPLS of OPLS and kernel PLS
+(src/cuda_resident_special.cuh:315, :492)."""
+import numpy as np
+import pytest
+
+from fastpls_b200 import api, workloads as W
+from oracle import pls_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+Q = 50
+
+
+def _data(n, p, seed):
+    return W.latent_classification(n, p, Q, 50, 0.5, seed, dtype=np.float64)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_simpls_block_fit(precision):
+    n, p, a = 4000, 2500, 8
+    x, lab = _data(n, p, 61)
+    xt, _ = _data(300, p, 62)
+    assert O.simpls_block_size(n, p, Q, a, True) == a
+    if precision == 32:
+        x = x.astype(np.float32).astype(np.float64)
+        xt = xt.astype(np.float32).astype(np.float64)
+    model = api.fit_resident(x, labels=lab, classes=Q, ncomp=a, precision=precision)
+    ref = O.simpls_fit(x, labels=lab, classes=Q, ncomp=a, scaling=1)
+    pre = [1, 3, 4, 8]
+    pred = model.predict_path(xt, pre).astype(np.float64)
+    tol = 1e-9 if precision == 64 else 2e-5
+    for j, k in enumerate(pre):
+        assert O.rel_err(pred[j], O.simpls_predict(ref, xt, k)) < tol
+    if precision == 64:
+        got = model.classify_path(xt, pre, top=1)
+        for j, k in enumerate(pre):
+            assert np.array_equal(got[j][:, 0], O.row_argmax(O.simpls_predict(ref, xt, k)))
+        R = model.export(0)
+        assert O.rel_err(O.align_signs(R, ref["R"]), ref["R"]) < 1e-9
+    model.close()
+
+
+def test_cv_classification_block_folds():
+    n, p = 5000, 3000
+    x, lab = _data(n, p, 63)
+    folds = W.uneven_folds(n, 5, 63)
+    pre = [1, 4, 6]
+    for f in range(1, 6):
+        assert O.simpls_block_size(int((folds != f).sum()), p, Q, 6, True) == 6
+    got = api.cv_classification(x, lab, Q, folds, pre, store_predictions=True)
+    ref = O.cv_classification(x, lab, Q, folds, pre, store_predictions=True)
+    assert np.array_equal(got["predictions"], ref["predictions"])
+    assert np.allclose(got["metrics"], ref["metrics"])
+
+
+def test_opls_classification_block():
+    n, p, a = 4000, 2500, 6
+    x, lab = _data(n, p, 64)
+    xt, _ = _data(200, p, 65)
+    model = api.fit_resident(x, labels=lab, classes=Q, ncomp=a, method="opls", north=1)
+    ref = O.opls_fit(x, labels=lab, classes=Q, ncomp=a, north=1)
+    pred = model.predict_path(xt, [2, 6])
+    for j, k in enumerate([2, 6]):
+        assert O.rel_err(pred[j], O.opls_predict(ref, xt, k)) < 1e-9
+    model.close()
+
+
+def test_kernelpls_classification_block():
+    n, p, a = 3200, 120, 6
+    x, lab = _data(n, p, 66)
+    xt, _ = _data(150, p, 67)
+    assert O.simpls_block_size(n, n, Q, a, True) == a
+    model = api.fit_resident(x, labels=lab, classes=Q, ncomp=a, method="kernelpls",
+                             kernel="rbf", gamma=1e-4)
+    ref = O.kernelpls_fit(x, labels=lab, classes=Q, ncomp=a, kind=2, gamma=1e-4)
+    pred = model.predict_path(xt, [3, 6])
+    for j, k in enumerate([3, 6]):
+        assert O.rel_err(pred[j], O.kernelpls_predict(ref, xt, k)) < 1e-9
+    model.close()
