@@ -38,6 +38,42 @@ def _dtype(precision):
     return np.float32 if precision == 32 else np.float64
 
 
+def to_bf16(a) -> np.ndarray:
+    """BF16 bit patterns (uint16) of ``a``, rounded to nearest even from FP32.
+
+    Predictors in precision 16 are handed to the library as these bits; a
+    uint16 array is taken as bits already."""
+    a = np.asarray(a)
+    if a.dtype == np.uint16:
+        return a
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+    nan = (u & 0x7F800000) == 0x7F800000
+    r = ((u + np.uint32(0x7FFF) + ((u >> 16) & np.uint32(1))) >> 16).astype(np.uint16)
+    # NaN and infinity keep their class (truncation keeps the quiet bit set)
+    return np.where(nan, (u >> 16).astype(np.uint16) | np.where((u & 0x7FFFFF) != 0, 0x40, 0).astype(np.uint16), r)
+
+
+def from_bf16(bits) -> np.ndarray:
+    """FP32 values of BF16 bit patterns."""
+    b = np.ascontiguousarray(bits, dtype=np.uint16)
+    return (b.astype(np.uint32) << 16).view(np.float32)
+
+
+def _xmat(a, precision):
+    """Predictor matrix in the storage type of ``precision`` (16 = BF16 bits)."""
+    if precision == 16:
+        b = to_bf16(a)
+        if b.ndim == 1:
+            b = b[:, None]
+        return np.asfortranarray(b)
+    return _mat(a, _dtype(precision))
+
+
+def _odtype(precision):
+    """Responses and results: FP32 for BF16 predictors."""
+    return np.float32 if precision == 16 else _dtype(precision)
+
+
 def has_cuda() -> bool:
     """True when a CUDA device is visible (has_cuda(), R/native_api.R:601)."""
     return _lib.load().fastpls_b200_device_count() > 0
@@ -71,7 +107,11 @@ class ResidentModel:
 
     @property
     def dtype(self):
-        return _dtype(self.precision)
+        """Type of responses and results (FP32 when predictors are BF16)."""
+        return _odtype(self.precision)
+
+    def _x(self, x):
+        return _xmat(x, self.precision)
 
     def close(self):
         if not self._freed and self.handle:
@@ -108,7 +148,7 @@ class ResidentModel:
         return self.export(2)
 
     def predict_path(self, x, prefixes, lda=False) -> np.ndarray:
-        x = _mat(x, self.dtype)
+        x = self._x(x)
         pre = np.ascontiguousarray(prefixes, dtype=np.int32)
         rows = x.shape[0]
         out = np.zeros(rows * self.q * len(pre), dtype=self.dtype)
@@ -120,7 +160,7 @@ class ResidentModel:
         return out.reshape((len(pre), self.q, rows)).transpose(0, 2, 1)
 
     def classify_path(self, x, prefixes, lda=False, top=1, responses=False):
-        x = _mat(x, self.dtype)
+        x = self._x(x)
         pre = np.ascontiguousarray(prefixes, dtype=np.int32)
         rows = x.shape[0]
         labels = np.zeros(rows * top * len(pre), dtype=np.int32)
@@ -142,7 +182,7 @@ class ResidentModel:
         return lab
 
     def project(self, x, prefix):
-        x = _mat(x, self.dtype)
+        x = self._x(x)
         rows = x.shape[0]
         out = np.zeros((rows, prefix), dtype=self.dtype, order="F")
         err, cap = _lib.error_buffer()
@@ -152,7 +192,7 @@ class ResidentModel:
         return out
 
     def response_sums(self, x, y=None, labels=None, prefix=None):
-        x = _mat(x, self.dtype)
+        x = self._x(x)
         rows = x.shape[0]
         prefix = self.ncomp if prefix is None else prefix
         yy = None if y is None else _mat(y, self.dtype)
@@ -186,9 +226,12 @@ def fit_resident(X, Y=None, labels=None, classes=None, ncomp=2,
                  scaling="centering", method="simpls", precision=64,
                  oversample=32, power=5, seed=1, retain_scores=True,
                  north=1, kernel="rbf", gamma=None, degree=3, coef0=1.0):
-    """Fit one resident model through ``fastpls_resident_<method>_create``."""
-    dt = _dtype(precision)
-    x = _mat(X, dt)
+    """Fit one resident model through ``fastpls_resident_<method>_create``.
+
+    ``precision`` 32 or 64 as in the reference; 16 stores the predictors as
+    BF16 (``to_bf16``) with FP32 responses and results, all arithmetic FP64."""
+    dt = _odtype(precision)
+    x = _xmat(X, precision)
     n, p = x.shape
     lib = _lib.load()
     err, cap = _lib.error_buffer()

@@ -321,7 +321,7 @@ void* fastpls_resident_simpls_create(const void* x, const void* y, const int* la
                                      int scaling, int oversample, int power, int retain_scores,
                                      unsigned long long seed, char* error, size_t error_capacity) {
   return guarded_create(error, error_capacity, "unknown resident CUDA fitting error", [&]() -> void* {
-    if (!x || (precision != 32 && precision != 64))
+    if (!x || (precision != 32 && precision != 64 && precision != 16))
       throw std::invalid_argument("invalid resident matrix or precision");
     if (retain_scores != 0 && retain_scores != 1)
       throw std::invalid_argument("invalid resident score-retention request");
@@ -335,7 +335,7 @@ void* fastpls_resident_plssvd_create(const void* x, const void* y, const int* la
                                      int scaling, int oversample, int power, int retain_scores,
                                      unsigned long long seed, char* error, size_t error_capacity) {
   return guarded_create(error, error_capacity, "unknown resident CUDA PLS-SVD fitting error", [&]() -> void* {
-    if (!x || (precision != 32 && precision != 64))
+    if (!x || (precision != 32 && precision != 64 && precision != 16))
       throw std::invalid_argument("invalid resident matrix or precision");
     if (retain_scores != 0 && retain_scores != 1)
       throw std::invalid_argument("invalid resident score-retention request");
@@ -350,7 +350,7 @@ void* fastpls_resident_opls_create(const void* x, const void* y, const int* labe
                                    unsigned long long seed, int north, char* error,
                                    size_t error_capacity) {
   return guarded_create(error, error_capacity, "unknown resident CUDA OPLS fitting error", [&]() -> void* {
-    if (!x || (precision != 32 && precision != 64) || north < 0)
+    if (!x || (precision != 32 && precision != 64 && precision != 16) || north < 0)
       throw std::invalid_argument("invalid resident CUDA OPLS input");
     FitRequest r = request(kOpls, x, y, labels, n, p, q, components, scaling, oversample, power,
                            retain_scores, seed);
@@ -367,7 +367,7 @@ void* fastpls_resident_kernelpls_create(const void* x, const void* y, const int*
                                         size_t error_capacity) {
   return guarded_create(error, error_capacity, "unknown resident CUDA nonlinear kernel PLS fitting error",
                         [&]() -> void* {
-    if (!x || (precision != 32 && precision != 64) || (kernel != 2 && kernel != 3))
+    if (!x || (precision != 32 && precision != 64 && precision != 16) || (kernel != 2 && kernel != 3))
       throw std::invalid_argument("invalid resident CUDA nonlinear kernel PLS input");
     FitRequest r = request(kKernelPls, x, y, labels, n, p, q, components, scaling, oversample, power,
                            retain_scores, seed);

@@ -1,6 +1,7 @@
 // Shared device/host utilities for the B200 fastPLS fitting library.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -113,6 +114,17 @@ template <class T>
 __device__ __forceinline__ double as_f64(T v) {
   return static_cast<double>(v);
 }
+
+// BF16 storage of the predictors (precision 16): widened exactly to FP64
+using bf16 = __nv_bfloat16;
+__device__ __forceinline__ double as_f64(bf16 v) {
+  return static_cast<double>(__bfloat162float(v));
+}
+
+// type of responses and results for a predictor storage type: BF16
+// predictors take FP32 responses and return FP32 results
+template <class T> struct io_type { using type = T; };
+template <> struct io_type<bf16> { using type = float; };
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -620,9 +620,11 @@ void predict_from_scores(const DeviceModel& model, const double* scores,
   gemm_f64(g, stream);
 }
 
+template void prepare_responses<float>(const float*, const int*, int, int, double*,
+                                       double*, double*, int*, cudaStream_t);
+template void prepare_responses<double>(const double*, const int*, int, int, double*,
+                                        double*, double*, int*, cudaStream_t);
 #define FPLS_INSTANTIATE(T)                                                    \
-  template void prepare_responses<T>(const T*, const int*, int, int, double*, \
-                                     double*, double*, int*, cudaStream_t);   \
   template void fit_simpls<T>(const T*, int, int, long, const double*,        \
                               const double*, int, int, int, DeviceModel&,     \
                               Workspace&, cudaStream_t, int);                 \
@@ -633,6 +635,7 @@ void predict_from_scores(const DeviceModel& model, const double* scores,
                                      double*, Workspace&, cudaStream_t);
 FPLS_INSTANTIATE(float)
 FPLS_INSTANTIATE(double)
+FPLS_INSTANTIATE(bf16)
 #undef FPLS_INSTANTIATE
 
 }  // namespace fpls

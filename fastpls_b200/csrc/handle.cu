@@ -158,8 +158,13 @@ void check_path(const int* prefixes, int count, int a) {
 
 }  // namespace
 
+// T: storage type of the predictors (float, double, or bf16 for precision
+// 16); TO: type of responses and of every result written back (T, or float
+// for bf16 predictors).
 template <class T>
 class TypedHandle final : public ResidentHandle {
+  using TO = typename io_type<T>::type;
+
  public:
   explicit TypedHandle(const FitRequest& rq) : rq_(rq) {
     try {
@@ -185,7 +190,7 @@ class TypedHandle final : public ResidentHandle {
     const int q = model_.m;
     pred_.reserve((size_t)rows * q, stream_);
     conv_.reserve((size_t)rows * q, stream_);
-    T* dst = static_cast<T*>(out);
+    TO* dst = static_cast<TO*>(out);
     for (int j = 0; j < count; ++j) {
       const int k = prefixes[j];
       if (lda) lda_state().discriminants(scores_.get(), rows, rows, k, pred_.get(), rows, stream_);
@@ -210,7 +215,7 @@ class TypedHandle final : public ResidentHandle {
     disc_.reserve((size_t)rows * q, stream_);
     conv_.reserve((size_t)rows * q, stream_);
     top_.reserve((size_t)rows * top, stream_);
-    T* resp = static_cast<T*>(response_out);
+    TO* resp = static_cast<TO*>(response_out);
     for (int j = 0; j < count; ++j) {
       const int k = prefixes[j];
       const double* decoded = pred_.get();
@@ -236,7 +241,7 @@ class TypedHandle final : public ResidentHandle {
     upload_rows(x, rows);
     score_rows(rows, prefix);
     conv_.reserve((size_t)rows * prefix, stream_);
-    download(scores_.get(), (long)rows * prefix, static_cast<T*>(out));
+    download(scores_.get(), (long)rows * prefix, static_cast<TO*>(out));
     FPLS_CHECK(cudaStreamSynchronize(stream_));
   }
 
@@ -252,24 +257,24 @@ class TypedHandle final : public ResidentHandle {
     score_rows(rows, prefix);
     pred_.reserve((size_t)rows * q, stream_);
     predict_from_scores(model_, scores_.get(), rows, rows, prefix, pred_.get(), rows, stream_);
-    DeviceArray<T> yd;
+    DeviceArray<TO> yd;
     DeviceArray<int> ld;
     if (labels) {
       ld.allocate(rows, stream_);
       FPLS_CHECK(cudaMemcpyAsync(ld.get(), labels, sizeof(int) * rows, cudaMemcpyHostToDevice, stream_));
     } else {
       yd.allocate((size_t)rows * q, stream_);
-      FPLS_CHECK(cudaMemcpyAsync(yd.get(), y, sizeof(T) * rows * q, cudaMemcpyHostToDevice, stream_));
+      FPLS_CHECK(cudaMemcpyAsync(yd.get(), y, sizeof(TO) * rows * q, cudaMemcpyHostToDevice, stream_));
     }
     DeviceArray<double> sums((size_t)3 * q, stream_);
     FPLS_CHECK(cudaMemsetAsync(ws_.flag.get(), 0, sizeof(int), stream_));
-    response_sums_kernel<T><<<q, 256, 0, stream_>>>(pred_.get(), yd.get(), ld.get(),
+    response_sums_kernel<TO><<<q, 256, 0, stream_>>>(pred_.get(), yd.get(), ld.get(),
                                                     model_.ymean.get(), rows, q,
                                                     sums.get(), ws_.flag.get());
     count_launch();
     FPLS_LAUNCH("response_sums");
     conv_.reserve((size_t)3 * q, stream_);
-    download(sums.get(), 3L * q, static_cast<T*>(out));
+    download(sums.get(), 3L * q, static_cast<TO*>(out));
     raise_on_flag(ws_, stream_, "nonfinite response/prediction or invalid class label in resident metrics");
   }
 
@@ -290,7 +295,7 @@ class TypedHandle final : public ResidentHandle {
     }
     if (!src) throw std::invalid_argument("resident field is not available after compaction");
     conv_.reserve(size, stream_);
-    download(src, (long)size, static_cast<T*>(out));
+    download(src, (long)size, static_cast<TO*>(out));
     FPLS_CHECK(cudaStreamSynchronize(stream_));
   }
 
@@ -338,7 +343,7 @@ class TypedHandle final : public ResidentHandle {
     if (cls && q < 2) throw std::invalid_argument("classification requires at least two classes");
     xtrain_.allocate((size_t)n * p, stream_);
     FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
-    DeviceArray<T> y;
+    DeviceArray<TO> y;
     if (cls) {
       model_.labels.allocate(n, stream_);
       FPLS_CHECK(cudaMemcpyAsync(model_.labels.get(), rq_.labels, sizeof(int) * n, cudaMemcpyHostToDevice, stream_));
@@ -347,7 +352,7 @@ class TypedHandle final : public ResidentHandle {
         if (rq_.labels[i] >= 1 && rq_.labels[i] <= q) ++model_.class_counts[rq_.labels[i] - 1];
     } else {
       y.allocate((size_t)n * q, stream_);
-      FPLS_CHECK(cudaMemcpyAsync(y.get(), rq_.y, sizeof(T) * n * q, cudaMemcpyHostToDevice, stream_));
+      FPLS_CHECK(cudaMemcpyAsync(y.get(), rq_.y, sizeof(TO) * n * q, cudaMemcpyHostToDevice, stream_));
     }
     model_.classification = cls;
     ws_.ensure(n, p, q, a, stream_);
@@ -355,7 +360,7 @@ class TypedHandle final : public ResidentHandle {
     DeviceArray<double> yc((size_t)n * q, stream_);
     DeviceArray<double> ycsum(q, stream_);
     model_.ymean.allocate(q, stream_);
-    prepare_responses<T>(y.get(), model_.labels.get(), n, q, yc.get(),
+    prepare_responses<TO>(y.get(), model_.labels.get(), n, q, yc.get(),
                          model_.ymean.get(), ycsum.get(), ws_.flag.get(), stream_);
     if (rq_.method == kPlssvd)
       fit_plssvd<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_);
@@ -394,16 +399,16 @@ class TypedHandle final : public ResidentHandle {
     FPLS_CHECK(cudaMemcpyAsync(xbuf_.get(), x, sizeof(T) * rows * rq_.p, cudaMemcpyHostToDevice, stream_));
   }
 
-  void download(const double* src, long count, T* dst) {
-    const T* from = nullptr;
-    if (std::is_same<T, double>::value) {
-      from = reinterpret_cast<const T*>(src);
+  void download(const double* src, long count, TO* dst) {
+    const TO* from = nullptr;
+    if (std::is_same<TO, double>::value) {
+      from = reinterpret_cast<const TO*>(src);
     } else {
-      convert<T>(src, count, conv_.get(), stream_);
+      convert<TO>(src, count, conv_.get(), stream_);
       from = conv_.get();
     }
-    FPLS_CHECK(cudaMemcpyAsync(dst, from, sizeof(T) * count, cudaMemcpyDeviceToHost, stream_));
-    if (!std::is_same<T, double>::value) FPLS_CHECK(cudaStreamSynchronize(stream_));
+    FPLS_CHECK(cudaMemcpyAsync(dst, from, sizeof(TO) * count, cudaMemcpyDeviceToHost, stream_));
+    if (!std::is_same<TO, double>::value) FPLS_CHECK(cudaStreamSynchronize(stream_));
   }
 
   LdaState& lda_state() {
@@ -497,7 +502,8 @@ class TypedHandle final : public ResidentHandle {
   cudaStream_t stream_ = nullptr;
   DeviceModel model_;
   Workspace ws_;
-  DeviceArray<T> xtrain_, xbuf_, conv_;
+  DeviceArray<T> xtrain_, xbuf_;
+  DeviceArray<TO> conv_;
   DeviceArray<double> scores_, pred_, disc_, loadings_, var_ss_, design_;
   DeviceArray<int> top_;
   std::unique_ptr<LdaState> lda_;
@@ -506,6 +512,7 @@ class TypedHandle final : public ResidentHandle {
 ResidentHandle* make_handle(int precision, const FitRequest& rq) {
   if (precision == 32) return new TypedHandle<float>(rq);
   if (precision == 64) return new TypedHandle<double>(rq);
+  if (precision == 16) return new TypedHandle<bf16>(rq);
   throw std::invalid_argument("invalid resident matrix or precision");
 }
 

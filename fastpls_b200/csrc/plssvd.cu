@@ -193,5 +193,8 @@ template void fit_plssvd<float>(const float*, int, int, long, const double*,
 template void fit_plssvd<double>(const double*, int, int, long, const double*,
                                  const double*, int, int, int, DeviceModel&,
                                  Workspace&, cudaStream_t);
+template void fit_plssvd<bf16>(const bf16*, int, int, long, const double*,
+                               const double*, int, int, int, DeviceModel&,
+                               Workspace&, cudaStream_t);
 
 }  // namespace fpls

@@ -391,6 +391,7 @@ void kernel_scores(const DeviceModel& model, const T* X, int rows, long ld, int 
                                  double*, long, Workspace&, cudaStream_t);
 FPLS_INSTANTIATE(float)
 FPLS_INSTANTIATE(double)
+FPLS_INSTANTIATE(bf16)
 #undef FPLS_INSTANTIATE
 
 }  // namespace fpls

@@ -381,6 +381,7 @@ void topk_rows(const double* values, int rows, int classes, int top, int* out,
                                long, cudaStream_t);
 FPLS_INSTANTIATE(float)
 FPLS_INSTANTIATE(double)
+FPLS_INSTANTIATE(bf16)
 template void gather_rows<int>(const int*, long, int, const int*, int, int*,
                                long, cudaStream_t);
 #undef FPLS_INSTANTIATE
