@@ -122,10 +122,23 @@ class Server {
         // a prediction may be queued behind the fit of its model: it is
         // admitted once that fit has produced the model
         auto ft = all_.find(r->model);
-        if (ft == all_.end() || ft->second->kind != kFit || ft->second->done)
+        if (ft == all_.end() || ft->second->kind != kFit ||
+            (ft->second->done && ft->second->status == 0))
           throw std::invalid_argument("unknown model ticket");
         if (ft->second->fit.p != r->fit.p || ft->second->precision != r->precision)
           throw std::invalid_argument("prediction rows do not match the model's columns or precision");
+        if (ft->second->done) {
+          // the fit has already failed (and is not yet collected): the
+          // prediction completes at once with that error
+          r->status = 1;
+          r->error = "the model's fit failed: " + ft->second->error;
+          r->started = r->finished = Clock::now();
+          r->done = true;
+          const unsigned long long t = r->ticket;
+          all_[t] = std::move(r);
+          cv_done_.notify_all();
+          return t;
+        }
         r->deferred = true;
       }
     } else {

@@ -5,8 +5,16 @@
 
 namespace fpls {
 
-// Cyclic Jacobi eigen-decomposition of a symmetric m x m matrix held in
-// shared memory (column-major A[i + j*m]); eigenvectors accumulate in E.
+// Jacobi eigen-decomposition of a symmetric m x m matrix held in shared
+// memory (column-major A[i + j*m]); eigenvectors accumulate in E.
+// Parallel ordering (Brent-Luk round robin): each sweep runs m - 1 (m even)
+// or m (m odd) rounds of disjoint rotations. The rotations of a round go in
+// groups of 32, one per lane: each lane computes its rotation, then the group
+// is applied (columns of A and E, then rows of A). Rotations of one round
+// touch disjoint rows and columns, so a rotation's 2 x 2 block is unchanged
+// by the others of its round. Each rotation annihilates A[p, q] as in the
+// classical cyclic method (tangent of the smaller root of t^2 + 2 theta t = 1,
+// theta = (a_qq - a_pp) / (2 a_pq)).
 // Executed by the first warp of the block; the caller synchronises after.
 // Returns the number of sweeps used (<= max_sweeps).
 __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
@@ -15,8 +23,21 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
   if (threadIdx.x >= 32) return 0;
   for (int k = lane; k < m * m; k += 32) E[k] = (k % m == k / m) ? 1.0 : 0.0;
   __syncwarp();
+  const int players = m + (m & 1);  // a dummy player for odd m sits out
+  const int half = players / 2;     // rotations per round
+  const int groups = (half + 31) / 32;
+  // round-robin schedule (circle method): slot 0 pairs the fixed player
+  // players-1 with player `round`; slot s >= 1 pairs (round + s) and
+  // (round - s) modulo players-1, so both advance by one each round
+  int sa[8], sb[8];  // this lane's slots g*32 + lane, g < groups (m <= 512)
+  const int wrap = players - 1;
+  // this lane's first work item (rotation k, row i) of a group, and the
+  // step between items 32 apart: k += dk, i += di with carry
+  const int dk = 32 / m, di = 32 % m;
+  const int k0 = lane / m, i0 = lane % m;
   int sweep = 0;
-  for (; sweep < max_sweeps; ++sweep) {
+  double prev = 0.0;
+  for (; sweep < max_sweeps && m > 1; ++sweep) {
     double off = 0.0, diag = 0.0;
     for (int k = lane; k < m * m; k += 32) {
       const int i = k % m, j = k / m;
@@ -26,34 +47,96 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
     off = warp_sum(off);
     diag = warp_sum(diag);
     if (off <= 1e-30 * diag || off == 0.0) break;
-    for (int pp = 0; pp < m - 1; ++pp) {
-      for (int qq = pp + 1; qq < m; ++qq) {
-        const double apq = A[pp + qq * m];
-        if (apq == 0.0) continue;
-        const double app = A[pp + pp * m], aqq = A[qq + qq * m];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double tt = (theta >= 0 ? 1.0 : -1.0) /
-                          (fabs(theta) + sqrt(theta * theta + 1.0));
-        const double c = 1.0 / sqrt(tt * tt + 1.0), s = tt * c;
-        __syncwarp();
-        // A <- J^T A J with J the (pp, qq) rotation: columns then rows
-        for (int k = lane; k < m; k += 32) {
-          const double akp = A[k + pp * m], akq = A[k + qq * m];
-          A[k + pp * m] = c * akp - s * akq;
-          A[k + qq * m] = s * akp + c * akq;
+    // at the rounding floor (large m) the off-diagonal mass stops shrinking
+    if (sweep > 0 && off <= 1e-24 * diag && off > 0.25 * prev) break;
+    prev = off;
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      const int slot = g * 32 + lane;
+      sa[g] = slot == 0 ? wrap : slot % wrap;
+      sb[g] = slot == 0 ? 0 : (wrap - slot % wrap) % wrap;
+    }
+    for (int round = 0; round < wrap; ++round) {
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        if (g >= groups) break;
+        const int count = min(32, half - g * 32);
+        int p = 0, q = 0;
+        double c = 1.0, s = 0.0;
+        if (lane < count) {
+          const int a = min(sa[g], sb[g]), b = max(sa[g], sb[g]);
+          if (b < m) {
+            p = a;
+            q = b;
+            const double apq = A[p + q * m];
+            if (apq != 0.0) {
+              // t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)) with
+              // theta = d / e, d = a_qq - a_pp, e = 2 a_pq, written as
+              // sgn(d) e / (|d| + sqrt(d^2 + e^2)): one square root and one
+              // division on the dependent path instead of two of each
+              const double d = A[q + q * m] - A[p + p * m], e = 2.0 * apq;
+              const double tt = (d >= 0 ? e : -e) / (fabs(d) + sqrt(fma(d, d, e * e)));
+              c = rsqrt(fma(tt, tt, 1.0));
+              s = tt * c;
+            }
+          }
         }
         __syncwarp();
-        for (int k = lane; k < m; k += 32) {
-          const double apk = A[pp + k * m], aqk = A[qq + k * m];
-          A[pp + k * m] = c * apk - s * aqk;
-          A[qq + k * m] = s * apk + c * aqk;
-        }
-        for (int k = lane; k < m; k += 32) {
-          const double ekp = E[k + pp * m], ekq = E[k + qq * m];
-          E[k + pp * m] = c * ekp - s * ekq;
-          E[k + qq * m] = s * ekp + c * ekq;
+        const int work = count * m;
+        // A <- A J and E <- E J: columns p, q of every rotation of the group
+        int k = k0, i = i0;
+        for (int w = lane; w - lane < work; w += 32) {
+          const int kk = w < work ? k : 0;
+          const int pk = __shfl_sync(0xffffffffu, p, kk);
+          const int qk = __shfl_sync(0xffffffffu, q, kk);
+          const double ck = __shfl_sync(0xffffffffu, c, kk);
+          const double sk = __shfl_sync(0xffffffffu, s, kk);
+          if (w < work && sk != 0.0) {
+            const double akp = A[i + pk * m], akq = A[i + qk * m];
+            A[i + pk * m] = ck * akp - sk * akq;
+            A[i + qk * m] = sk * akp + ck * akq;
+            const double ekp = E[i + pk * m], ekq = E[i + qk * m];
+            E[i + pk * m] = ck * ekp - sk * ekq;
+            E[i + qk * m] = sk * ekp + ck * ekq;
+          }
+          k += dk;
+          i += di;
+          if (i >= m) {
+            i -= m;
+            ++k;
+          }
         }
         __syncwarp();
+        // A <- J^T A: rows p, q of every rotation of the group
+        k = k0;
+        i = i0;
+        for (int w = lane; w - lane < work; w += 32) {
+          const int kk = w < work ? k : 0;
+          const int pk = __shfl_sync(0xffffffffu, p, kk);
+          const int qk = __shfl_sync(0xffffffffu, q, kk);
+          const double ck = __shfl_sync(0xffffffffu, c, kk);
+          const double sk = __shfl_sync(0xffffffffu, s, kk);
+          if (w < work && sk != 0.0) {
+            const double apk = A[pk + i * m], aqk = A[qk + i * m];
+            A[pk + i * m] = ck * apk - sk * aqk;
+            A[qk + i * m] = sk * apk + ck * aqk;
+          }
+          k += dk;
+          i += di;
+          if (i >= m) {
+            i -= m;
+            ++k;
+          }
+        }
+        __syncwarp();
+        // next round: slots >= 1 advance both players by one
+        const int slot = g * 32 + lane;
+        if (slot == 0) {
+          ++sb[g];
+        } else {
+          sa[g] = sa[g] + 1 == wrap ? 0 : sa[g] + 1;
+          sb[g] = sb[g] + 1 == wrap ? 0 : sb[g] + 1;
+        }
       }
     }
   }

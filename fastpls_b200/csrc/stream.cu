@@ -1,5 +1,5 @@
 // HBM-streaming kernels over the resident predictor matrix X (n x p,
-// column-major, FP32 or FP64 storage, FP64 arithmetic).
+// column-major, BF16, FP32 or FP64 storage, FP64 arithmetic).
 //
 // These are the GEMV-shaped steps of a single fit: the column moments
 // (centre, scale, X^T Yc) in one pass, t = X r (scores) and p = X^T t
@@ -17,6 +17,31 @@ namespace fpls {
 namespace {
 
 constexpr int kThreads = 256;
+
+// Two consecutive rows of one column in one load (bf16x2, float2, double2):
+// 4-16 bytes per lane, 128-512 bytes per warp request. Used when the column
+// stride is even and X is aligned to the pair size.
+template <class T> struct Pair;
+template <> struct Pair<float> {
+  using type = float2;
+  static __device__ __forceinline__ double lo(type v) { return v.x; }
+  static __device__ __forceinline__ double hi(type v) { return v.y; }
+};
+template <> struct Pair<double> {
+  using type = double2;
+  static __device__ __forceinline__ double lo(type v) { return v.x; }
+  static __device__ __forceinline__ double hi(type v) { return v.y; }
+};
+template <> struct Pair<bf16> {
+  using type = __nv_bfloat162;
+  static __device__ __forceinline__ double lo(type v) { return __low2float(v); }
+  static __device__ __forceinline__ double hi(type v) { return __high2float(v); }
+};
+
+template <class T>
+bool pair_aligned(const T* X, long ld) {
+  return ld % 2 == 0 && reinterpret_cast<uintptr_t>(X) % (2 * sizeof(T)) == 0;
+}
 
 // ---------------------------------------------------------------------------
 // X^T V (and optionally column sums / sums of squares) -- warp per column.
@@ -93,6 +118,108 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Same contract as xtv_kernel, with each lane reading row pairs: lane l takes
+// rows 2(l + 32u) and 2(l + 32u) + 1 of the chunk (rc even, column stride even).
+template <class T, int MB, bool MOMENTS>
+__global__ void __launch_bounds__(kThreads)
+    xtv_pair_kernel(const T* __restrict__ X, int n, int p, long ld,
+                    const double* __restrict__ V, long ldv, int nb, int rc,
+                    double* __restrict__ partial) {
+  using P = Pair<T>;
+  using T2 = typename P::type;
+  extern __shared__ double vs[];  // rc x nb
+  const int chunk = blockIdx.y;
+  const int r0 = chunk * rc;
+  const int rows = min(rc, n - r0);
+  for (int idx = threadIdx.x; idx < rows * nb; idx += blockDim.x) {
+    const int r = idx % rows, c = idx / rows;
+    vs[r + c * rc] = V[(r0 + r) + (long)c * ldv];
+  }
+  __syncthreads();
+  const int slots = nb + (MOMENTS ? 2 : 0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pairs = rows >> 1;
+  for (int jj = warp; jj < 32; jj += kThreads / 32) {
+    const int j = blockIdx.x * 32 + jj;
+    if (j >= p) break;
+    const T* col = X + (long)j * ld + r0;
+    const T2* col2 = reinterpret_cast<const T2*>(col);
+    double acc[MB > 0 ? MB : 1];
+#pragma unroll
+    for (int c = 0; c < (MB > 0 ? MB : 1); ++c) acc[c] = 0.0;
+    double s = 0.0, ss = 0.0;
+    int q = lane;
+    for (; q + 96 < pairs; q += 128) {
+      T2 x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = col2[q + 32 * u];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double a = P::lo(x[u]), b = P::hi(x[u]);
+        const int r = 2 * (q + 32 * u);
+        if (MOMENTS) {
+          s += a;
+          ss = fma(a, a, ss);
+          s += b;
+          ss = fma(b, b, ss);
+        }
+#pragma unroll
+        for (int c = 0; c < MB; ++c)
+          if (c < nb) {
+            const double2 v = *reinterpret_cast<const double2*>(vs + r + c * rc);
+            acc[c] = fma(a, v.x, acc[c]);
+            acc[c] = fma(b, v.y, acc[c]);
+          }
+      }
+    }
+    for (; q < pairs; q += 32) {
+      const T2 x = col2[q];
+      const double a = P::lo(x), b = P::hi(x);
+      const int r = 2 * q;
+      if (MOMENTS) {
+        s += a;
+        ss = fma(a, a, ss);
+        s += b;
+        ss = fma(b, b, ss);
+      }
+#pragma unroll
+      for (int c = 0; c < MB; ++c)
+        if (c < nb) {
+          const double2 v = *reinterpret_cast<const double2*>(vs + r + c * rc);
+          acc[c] = fma(a, v.x, acc[c]);
+          acc[c] = fma(b, v.y, acc[c]);
+        }
+    }
+    if ((rows & 1) && lane == 0) {  // odd last row of the final chunk
+      const int r = rows - 1;
+      const double a = as_f64(col[r]);
+      if (MOMENTS) {
+        s += a;
+        ss = fma(a, a, ss);
+      }
+#pragma unroll
+      for (int c = 0; c < MB; ++c)
+        if (c < nb) acc[c] = fma(a, vs[r + c * rc], acc[c]);
+    }
+    double* out = partial + ((long)chunk * p + j) * slots;
+#pragma unroll
+    for (int c = 0; c < MB; ++c) {
+      if (c < nb) {
+        const double v = warp_sum(acc[c]);
+        if (lane == 0) out[c] = v;
+      }
+    }
+    if (MOMENTS) {
+      s = warp_sum(s);
+      ss = warp_sum(ss);
+      if (lane == 0) {
+        out[nb] = s;
+        out[nb + 1] = ss;
+      }
+    }
+  }
+}
+
 // Sum the per-chunk partials: out_c[j] (+ c*ldo) for each slot c < nb, and
 // the moment slots into sum/sumsq.
 __global__ void xtv_finish(const double* __restrict__ partial, int chunks,
@@ -117,7 +244,7 @@ void xtv_launch(const T* X, int n, int p, long ld, const double* V, long ldv,
   // rows per chunk: keep the staged V block <= 64 KB and give the grid
   // enough blocks to cover every SM several times.
   int rc = 2048;
-  if (nb > 0) rc = std::min(rc, std::max(128, (64 * 1024 / 8) / nb));
+  if (nb > 0) rc = std::min(rc, std::max(128, (64 * 1024 / 8) / nb / 64 * 64));
   const int col_tiles = (int)ceil_div(p, 32);
   int chunks = (int)ceil_div(n, rc);
   const int want = 6 * num_sms();
@@ -132,12 +259,21 @@ void xtv_launch(const T* X, int n, int p, long ld, const double* V, long ldv,
   const int slots = nb + (MOMENTS ? 2 : 0);
   scratch.reserve((size_t)chunks * p * slots, stream);
   const size_t smem = (size_t)rc * std::max(nb, 1) * sizeof(double);
-  if (smem > 48 * 1024)
-    FPLS_CHECK(cudaFuncSetAttribute(xtv_kernel<T, MB, MOMENTS>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
-  xtv_kernel<T, MB, MOMENTS><<<dim3(col_tiles, chunks), kThreads, smem, stream>>>(
-      X, n, p, ld, V, ldv, nb, rc, scratch.get());
+  if (pair_aligned(X, ld)) {
+    if (smem > 48 * 1024)
+      FPLS_CHECK(cudaFuncSetAttribute(xtv_pair_kernel<T, MB, MOMENTS>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    xtv_pair_kernel<T, MB, MOMENTS><<<dim3(col_tiles, chunks), kThreads, smem, stream>>>(
+        X, n, p, ld, V, ldv, nb, rc, scratch.get());
+  } else {
+    if (smem > 48 * 1024)
+      FPLS_CHECK(cudaFuncSetAttribute(xtv_kernel<T, MB, MOMENTS>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    xtv_kernel<T, MB, MOMENTS><<<dim3(col_tiles, chunks), kThreads, smem, stream>>>(
+        X, n, p, ld, V, ldv, nb, rc, scratch.get());
+  }
   count_launch();
   FPLS_LAUNCH("xtv_kernel");
   const long total = (long)p * slots;
@@ -222,6 +358,95 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// X R with 16-byte row vectors: thread t of a 256 x V row tile takes rows
+// V t .. V t + V - 1 (V = 16 / sizeof(T): 8 BF16, 4 FP32, 2 FP64 rows) with
+// one 16-byte load per column, 4 columns per step. Needs a column stride
+// that is a multiple of 8 elements and a 16-byte aligned X. Each row's sum
+// runs over the chunk's columns in order, exactly as in xr_kernel.
+template <class T>
+struct Vec16 {
+  static constexpr int V = 16 / sizeof(T);
+  static __device__ __forceinline__ void unpack(const uint4& raw, double (&x)[V]) {
+    const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+    for (int e = 0; e < V; ++e) x[e] = as_f64(v[e]);
+  }
+};
+
+template <class T, int NB>
+__global__ void __launch_bounds__(kThreads)
+    xr_vec_kernel(const T* __restrict__ X, int n, int p, long ld,
+                  const double* __restrict__ R, long ldr, int nb, int cc,
+                  double* __restrict__ partial) {
+  constexpr int V = Vec16<T>::V;
+  extern __shared__ double rs[];  // cc x NB
+  const int chunk = blockIdx.y;
+  const int c0 = chunk * cc;
+  const int cols = min(cc, p - c0);
+  for (int idx = threadIdx.x; idx < cols * NB; idx += blockDim.x) {
+    const int j = idx / NB, c = idx % NB;
+    rs[idx] = c < nb ? R[(c0 + j) + (long)c * ldr] : 0.0;
+  }
+  __syncthreads();
+  const int r0 = blockIdx.x * (kThreads * V) + threadIdx.x * V;
+  if (r0 >= n) return;
+  double acc[V][NB];
+#pragma unroll
+  for (int e = 0; e < V; ++e)
+#pragma unroll
+    for (int c = 0; c < NB; ++c) acc[e][c] = 0.0;
+  const T* base = X + (long)c0 * ld + r0;
+  if (r0 + V <= n) {
+    int j = 0;
+    for (; j + 3 < cols; j += 4) {
+      uint4 raw[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        raw[u] = __ldcs(reinterpret_cast<const uint4*>(base + (long)(j + u) * ld));
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        double x[V];
+        Vec16<T>::unpack(raw[u], x);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+          const double r = rs[(j + u) * NB + c];
+#pragma unroll
+          for (int e = 0; e < V; ++e) acc[e][c] = fma(x[e], r, acc[e][c]);
+        }
+      }
+    }
+    for (; j < cols; ++j) {
+      double x[V];
+      Vec16<T>::unpack(__ldcs(reinterpret_cast<const uint4*>(base + (long)j * ld)), x);
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        const double r = rs[j * NB + c];
+#pragma unroll
+        for (int e = 0; e < V; ++e) acc[e][c] = fma(x[e], r, acc[e][c]);
+      }
+    }
+  } else {  // ragged last rows: element loads
+    for (int j = 0; j < cols; ++j) {
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        if (r0 + e >= n) break;
+        const double x = as_f64(base[(long)j * ld + e]);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) acc[e][c] = fma(x, rs[j * NB + c], acc[e][c]);
+      }
+    }
+  }
+  double* out = partial + (long)chunk * n * nb;
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    if (c < nb) {
+#pragma unroll
+      for (int e = 0; e < V; ++e)
+        if (r0 + e < n) out[r0 + e + (long)c * n] = acc[e][c];
+    }
+  }
+}
+
 __global__ void xr_finish(const double* __restrict__ partial, int chunks, int n,
                           int nb, const double* offset, double* out, long ldo) {
   const long total = (long)n * nb;
@@ -239,16 +464,25 @@ template <class T, int NB>
 void xr_launch(const T* X, int n, int p, long ld, const double* R, long ldr,
                int nb, const double* offset, double* out, long ldo,
                DeviceArray<double>& scratch, cudaStream_t stream) {
-  const int row_tiles = (int)ceil_div(n, 2 * kThreads);
-  const int want = 6 * num_sms();
-  int chunks = std::max(1, std::min((int)ceil_div(want, row_tiles), (int)ceil_div(p, 64)));
+  // 16-byte row vectors for the one- and two-column products (HBM-bound);
+  // wider products are FP64-issue-bound and keep two rows per thread. The
+  // column chunks depend on n and p only (a nominal 1024-row tile), so every
+  // storage type and both kernels sum each row in the same order.
+  const bool vec = NB <= 2 && ld % 8 == 0 && reinterpret_cast<uintptr_t>(X) % 16 == 0;
+  const int nominal_tiles = (int)ceil_div(n, 1024);
+  const int want = 16 * num_sms();
+  int chunks = std::max(1, std::min((int)ceil_div(want, nominal_tiles), (int)ceil_div(p, 64)));
   int cc = (int)ceil_div(p, chunks);
   cc = std::min(cc, (48 * 1024 / 8) / NB);
   chunks = (int)ceil_div(p, cc);
   scratch.reserve((size_t)chunks * n * nb, stream);
   const size_t smem = (size_t)cc * NB * sizeof(double);
-  xr_kernel<T, NB><<<dim3(row_tiles, chunks), kThreads, smem, stream>>>(
-      X, n, p, ld, R, ldr, nb, cc, scratch.get());
+  if (vec)
+    xr_vec_kernel<T, NB><<<dim3(ceil_div(n, kThreads * Vec16<T>::V), chunks), kThreads, smem, stream>>>(
+        X, n, p, ld, R, ldr, nb, cc, scratch.get());
+  else
+    xr_kernel<T, NB><<<dim3(ceil_div(n, 2 * kThreads), chunks), kThreads, smem, stream>>>(
+        X, n, p, ld, R, ldr, nb, cc, scratch.get());
   count_launch();
   FPLS_LAUNCH("xr_kernel");
   const long total = (long)n * nb;

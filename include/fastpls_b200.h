@@ -18,6 +18,13 @@
  *   - a handle owns one CUDA stream; calls are synchronous and a handle is
  *     not safe for concurrent calls. Every handle, whatever the method, is
  *     released with fastpls_resident_simpls_destroy.
+ * Addition: the four _create functions also take precision 16. The
+ * predictors x (and the rows later given to that handle's predict, classify,
+ * project and response-sums calls) are then BF16 bit patterns (uint16, the
+ * upper half of an IEEE-754 float), kept in BF16 on the device; responses y
+ * and every result written back (predictions, scores, exports, sums) are
+ * FP32. Arithmetic stays FP64, so a BF16 fit equals the FP64 fit of the
+ * BF16-rounded values.
  * Arithmetic: products and reductions are FP64 on the device whatever the
  * storage precision, so results agree with the reference's FP64 CPU path to
  * ~1e-10 relative. The one exception is the batched CV x permutation engine,
