@@ -49,7 +49,7 @@ def test_create_rejects_bad_precision(lib):
     x = np.zeros((4, 3))
     err, cap = _err()
     h = lib.fastpls_resident_simpls_create(
-        x.ctypes.data_as(C.c_void_p), None, None, 16, 4, 3, 1, 1, 1, 32, 5, 1,
+        x.ctypes.data_as(C.c_void_p), None, None, 8, 4, 3, 1, 1, 1, 32, 5, 1,
         C.c_ulonglong(1), err, cap)
     assert not h and err.value == b"invalid resident matrix or precision"
     h = lib.fastpls_resident_simpls_create(
