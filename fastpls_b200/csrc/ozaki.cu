@@ -283,8 +283,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
       for (int pass = 0; pass < npass && ok; ++pass) {
         const int dhi = min(S - 1, pass * ACC + ACC - 1);
         const int ns = min(S, dhi + 1);
-        const uint32_t bytes = (uint32_t)ns * (OZ_A_PLANE + Shape::B_PLANE);
-        for (int kb = 0; kb < args.kblocks; ++kb) {
+        // a stage has S plane slots of A and of B: a pass that needs ns < S
+        // digit planes packs S / ns k-blocks into each stage
+        const int kbs = S / ns;
+        for (int kb = 0; kb < args.kblocks; kb += kbs) {
+          const int nk = min(kbs, args.kblocks - kb);
           const int st = it % stages;
           if (it >= (uint32_t)stages &&
               !mbar_wait(&empty_bar[st], ((it / stages) - 1) & 1, abort, args.flag)) {
@@ -293,15 +296,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           }
           uint8_t* a_dst = smem + st * stage_bytes;
           uint8_t* b_dst = a_dst + S * OZ_A_PLANE;
-          mbar_expect_tx(&full_bar[st], bytes);
-          const long slab = (long)(args.kb0 + kb) * S;
-          for (int j = 0; j < ns; ++j) {
-            bulk_load(a_dst + j * OZ_A_PLANE,
-                      digits_a + ((slab + j) * args.rows_pa + (long)tm * OZ_BM) * OZ_BK,
-                      (uint32_t)OZ_A_PLANE, &full_bar[st]);
-            bulk_load(b_dst + j * Shape::B_PLANE,
-                      digits_b + ((slab + j) * args.rows_pb + (long)tn * BN) * OZ_BK,
-                      (uint32_t)Shape::B_PLANE, &full_bar[st]);
+          mbar_expect_tx(&full_bar[st], (uint32_t)(nk * ns) * (OZ_A_PLANE + Shape::B_PLANE));
+          for (int q = 0; q < nk; ++q) {
+            const long slab = (long)(args.kb0 + kb + q) * S;
+            for (int j = 0; j < ns; ++j) {
+              bulk_load(a_dst + (q * ns + j) * OZ_A_PLANE,
+                        digits_a + ((slab + j) * args.rows_pa + (long)tm * OZ_BM) * OZ_BK,
+                        (uint32_t)OZ_A_PLANE, &full_bar[st]);
+              bulk_load(b_dst + (q * ns + j) * Shape::B_PLANE,
+                        digits_b + ((slab + j) * args.rows_pb + (long)tn * BN) * OZ_BK,
+                        (uint32_t)Shape::B_PLANE, &full_bar[st]);
+            }
           }
           ++it;
         }
@@ -323,7 +328,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           if (!mbar_wait(&acc_empty, (pass - 1) & 1, abort, args.flag)) break;
           tc_fence_after();
         }
-        for (int kb = 0; kb < args.kblocks; ++kb) {
+        const int ns = min(S, dhi + 1);
+        const int kbs = S / ns;
+        for (int kb = 0; kb < args.kblocks; kb += kbs) {
+          const int nk = min(kbs, args.kblocks - kb);
           const int st = it % stages;
           if (!mbar_wait(&full_bar[st], (it / stages) & 1, abort, args.flag)) {
             ok = false;
@@ -332,13 +340,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           tc_fence_after();
           const uint32_t a0 = smem_u32(smem + st * stage_bytes);
           const uint32_t b0 = a0 + S * OZ_A_PLANE;
-          for (int d = dlo; d <= dhi; ++d)
-            for (int s = 0; s <= d; ++s) {
-              const uint64_t ad = core_desc(a0 + s * OZ_A_PLANE);
-              const uint64_t bd = core_desc(b0 + (d - s) * Shape::B_PLANE);
-              const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
-              tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
-            }
+          for (int q = 0; q < nk; ++q)
+            for (int d = dlo; d <= dhi; ++d)
+              for (int s = 0; s <= d; ++s) {
+                const uint64_t ad = core_desc(a0 + (q * ns + s) * OZ_A_PLANE);
+                const uint64_t bd = core_desc(b0 + (q * ns + d - s) * Shape::B_PLANE);
+                const uint32_t acc = (kb + q > 0 || s > 0) ? 1u : 0u;
+                tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
+              }
           tc_commit(&empty_bar[st]);
           ++it;
         }
