@@ -16,7 +16,9 @@ namespace fpls {
 // classical cyclic method (tangent of the smaller root of t^2 + 2 theta t = 1,
 // theta = (a_qq - a_pp) / (2 a_pq)).
 // Executed by the first warp of the block; the caller synchronises after.
-// Returns the number of sweeps used (<= max_sweeps).
+// Returns the number of sweeps used (<= max_sweeps). GMAX bounds the groups
+// of 32 rotations per round: m <= 64 GMAX.
+template <int GMAX = 1>
 __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
                                         int max_sweeps = 40) {
   const int lane = threadIdx.x & 31;
@@ -29,7 +31,7 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
   // round-robin schedule (circle method): slot 0 pairs the fixed player
   // players-1 with player `round`; slot s >= 1 pairs (round + s) and
   // (round - s) modulo players-1, so both advance by one each round
-  int sa[8], sb[8];  // this lane's slots g*32 + lane, g < groups (m <= 512)
+  int sa[GMAX], sb[GMAX];  // this lane's slots g*32 + lane, g < groups
   const int wrap = players - 1;
   // this lane's first work item (rotation k, row i) of a group, and the
   // step between items 32 apart: k += dk, i += di with carry
@@ -51,14 +53,14 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
     if (sweep > 0 && off <= 1e-24 * diag && off > 0.25 * prev) break;
     prev = off;
 #pragma unroll
-    for (int g = 0; g < 8; ++g) {
+    for (int g = 0; g < GMAX; ++g) {
       const int slot = g * 32 + lane;
       sa[g] = slot == 0 ? wrap : slot % wrap;
       sb[g] = slot == 0 ? 0 : (wrap - slot % wrap) % wrap;
     }
     for (int round = 0; round < wrap; ++round) {
 #pragma unroll
-      for (int g = 0; g < 8; ++g) {
+      for (int g = 0; g < GMAX; ++g) {
         if (g >= groups) break;
         const int count = min(32, half - g * 32);
         int p = 0, q = 0;

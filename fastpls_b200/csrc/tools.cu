@@ -195,7 +195,7 @@ __global__ void small_svd_from_gram(const double* __restrict__ G, int l, int k,
   int* order = reinterpret_cast<int*>(E + l * l);
   for (int idx = threadIdx.x; idx < l * l; idx += blockDim.x) A[idx] = G[idx];
   __syncthreads();
-  jacobi_eigen_warp(A, E, l, 60);
+  jacobi_eigen_warp<4>(A, E, l, 60);
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 0; i < l; ++i) order[i] = i;
