@@ -450,8 +450,15 @@ def fastcor(a, b=None, byrow=True, diag=True, precision=64):
     return out
 
 
-def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64):
-    """Truncated SVD on the device (fastsvd(backend = "cuda")): u, d, v."""
+AUDIT_FIELDS = ("certified", "deterministic_fallback", "attempts", "effective_oversample",
+                "effective_power", "effective_seed", "subspace_error",
+                "singular_value_error", "triplet_residual", "omitted_direction_ratio")
+
+
+def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64, audit=False):
+    """Truncated SVD on the device with the audited rSVD policy
+    (fastsvd(backend = "cuda")): u, d, v (and the audit record as a dict
+    when ``audit``)."""
     dt = _dtype(precision)
     X = _mat(x, dt)
     n, p = X.shape
@@ -459,11 +466,19 @@ def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64):
     u = np.zeros((n, k), order="F")
     v = np.zeros((p, k), order="F")
     d = np.zeros(k)
+    rec = np.zeros(10)
     err, cap = _lib.error_buffer()
-    rc = _lib.load().fastpls_b200_fastsvd(_p(X), precision, n, p, k, int(oversample),
-                                          int(power), C.c_ulonglong(seed), _p(u), _p(d),
-                                          _p(v), err, cap)
+    rc = _lib.load().fastpls_b200_fastsvd_audited(
+        _p(X), precision, n, p, k, int(oversample), int(power), C.c_ulonglong(seed), _p(u),
+        _p(d), _p(v), _p(rec), err, cap)
     _lib.check(rc, err)
+    if audit:
+        info = dict(zip(AUDIT_FIELDS, rec.tolist()))
+        for key in ("certified", "deterministic_fallback"):
+            info[key] = bool(info[key])
+        for key in ("attempts", "effective_oversample", "effective_power", "effective_seed"):
+            info[key] = int(info[key])
+        return u, d, v, info
     return u, d, v
 
 

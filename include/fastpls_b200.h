@@ -283,17 +283,36 @@ FASTPLS_B200_API int fastpls_b200_fastcor(const void* a, const void* b, int prec
                                           double* out, char* error,
                                           size_t error_capacity);
 
-/* Truncated SVD of x (n x p) by FP64 randomized subspace iteration on the
- * device (fastsvd(backend = "cuda"); the reference's CUDA route errors,
- * R/main.R:7932-7943): sketch width min(k + oversample, min(n, p)) <= 256,
- * `power` power iterations, Gaussian sketch from `seed`. Outputs (host, FP64):
- * u n x k (may be NULL), d k, v p x k (may be NULL); singular values are in
- * decreasing order, each (u, v) pair sign-normalised. */
+/* Truncated SVD of x (n x p) on the device with the reference's audited
+ * randomized SVD policy (fastsvd(backend = "cuda"); the reference's CUDA route
+ * errors, R/main.R:7932-7943; policy: inst/include/fastpls/core/
+ * audited_rsvd.hpp:298-414). FP64 randomized subspace iteration (Gaussian
+ * sketch from `seed`, `power` power iterations, sketch width
+ * min(k + 1 + oversample, min(n, p)) of at most 120 columns, since the small
+ * eigenproblem is solved in one block's shared memory) at rank k + 1; the result is returned only when certified: the
+ * triplet residual is <= 1e-2 of d_1 and no direction outside the first k
+ * is larger than 1.01 d_k, or two consecutive attempts agree (subspace 1e-3,
+ * singular values 1e-5, residual 1e-6). Attempts escalate oversample to 32
+ * and 48 and power to 3 and 4 with new seeds, then up to four recoveries with
+ * wider sketches; otherwise the call fails with the reference's message.
+ * min(n, p) < 6 is solved exactly. Outputs (host, FP64): u n x k (may be
+ * NULL), d k, v p x k (may be NULL); singular values in decreasing order,
+ * each (u, v) pair sign-normalised. */
 FASTPLS_B200_API int fastpls_b200_fastsvd(const void* x, int precision, int n, int p,
                                           int k, int oversample, int power,
                                           unsigned long long seed, double* u,
                                           double* d, double* v, char* error,
                                           size_t error_capacity);
+
+/* fastpls_b200_fastsvd with the audit record (RsvdAudit,
+ * audited_rsvd.hpp:19-30) in audit[10]: certified, deterministic fallback,
+ * attempts, effective oversample, effective power, effective seed, subspace
+ * error, singular value error, triplet residual, omitted direction ratio. */
+FASTPLS_B200_API int fastpls_b200_fastsvd_audited(const void* x, int precision, int n,
+                                                  int p, int k, int oversample, int power,
+                                                  unsigned long long seed, double* u,
+                                                  double* d, double* v, double* audit,
+                                                  char* error, size_t error_capacity);
 
 /* ---- serving loop (no counterpart in the reference) ---------------------
  * A server owns `workers` threads, each driving resident handles on its own
