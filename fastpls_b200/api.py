@@ -266,6 +266,51 @@ def fit_resident(X, Y=None, labels=None, classes=None, ncomp=2,
                          classification=labels is not None, feature_p=feature_p)
 
 
+def export_model(model: ResidentModel, scores=True) -> dict:
+    """The fields a SIMPLS / OPLS model needs to be rebuilt by
+    ``import_model`` (export field ids 0, 1, 2, 3, 4, 5), as FP64 arrays."""
+    out = {"method": model.method, "scaling": None, "classification": model.classification,
+           "weights": model.export(0).astype(np.float64),
+           "response_loadings": model.export(1).astype(np.float64),
+           "mean_x": model.export(3).astype(np.float64),
+           "scale_x": model.export(4).astype(np.float64),
+           "mean_y": model.export(5).astype(np.float64)}
+    if scores:
+        out["scores"] = model.export(2).astype(np.float64)
+    return out
+
+
+def import_model(fields: dict, labels=None, precision=64, scaling="centering") -> ResidentModel:
+    """Rebuild a resident SIMPLS / OPLS model from exported fields
+    (``fastpls_b200_model_import``); ``labels`` (with ``fields["scores"]``)
+    enable LDA on a classification model."""
+    method = fields.get("method", "simpls")
+    if method not in ("simpls", "opls"):
+        raise ValueError("model import supports SIMPLS and OPLS models")
+    R = np.asfortranarray(fields["weights"], dtype=np.float64)
+    Qm = np.asfortranarray(fields["response_loadings"], dtype=np.float64)
+    p, a = R.shape
+    q = Qm.shape[0]
+    T = fields.get("scores")
+    T = None if T is None else np.asfortranarray(T, dtype=np.float64)
+    n = 0 if T is None else T.shape[0]
+    mx = np.ascontiguousarray(fields["mean_x"], dtype=np.float64)
+    sx = np.ascontiguousarray(fields["scale_x"], dtype=np.float64)
+    my = np.ascontiguousarray(fields["mean_y"], dtype=np.float64)
+    lab = None if labels is None else np.ascontiguousarray(labels, dtype=np.int32)
+    cls = bool(fields.get("classification", False) or labels is not None)
+    sc = fields.get("scaling") or scaling
+    sc = SCALING[sc] if isinstance(sc, str) else int(sc)
+    err, cap = _lib.error_buffer()
+    h = _lib.load().fastpls_b200_model_import(
+        METHODS[method], precision, n, p, q, a, sc, int(cls), _p(R), _p(Qm), _p(T), _p(mx),
+        _p(sx), _p(my), _p(lab), err, cap)
+    if not h:
+        raise _lib.FastplsError(err.value.decode(errors="replace"))
+    return ResidentModel(handle=h, precision=precision, n=n, p=p, q=q, ncomp=a, method=method,
+                         classification=cls, feature_p=p)
+
+
 def cuda_gemm(left, right, precision=64):
     dt = _dtype(precision)
     a = _mat(left, dt)

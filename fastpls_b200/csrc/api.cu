@@ -330,6 +330,33 @@ void* fastpls_resident_simpls_create(const void* x, const void* y, const int* la
   });
 }
 
+void* fastpls_b200_model_import(int method, int precision, int n, int p, int q, int components,
+                                int scaling, int classification, const double* weights,
+                                const double* response_loadings, const double* scores,
+                                const double* mean_x, const double* scale_x, const double* mean_y,
+                                const int* labels, char* error, size_t error_capacity) {
+  return guarded_create(error, error_capacity, "unknown resident CUDA import error", [&]() -> void* {
+    if (precision != 32 && precision != 64 && precision != 16)
+      throw std::invalid_argument("invalid resident matrix or precision");
+    fpls::ImportRequest im;
+    im.method = method;
+    im.n = n;
+    im.p = p;
+    im.q = q;
+    im.components = components;
+    im.scaling = scaling;
+    im.classification = classification != 0;
+    im.R = weights;
+    im.Q = response_loadings;
+    im.T = scores;
+    im.mean = mean_x;
+    im.scale = scale_x;
+    im.ymean = mean_y;
+    im.labels = labels;
+    return fpls::import_handle(precision, im);
+  });
+}
+
 void* fastpls_resident_plssvd_create(const void* x, const void* y, const int* labels,
                                      int precision, int n, int p, int q, int components,
                                      int scaling, int oversample, int power, int retain_scores,

@@ -175,6 +175,15 @@ class TypedHandle final : public ResidentHandle {
       throw;
     }
   }
+  explicit TypedHandle(const ImportRequest& im) {
+    try {
+      FPLS_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+      load(im);
+    } catch (...) {
+      release();
+      throw;
+    }
+  }
   ~TypedHandle() override { release(); }
 
   void predict_path(const void* x, int rows, const int* prefixes, int count,
@@ -379,6 +388,59 @@ class TypedHandle final : public ResidentHandle {
         : "resident SIMPLS failed: invalid labels, decomposition or component norm");
   }
 
+  void load(const ImportRequest& im) {
+    const int n = im.n, p = im.p, q = im.q, a = im.components;
+    if (im.method != kSimpls && im.method != kOpls)
+      throw std::invalid_argument("model import supports SIMPLS and OPLS models");
+    if (p < 1 || q < 1 || a < 1 || a > p || !im.R || !im.Q || !im.mean || !im.scale || !im.ymean ||
+        im.scaling < 1 || im.scaling > 3)
+      throw std::invalid_argument("invalid imported model fields");
+    if (im.labels && (!im.T || !im.classification || n < 2))
+      throw std::invalid_argument("imported labels need the training scores of a classification model");
+    if (im.T && n < 1) throw std::invalid_argument("invalid imported model fields");
+    if (im.classification && q < 2)
+      throw std::invalid_argument("classification requires at least two classes");
+    for (int j = 0; j < p; ++j)
+      if (!std::isfinite(im.mean[j]) || !std::isfinite(im.scale[j]) || im.scale[j] == 0.0)
+        throw std::invalid_argument("invalid imported model fields");
+    rq_.method = im.method;
+    rq_.n = im.T ? n : 0;
+    rq_.p = p;
+    rq_.q = q;
+    rq_.components = a;
+    rq_.scaling = im.scaling;
+    model_.method = im.method;
+    model_.n = rq_.n;
+    model_.p = p;
+    model_.feature_p = p;
+    model_.m = q;
+    model_.a = a;
+    model_.scaling = im.scaling;
+    model_.classification = im.classification;
+    auto up = [&](DeviceArray<double>& dst, const double* src, size_t count) {
+      dst.allocate(count, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(dst.get(), src, sizeof(double) * count, cudaMemcpyHostToDevice, stream_));
+    };
+    up(model_.R, im.R, (size_t)p * a);
+    up(model_.Q, im.Q, (size_t)q * a);
+    up(model_.mean, im.mean, p);
+    up(model_.scale, im.scale, p);
+    up(model_.ymean, im.ymean, q);
+    if (im.T) up(model_.T, im.T, (size_t)n * a);
+    if (im.labels) {
+      model_.class_counts.assign(q, 0);
+      for (int i = 0; i < n; ++i) {
+        if (im.labels[i] < 1 || im.labels[i] > q) throw std::invalid_argument("invalid imported labels");
+        ++model_.class_counts[im.labels[i] - 1];
+      }
+      model_.labels.allocate(n, stream_);
+      FPLS_CHECK(cudaMemcpyAsync(model_.labels.get(), im.labels, sizeof(int) * n, cudaMemcpyHostToDevice,
+                                 stream_));
+    }
+    ws_.ensure(std::max(rq_.n, 1), p, q, a, stream_);
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
   const double* q_export() { return model_.Q.get(); }
 
   double* scores(int rows, int k) {
@@ -414,6 +476,8 @@ class TypedHandle final : public ResidentHandle {
   LdaState& lda_state() {
     if (!lda_) {
       if (!model_.classification) throw std::invalid_argument("LDA requires class labels");
+      if (!model_.T || !model_.labels)
+        throw std::invalid_argument("LDA requires the training scores and labels of the model");
       auto next = std::make_unique<LdaState>();
       next->train(model_.T.get(), model_.n, model_.n, model_.a, model_.labels.get(),
                   model_.m, model_.class_counts, ws_.flag.get(), stream_);
@@ -508,6 +572,13 @@ class TypedHandle final : public ResidentHandle {
   DeviceArray<int> top_;
   std::unique_ptr<LdaState> lda_;
 };
+
+ResidentHandle* import_handle(int precision, const ImportRequest& im) {
+  if (precision == 32) return new TypedHandle<float>(im);
+  if (precision == 64) return new TypedHandle<double>(im);
+  if (precision == 16) return new TypedHandle<bf16>(im);
+  throw std::invalid_argument("invalid resident matrix or precision");
+}
 
 ResidentHandle* make_handle(int precision, const FitRequest& rq) {
   if (precision == 32) return new TypedHandle<float>(rq);

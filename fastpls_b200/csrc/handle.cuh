@@ -49,4 +49,23 @@ struct FitRequest {
 
 ResidentHandle* make_handle(int precision, const FitRequest& request);
 
+// A fitted SIMPLS or OPLS model rebuilt from its exported fields (R, Q, the
+// predictor means and scales, the response means; optionally the training
+// scores T and labels for LDA), so a model saved by the host survives without
+// refitting. FP64 host arrays; `precision` is that of later prediction rows.
+struct ImportRequest {
+  int method = kSimpls;
+  int n = 0, p = 0, q = 0, components = 0, scaling = 1;
+  bool classification = false;
+  const double* R = nullptr;      // p x a
+  const double* Q = nullptr;      // q x a
+  const double* T = nullptr;      // n x a (optional)
+  const double* mean = nullptr;   // p
+  const double* scale = nullptr;  // p
+  const double* ymean = nullptr;  // q
+  const int* labels = nullptr;    // n, one-based (optional, needs T)
+};
+
+ResidentHandle* import_handle(int precision, const ImportRequest& request);
+
 }  // namespace fpls

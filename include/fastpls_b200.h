@@ -314,6 +314,23 @@ FASTPLS_B200_API int fastpls_b200_fastsvd_audited(const void* x, int precision, 
                                                   double* d, double* v, double* audit,
                                                   char* error, size_t error_capacity);
 
+/* Rebuild a resident SIMPLS (method 3) or OPLS (method 4) model from its
+ * exported fields, so a model saved by the host survives without refitting
+ * (today the reference's handle is lost on session save/load, "refit the
+ * model", src/cuda_resident_r.cpp:199-201). FP64 host arrays: weights =
+ * export field 0 (p x a), response_loadings = field 1 (q x a), mean_x /
+ * scale_x / mean_y = fields 3 / 4 / 5; scores = field 2 (n x a) and the
+ * one-based training labels are optional and enable LDA for a
+ * classification model. `precision` (16, 32, 64) is that of later prediction
+ * rows and results, as for the _create functions. Returns a handle released
+ * with fastpls_resident_simpls_destroy; fields 6 and 7 need the training
+ * predictors and are not available on an imported model. */
+FASTPLS_B200_API void* fastpls_b200_model_import(
+    int method, int precision, int n, int p, int q, int components, int scaling,
+    int classification, const double* weights, const double* response_loadings,
+    const double* scores, const double* mean_x, const double* scale_x,
+    const double* mean_y, const int* labels, char* error, size_t error_capacity);
+
 /* ---- serving loop (no counterpart in the reference) ---------------------
  * A server owns `workers` threads, each driving resident handles on its own
  * CUDA stream, and admits queued requests by their HBM footprint against
