@@ -205,6 +205,18 @@ class ResidentModel:
         _lib.check(rc, err)
         return out.reshape((self.q, 3))
 
+    def vip(self):
+        """Variable importance in projection (ViP()): an array of shape
+        (q, ncomp, feature_p), entry [r, c, j] for response r and the
+        component prefix 1..c+1."""
+        fp = self.feature_p or self.p
+        out = np.zeros(self.q * self.ncomp * fp)
+        err, cap = _lib.error_buffer()
+        rc = _lib.load().fastpls_b200_resident_vip(C.c_void_p(self.handle), _p(out), out.size,
+                                                   err, cap)
+        _lib.check(rc, err)
+        return out.reshape((self.q, fp, self.ncomp)).transpose(0, 2, 1)
+
     def controls(self):
         vals = [C.c_int(0) for _ in range(6)]
         err, cap = _lib.error_buffer()

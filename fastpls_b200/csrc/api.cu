@@ -489,6 +489,14 @@ int fastpls_resident_compact(void* model, int prepare_lda, char* error, size_t e
 }
 
 // ------------------------------------------------------------------ additions
+int fastpls_b200_resident_vip(void* model, double* out, size_t size, char* error,
+                              size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown VIP calculation error", [&] {
+    if (!model) throw std::invalid_argument("VIP requires a fitted fastPLS model");
+    static_cast<ResidentHandle*>(model)->vip(out, size);
+  });
+}
+
 int fastpls_b200_device_count(void) {
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess) {

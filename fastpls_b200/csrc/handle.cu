@@ -111,6 +111,45 @@ __global__ void column_sums_kernel(const double* __restrict__ M, int rows,
   if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
+__global__ void column_sumsq_kernel(const double* __restrict__ M, int rows,
+                                    long ld, double* out) {
+  __shared__ double scratch[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+    const double v = M[i + (long)blockIdx.x * ld];
+    s = fma(v, v, s);
+  }
+  s = block_sum(s, scratch);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+// Variable importance in projection per response and component prefix
+// (vip_values, src/r_api.cpp:3973-4025): with SS_c = q_rc^2 ||t_c||^2,
+// vip[r][c, j] = sqrt(fp * sum_{c' <= c} (w_jc'^2 / ||w_c'||^2) SS_c' /
+// sum_{c' <= c} SS_c'); NaN while the denominator is zero. out holds, per
+// response r, an a x fp column-major block at offset r a fp.
+__global__ void vip_kernel(const double* __restrict__ R, int fp, const double* __restrict__ Q,
+                           int m, const double* __restrict__ tss,
+                           const double* __restrict__ wss, int a, double* __restrict__ out) {
+  const long total = (long)m * fp;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / fp), j = (int)(idx % fp);
+    double num = 0.0, den = 0.0;
+    double* o = out + (long)r * a * fp + (long)j * a;
+    for (int c = 0; c < a; ++c) {
+      const double q = Q[r + (long)c * m];
+      const double explained = q * q * tss[c];
+      den += explained;
+      if (wss[c] > 0.0) {
+        const double w = R[j + (long)c * fp];
+        num += w * w * explained / wss[c];
+      }
+      o[c] = den > 0.0 ? sqrt(fp * num / den) : nan("");
+    }
+  }
+}
+
 // result[j] = ||sequential_j||^2 * gram_jj ; result[a] = sum_j column SS of Xs
 __global__ void variance_finish_kernel(const double* __restrict__ sequential,
                                        const double* __restrict__ gram,
@@ -305,6 +344,24 @@ class TypedHandle final : public ResidentHandle {
     if (!src) throw std::invalid_argument("resident field is not available after compaction");
     conv_.reserve(size, stream_);
     download(src, (long)size, static_cast<TO*>(out));
+    FPLS_CHECK(cudaStreamSynchronize(stream_));
+  }
+
+  void vip(double* out, std::size_t size) override {
+    const int a = model_.a, m = model_.m, fp = model_.feature_p;
+    if (!out || size != (std::size_t)m * a * fp)
+      throw std::invalid_argument("invalid resident VIP output size");
+    if (model_.method == kPlssvd && !model_.Q)
+      throw std::invalid_argument("VIP requires response loadings");
+    if (!model_.T) throw std::invalid_argument("VIP requires a model fitted with fit = TRUE");
+    DeviceArray<double> tss(a, stream_), wss(a, stream_), res(size, stream_);
+    column_sumsq_kernel<<<a, 256, 0, stream_>>>(model_.T.get(), model_.n, model_.n, tss.get());
+    column_sumsq_kernel<<<a, 256, 0, stream_>>>(model_.R.get(), fp, fp, wss.get());
+    vip_kernel<<<(unsigned)std::min<long>(((long)m * fp + 255) / 256, 8L * num_sms()), 256, 0, stream_>>>(
+        model_.R.get(), fp, q_export(), m, tss.get(), wss.get(), a, res.get());
+    count_launch(3);
+    FPLS_LAUNCH("vip");
+    FPLS_CHECK(cudaMemcpyAsync(out, res.get(), sizeof(double) * size, cudaMemcpyDeviceToHost, stream_));
     FPLS_CHECK(cudaStreamSynchronize(stream_));
   }
 

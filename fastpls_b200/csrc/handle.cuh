@@ -32,6 +32,7 @@ class ResidentHandle {
                         int* block_limit, int* implicit_operator,
                         int* crossprod_cache) = 0;
   virtual void compact(bool prepare_lda) = 0;
+  virtual void vip(double* out, std::size_t size) = 0;
 };
 
 struct FitRequest {

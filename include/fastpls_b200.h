@@ -314,6 +314,16 @@ FASTPLS_B200_API int fastpls_b200_fastsvd_audited(const void* x, int precision, 
                                                   double* d, double* v, double* audit,
                                                   char* error, size_t error_capacity);
 
+/* Variable importance in projection of a resident model (ViP(),
+ * R/main.R:12769, vip_values in src/r_api.cpp:3973-4025) computed on the
+ * device from R, Q and the training scores: for response r, component prefix
+ * c and feature j, sqrt(fp * sum_{c' <= c} (R_jc'^2 / ||R_c'||^2) SS_c' /
+ * sum_{c' <= c} SS_c') with SS_c = Q_rc^2 ||T_c||^2 (NaN while the
+ * denominator is zero). out (FP64, size = q * a * fp doubles, fp = rows of
+ * export field 0) holds per response an a x fp column-major block. */
+FASTPLS_B200_API int fastpls_b200_resident_vip(void* model, double* out, size_t size,
+                                               char* error, size_t error_capacity);
+
 /* Rebuild a resident SIMPLS (method 3) or OPLS (method 4) model from its
  * exported fields, so a model saved by the host survives without refitting
  * (today the reference's handle is lost on session save/load, "refit the

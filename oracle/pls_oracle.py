@@ -36,7 +36,7 @@ __all__ = [
     "row_argmax", "topk", "response_sums", "cv_regression", "opls_fit",
     "opls_predict", "kernelpls_fit", "kernelpls_predict",
     "cv_classification", "permutation_pvalue", "align_signs", "rel_err",
-    "fastcor",
+    "fastcor", "vip",
 ]
 
 
@@ -607,6 +607,29 @@ def permutation_pvalue(permuted, observed, lower_tail=False):
 # --------------------------------------------------------------------------
 # comparison helpers
 # --------------------------------------------------------------------------
+def vip(R, Q, T):
+    """Variable importance in projection (vip_values, src/r_api.cpp:3973-4025):
+    array (q, a, p); entry [r, c, j] = sqrt(p * sum_{c'<=c} (R_jc'^2 /
+    ||R_c'||^2) SS_c' / sum_{c'<=c} SS_c') with SS_c = Q_rc^2 ||T_c||^2."""
+    R = np.asarray(R, dtype=np.float64)
+    Q = np.asarray(Q, dtype=np.float64)
+    T = np.asarray(T, dtype=np.float64)
+    p, a = R.shape
+    tss = (T * T).sum(axis=0)
+    wss = (R * R).sum(axis=0)
+    wn = np.where(wss > 0, R * R / np.where(wss > 0, wss, 1.0), 0.0)   # p x a
+    out = np.empty((Q.shape[0], a, p))
+    for r in range(Q.shape[0]):
+        expl = Q[r] ** 2 * tss                     # a
+        den = np.cumsum(expl)
+        num = np.cumsum(wn * expl, axis=1)         # p x a
+        with np.errstate(invalid="ignore", divide="ignore"):
+            val = np.sqrt(p * num / den)
+        val[:, den <= 0] = np.nan
+        out[r] = val.T
+    return out
+
+
 def align_signs(test, ref):
     """Flip columns of ``test`` so each has a non-negative inner product with
     the matching column of ``ref`` (singular-vector sign alignment)."""
