@@ -39,6 +39,9 @@ namespace fpls {
 namespace {
 
 constexpr int BT = 256;
+// The deflation runs one CTA per instance through dependent phases; 128
+// threads keep every instance of a lane (~670) resident in one wave.
+constexpr int DEFL_BT = 128;
 
 struct InstanceView {
   int n, q, kmax, B;        // rows, responses, max components, perms per fold
@@ -765,11 +768,11 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
       gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);
       const size_t smem_defl = (2 * (size_t)q * q + 2 * (size_t)kmax + q) * sizeof(double);
       if (q <= 4)
-        deflate_batched<4><<<c, BT, smem_defl, st>>>(v, L.Y1.get(), L.U.get(), L.Wb.get(),
+        deflate_batched<4><<<c, DEFL_BT, smem_defl, st>>>(v, L.Y1.get(), L.U.get(), L.Wb.get(),
                                                      L.KWb.get(), L.Ws.get(), L.C.get(),
                                                      L.G.get(), a, flag.get());
       else
-        deflate_batched<kBatchMaxResponses><<<c, BT, smem_defl, st>>>(
+        deflate_batched<kBatchMaxResponses><<<c, DEFL_BT, smem_defl, st>>>(
             v, L.Y1.get(), L.U.get(), L.Wb.get(), L.KWb.get(), L.Ws.get(), L.C.get(), L.G.get(),
             a, flag.get());
       count_launch();
