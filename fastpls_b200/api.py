@@ -539,6 +539,42 @@ def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64, audit=False)
     return u, d, v
 
 
+def cv_permutation_classification(X, labels, classes, folds, permutations, prefixes,
+                                  scaling="centering", precision=32, digits=None):
+    """Batched classification CV over the observed labels and their row
+    permutations (``fastpls_b200_simpls_cv_permutation_classification``,
+    argmax head). Returns dict(accuracy=(permutations + 1, prefixes), status)."""
+    if digits is not None:
+        old = product_digits()
+        set_product_digits(digits)
+        try:
+            return cv_permutation_classification(X, labels, classes, folds, permutations,
+                                                 prefixes, scaling, precision, None)
+        finally:
+            set_product_digits(old)
+    dt = _dtype(precision)
+    x = _mat(X, dt)
+    n, p = x.shape
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    folds = np.ascontiguousarray(folds, dtype=np.int32)
+    perms = None
+    P = 0
+    if permutations is not None and len(permutations):
+        perms = np.ascontiguousarray(permutations, dtype=np.int32)
+        P = perms.shape[0]
+    pre = np.ascontiguousarray(prefixes, dtype=np.int32)
+    k = len(pre)
+    acc = np.zeros((P + 1) * k)
+    status = np.zeros(int(folds.max()), dtype=np.int32)
+    sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
+    err, cap = _lib.error_buffer()
+    rc = _lib.load().fastpls_b200_simpls_cv_permutation_classification(
+        _p(x), _p(lab), _p(folds), _p(perms), P, precision, n, p, int(classes), _p(pre), k, sc,
+        _p(acc), _p(status), err, cap)
+    _lib.check(rc, err)
+    return dict(accuracy=acc.reshape((P + 1, k)), status=status)
+
+
 class Server:
     """Serving loop on the device (fastpls_b200_server_*): continuous
     admission of fit and predict requests by HBM footprint, resident models,

@@ -193,6 +193,93 @@ void cv_permutation(const void* predictors, const void* responses,
   }
 }
 
+// Classification CV x permutations on the batched engine: one-hot
+// indicators of the (permuted) labels as responses, the argmax head over the
+// classes present in each training fold (src/cuda_resident_api.cuh:620-745,
+// without LDA), accuracy per permutation and prefix. Training folds must hold
+// at least two classes and stay below the candidate-block threshold of
+// classification SIMPLS (n_train p classes < 5e8 or fewer than 4 components),
+// since the engine refreshes the direction every component.
+template <class T>
+void cv_permutation_classification(const T* predictors, const int* labels, const int* folds,
+                                   const int* permutations, int permutation_count, int n, int p,
+                                   int classes, const int* prefixes, int prefix_count,
+                                   int scaling, double* accuracy, int* status) {
+  if (!predictors || !labels || !folds || !prefixes || !accuracy || n < 2 || p < 1 ||
+      classes < 2 || classes > kBatchMaxResponses || prefix_count < 1 || scaling < 1 ||
+      scaling > 3 || permutation_count < 0 || (permutation_count > 0 && !permutations))
+    throw std::invalid_argument("invalid batched CUDA classification CV input");
+  int folds_n = 0;
+  for (int i = 0; i < n; ++i) {
+    if (labels[i] < 1 || labels[i] > classes || folds[i] < 0)
+      throw std::invalid_argument("invalid batched CUDA classification CV input");
+    folds_n = std::max(folds_n, folds[i]);
+  }
+  const int kmax = prefixes[prefix_count - 1];
+  const int B = permutation_count + 1;
+  std::vector<int> count((size_t)classes);
+  for (int b = 0; b < B; ++b)
+    for (int f = 1; f <= folds_n; ++f) {
+      std::fill(count.begin(), count.end(), 0);
+      int ntrain = 0, nheld = 0;
+      for (int r = 0; r < n; ++r) {
+        if (folds[r] == f) {
+          ++nheld;
+          continue;
+        }
+        const int src = b == 0 ? r : permutations[(size_t)(b - 1) * n + r];
+        if (src < 0 || src >= n) throw std::invalid_argument("invalid batched CUDA classification CV input");
+        ++count[labels[src] - 1];
+        ++ntrain;
+      }
+      if (nheld == 0) continue;
+      int active = 0;
+      for (int c = 0; c < classes; ++c) active += count[c] > 0;
+      if (active < 2)
+        throw std::invalid_argument("batched classification CV needs two classes in every training fold");
+      if (kmax >= 4 && (double)ntrain * p * active >= 5.0e8)
+        throw std::invalid_argument(
+            "batched classification CV does not take candidate blocks (n_train p classes >= 5e8); "
+            "use fastpls_resident_simpls_cv_classification");
+    }
+  std::vector<T> onehot((size_t)n * classes, T(0));
+  std::vector<int> zero_based(n);
+  for (int i = 0; i < n; ++i) {
+    onehot[(size_t)(labels[i] - 1) * n + i] = T(1);
+    zero_based[i] = labels[i] - 1;
+  }
+  cudaStream_t s = caller_stream();
+  const bool own = s == nullptr;
+  if (own) FPLS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct Guard {
+    cudaStream_t s;
+    bool own;
+    ~Guard() {
+      cudaStreamSynchronize(s);
+      if (own) cudaStreamDestroy(s);
+    }
+  } guard{s, own};
+  {
+    DeviceArray<T> X((size_t)n * p, s), Y((size_t)n * classes, s);
+    DeviceArray<int> P, L(n, s);
+    FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+    FPLS_CHECK(cudaMemcpyAsync(Y.get(), onehot.data(), sizeof(T) * n * classes, cudaMemcpyHostToDevice, s));
+    FPLS_CHECK(cudaMemcpyAsync(L.get(), zero_based.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    if (permutation_count > 0) {
+      P.allocate((size_t)permutation_count * n, s);
+      FPLS_CHECK(cudaMemcpyAsync(P.get(), permutations, sizeof(int) * permutation_count * n,
+                                 cudaMemcpyHostToDevice, s));
+    }
+    BatchedCv<T> engine;
+    engine.class_labels = L.get();
+    engine.run(X.get(), n, p, Y.get(), classes, folds, P.get(), permutation_count, prefixes,
+               prefix_count, scaling, s);
+    engine.accuracy(accuracy);
+    if (status)
+      for (size_t f = 0; f < engine.status.size(); ++f) status[f] = engine.status[f];
+  }
+}
+
 }  // namespace
 }  // namespace fpls
 
@@ -610,6 +697,25 @@ int fastpls_b200_simpls_cv_permutation(
       cv_permutation<double>(predictors, responses, folds, permutations, permutation_count, n, p, q,
                              prefixes, prefix_count, scaling, metric, metrics, q2, rmsd, observed_r2,
                              status, false);
+  });
+}
+
+int fastpls_b200_simpls_cv_permutation_classification(
+    const void* predictors, const int* labels, const int* folds, const int* permutations,
+    int permutation_count, int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, double* accuracy, int* status, char* error,
+    size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown batched CUDA CV error", [&] {
+    if (precision != 32 && precision != 64)
+      throw std::invalid_argument("invalid batched CUDA CV precision");
+    if (precision == 32)
+      cv_permutation_classification<float>(static_cast<const float*>(predictors), labels, folds,
+                                           permutations, permutation_count, n, p, classes, prefixes,
+                                           prefix_count, scaling, accuracy, status);
+    else
+      cv_permutation_classification<double>(static_cast<const double*>(predictors), labels, folds,
+                                            permutations, permutation_count, n, p, classes,
+                                            prefixes, prefix_count, scaling, accuracy, status);
   });
 }
 

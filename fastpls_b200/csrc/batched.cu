@@ -54,10 +54,43 @@ struct InstanceView {
   const int* test_rows;     // concatenated held-out rows per fold
   const int* test_off;      // F + 1
   const double* Y;          // n x q base responses (FP64)
+  const int* labels;        // n zero-based classes of the base rows, or null
+                            // (regression); classification counts hits
 };
 
 __device__ __forceinline__ int src_row(const InstanceView& v, int perm, int r) {
   return perm < 0 ? r : v.perms[(long)perm * v.n + r];
+}
+
+// One held-out row at a prefix slot: squared error over the responses
+// (regression), or 1 when the argmax over the classes present in the
+// instance's training rows (prior > 0; first index wins ties) is the row's
+// class (classification, as the reference's argmax head over its active
+// classes, src/cuda_resident_api.cuh:700-745).
+__device__ __forceinline__ double heldout_term(const InstanceView& v, int i, int b, int r,
+                                               const double* ymean, const double* yh, long ld) {
+  const int q = v.q;
+  if (v.labels) {
+    int best = -1;
+    double bv = 0.0;
+    for (int c = 0; c < q; ++c) {
+      const double ym = ymean[(long)i * q + c];
+      if (ym > 0.0) {
+        const double score = ym + yh[(long)c * ld];
+        if (best < 0 || score > bv) {
+          best = c;
+          bv = score;
+        }
+      }
+    }
+    return best == v.labels[src_row(v, b, r)] ? 1.0 : 0.0;
+  }
+  double err = 0.0;
+  for (int c = 0; c < q; ++c) {
+    const double e = v.Y[src_row(v, b, r) + (long)c * v.n] - (ymean[(long)i * q + c] + yh[(long)c * ld]);
+    err = fma(e, e, err);
+  }
+  return err;
 }
 
 // C0 (n x q) = responses of this instance centred over its training rows
@@ -250,14 +283,9 @@ __global__ void scores_batched(InstanceView v, const double* Y1, double* Tm,
   for (int k = threadIdx.x; k < nte; k += blockDim.x) {
     const int r = te[k];
     const double tt = (y[r] - mu) * inv;
-    for (int c = 0; c < q; ++c) {
-      const double val = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
-      yh[k + (long)c * yhat_ld] = val;
-      if (slot >= 0) {
-        const double e = v.Y[src_row(v, b, r) + (long)c * n] - (ymean[(long)i * q + c] + val);
-        err = fma(e, e, err);
-      }
-    }
+    for (int c = 0; c < q; ++c)
+      yh[k + (long)c * yhat_ld] = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
+    if (slot >= 0) err += heldout_term(v, i, b, r, ymean, yh + k, yhat_ld);
   }
   if (slot >= 0) {
     err = block_sum(err, scratch);
@@ -468,14 +496,9 @@ __global__ void __launch_bounds__(BT)
   for (int k = threadIdx.x; k < nte; k += blockDim.x) {
     const int r = te[k];
     const double tt = (y[r] - mu) * inv;
-    for (int c = 0; c < q; ++c) {
-      const double pv = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
-      yh[k + (long)c * yhat_ld] = pv;
-      if (slot >= 0) {
-        const double e = v.Y[src_row(v, b, r) + (long)c * n] - (ymean[(long)i * q + c] + pv);
-        err = fma(e, e, err);
-      }
-    }
+    for (int c = 0; c < q; ++c)
+      yh[k + (long)c * yhat_ld] = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
+    if (slot >= 0) err += heldout_term(v, i, b, r, ymean, yh + k, yhat_ld);
   }
   if (slot >= 0) {
     err = block_sum(err, scratch);
@@ -707,6 +730,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     v.test_rows = d_test_rows.get();
     v.test_off = d_test_off.get();
     v.Y = Y64.get();
+    v.labels = class_labels;
     L.C0.allocate(nq * c, st);
     L.C.allocate(nq * c, st);
     L.G.allocate((size_t)c * q * (q + 1) / 2, st);
@@ -848,6 +872,8 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
       throw std::invalid_argument("CUDA CV component count exceeds a fold rank");
     status[f] = test[f].empty() ? 2 : 1;
   }
+  heldout.assign(folds, 0);
+  for (int f = 0; f < folds; ++f) heldout[f] = (int)test[f].size();
   std::vector<int> slot(kmax + 1, -1);
   for (int j = 0; j < count; ++j) slot[prefixes_[j] - 1] = j;
   d_fold.allocate(n, s);
@@ -962,6 +988,22 @@ void BatchedCv<T>::metrics(int metric, double* metric_out, double* q2,
       if (metric_out) metric_out[o] = metric == 4 ? rm : metric == 3 ? qq : rr;
     }
   }
+}
+
+template <class T>
+void BatchedCv<T>::accuracy(double* out) const {
+  const int B = P + 1;
+  for (int b = 0; b < B; ++b)
+    for (int j = 0; j < prefix_count; ++j) {
+      double hits = 0.0, rows = 0.0;
+      for (int f = 0; f < folds; ++f) {
+        if (status[f] != 1) continue;
+        hits += inst_sse[((size_t)b * folds + f) * prefix_count + j];
+        rows += heldout[f];
+      }
+      out[(size_t)b * prefix_count + j] =
+          rows > 0 ? hits / rows : std::numeric_limits<double>::quiet_NaN();
+    }
 }
 
 template struct BatchedCv<float>;

@@ -27,10 +27,18 @@ struct BatchedCv {
   // index b * prefix_count + j, b = 0 the observed responses.
   void metrics(int metric, double* metric_out, double* q2, double* rmsd,
                double* r2) const;
+  // Classification (class_labels set before run): held-out accuracy of the
+  // argmax head per (permutation + 1) x prefix, same layout as metrics.
+  void accuracy(double* out) const;
+
+  // zero-based class of each base row (device, n) for classification, with
+  // Y the one-hot indicator of the classes; null for regression
+  const int* class_labels = nullptr;
 
   std::vector<int> status;          // per fold: 1 fitted, 2 empty
   std::vector<double> inst_sse;     // (P+1) x folds x prefixes
   std::vector<double> inst_sst;     // (P+1) x folds
+  std::vector<int> heldout;         // held-out rows per fold
   long double total_ss = 0.0L;
 
  private:

@@ -262,6 +262,24 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation(
     int metric, double* metrics, double* q2, double* rmsd,
     double* observed_r2, int* status, char* error, size_t error_capacity);
 
+/* Classification counterpart of fastpls_b200_simpls_cv_permutation (the
+ * classification perm.test of pls.single.cv, CPU-only in the reference,
+ * R/main.R:9419-9450): one-based labels (n, 1..classes, classes <= 32),
+ * folds and zero-based permutations as there; responses are the one-hot
+ * indicators of the permuted labels, each fold fit predicts the argmax over
+ * the classes present in its training rows (the reference's argmax head,
+ * src/cuda_resident_api.cuh:620-745; no LDA). accuracy ((B + 1) x
+ * prefix_count, row-major, B = permutation_count, row 0 the observed labels):
+ * held-out accuracy per prefix. Every training fold must hold two classes,
+ * and n_train p classes must stay below 5e8 when the path has 4 or more
+ * components (the reference switches to candidate blocks there); other
+ * inputs fail with an error. */
+FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_classification(
+    const void* predictors, const int* labels, const int* folds, const int* permutations,
+    int permutation_count, int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, double* accuracy, int* status, char* error,
+    size_t error_capacity);
+
 /* As above with predictors, responses, folds and permutations already in
  * device memory (prefixes and outputs stay on the host). */
 FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_device(

@@ -123,3 +123,37 @@ def test_batched_response_counts(q):
         ref = O.cv_regression(x, yb, folds, pre, family=3)
         for key in ("q2", "rmsd", "observed_r2"):
             assert np.allclose(got[key][b], ref[key], rtol=1e-9, atol=1e-11), (b, key)
+
+
+@pytest.mark.parametrize("digits", [0, 6])
+@pytest.mark.parametrize("scaling", [1, 2])
+def test_batched_classification_permutations(digits, scaling):
+    n, p, classes = 260, 150, 4
+    x, lab = W.latent_classification(n, p, classes, 3, 0.5, 41, dtype=np.float32)
+    lab = lab.copy()
+    lab[7] = 5          # a fifth class with one row: absent from four training folds
+    classes = 5
+    folds = W.uneven_folds(n, 5, 41)
+    perms = W.permutations(n, 3, 41)
+    pre = [1, 2, 4, 6]
+    got = api.cv_permutation_classification(x, lab, classes, folds, perms, pre,
+                                            scaling=scaling, digits=digits)
+    x64 = x.astype(np.float64)
+    for b in range(4):
+        lb = lab if b == 0 else lab[perms[b - 1]]
+        want = O.cv_classification(x64, lb, classes, folds, pre, scaling=scaling)["metrics"]
+        if digits == 0:
+            assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
+        else:   # int8 products: at most one borderline row may flip
+            assert np.all(np.abs(got["accuracy"][b] - want) <= 1.0 / n + 1e-12)
+    assert list(got["status"]) == [1] * 5
+
+
+def test_batched_classification_rejects_single_class_folds():
+    n = 120
+    x, _ = W.latent_classification(n, 40, 2, 3, 0.5, 42, dtype=np.float32)
+    folds = W.uneven_folds(n, 4, 42)
+    lab = np.ones(n, dtype=np.int32)
+    lab[folds == 1] = 2          # class 2 only in fold 1: its training rows hold one class
+    with pytest.raises(api._lib.FastplsError, match="two classes"):
+        api.cv_permutation_classification(x, lab, 2, folds, None, [1, 2])
