@@ -166,7 +166,7 @@ __device__ void dominant_z(const InstanceView& v, int i, const double* G, int* f
       A[d + c * q] = g[c * (c + 1) / 2 + d];
     }
   __syncthreads();
-  jacobi_eigen_warp(A, E, q);
+  jacobi_eigen(A, E, q);
   __syncthreads();
   if (threadIdx.x == 0) {
     int best = 0;

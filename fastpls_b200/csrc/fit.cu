@@ -129,7 +129,7 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
       A[d + c * m] = v;
     }
   __syncthreads();
-  jacobi_eigen_warp(A, E, m);
+  jacobi_eigen(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long taken = 0ull;  // m <= 64
@@ -430,7 +430,7 @@ void dominant_direction(const double* S, int p, int m, const double* gpk,
   const size_t smem_dir = 2 * (size_t)m * m * sizeof(double);
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
-  direction_kernel<<<1, 64, smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get(), 1);
+  direction_kernel<<<1, jacobi_threads(m), smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get(), 1);
   s_times_z<<<std::min<unsigned>(ceil_div(p, TB), 4 * num_sms()), TB, 0, s>>>(S, p, m, zs, w);
   count_launch(2);
   FPLS_LAUNCH("dominant_direction");
@@ -533,7 +533,7 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
     if (jb == use) {
       use = std::min(block, a_max - a);
       jb = 0;
-      direction_kernel<<<1, 64, smem_dir, stream>>>(gpk, m, use > 1 ? zblk.get() : zs, scal + 3,
+      direction_kernel<<<1, jacobi_threads(m), smem_dir, stream>>>(gpk, m, use > 1 ? zblk.get() : zs, scal + 3,
                                                     ws.flag.get(), use);
       count_launch();
       FPLS_LAUNCH("direction_kernel");

@@ -34,7 +34,7 @@ __global__ void small_svd_kernel(const double* __restrict__ gpk, int m, int k,
       A[d + c * m] = v;
     }
   __syncthreads();
-  jacobi_eigen_warp(A, E, m);
+  jacobi_eigen(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 0; i < m; ++i) order[i] = i;
@@ -138,7 +138,7 @@ void fit_plssvd(const T* X, int n, int p, long ld, const double* Yc,
   const size_t smem = 2 * (size_t)m * m * sizeof(double) + m * sizeof(int) + 16;
   if (smem > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(small_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  small_svd_kernel<<<1, 64, smem, stream>>>(gpk, m, k, model.sigma.get(),
+  small_svd_kernel<<<1, jacobi_threads(m), smem, stream>>>(gpk, m, k, model.sigma.get(),
                                             model.Q.get(), Z.get(), ws.flag.get());
   count_launch();
   FPLS_LAUNCH("small_svd");

@@ -5,95 +5,118 @@
 
 namespace fpls {
 
-// Jacobi eigen-decomposition of a symmetric m x m matrix held in shared
-// memory (column-major A[i + j*m]); eigenvectors accumulate in E.
+// Jacobi eigen-decomposition of a symmetric m x m matrix (m <= 128) held in
+// shared memory (column-major A[i + j*m]); eigenvectors accumulate in E.
 // Parallel ordering (Brent-Luk round robin): each sweep runs m - 1 (m even)
-// or m (m odd) rounds of disjoint rotations. The rotations of a round go in
-// groups of 32, one per lane: each lane computes its rotation, then the group
-// is applied (columns of A and E, then rows of A). Rotations of one round
-// touch disjoint rows and columns, so a rotation's 2 x 2 block is unchanged
-// by the others of its round. Each rotation annihilates A[p, q] as in the
-// classical cyclic method (tangent of the smaller root of t^2 + 2 theta t = 1,
-// theta = (a_qq - a_pp) / (2 a_pq)).
-// Executed by the first warp of the block; the caller synchronises after.
-// Returns the number of sweeps used (<= max_sweeps). GMAX bounds the groups
-// of 32 rotations per round: m <= 64 GMAX.
-template <int GMAX = 1>
-__device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
-                                        int max_sweeps = 40) {
-  const int lane = threadIdx.x & 31;
-  if (threadIdx.x >= 32) return 0;
-  for (int k = lane; k < m * m; k += 32) E[k] = (k % m == k / m) ? 1.0 : 0.0;
-  __syncwarp();
+// or m (m odd) rounds of up to m / 2 disjoint rotations. All threads of the
+// block cooperate (every thread must call it, with the same arguments): the
+// rotations of a round are computed one per thread into shared memory, then
+// applied together, element by element over the block (columns of A and E,
+// then rows of A). Rotations of one round touch disjoint rows and columns, so
+// a rotation's 2 x 2 block is unchanged by the others of its round. Each
+// rotation annihilates A[p, q] as in the classical cyclic method (tangent of
+// the smaller root of t^2 + 2 theta t = 1, theta = (a_qq - a_pp) / (2 a_pq)).
+// Stops at off <= 1e-30 diag (sums of squares) or at the rounding floor.
+// Returns the number of sweeps used (<= max_sweeps).
+constexpr int kJacobiMaxRotations = 64;
+
+// threads for a block that runs jacobi_eigen on an m x m matrix
+inline unsigned jacobi_threads(int m) { return m > 16 ? 256u : 64u; }
+
+__device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps = 40) {
+  __shared__ int rot_p[kJacobiMaxRotations], rot_q[kJacobiMaxRotations];
+  __shared__ double rot_c[kJacobiMaxRotations], rot_s[kJacobiMaxRotations];
+  __shared__ double red[32];
+  if (m > 2 * kJacobiMaxRotations) return 0;  // callers keep m <= 128
+  // small matrices: the first warp alone (warp barriers are cheaper than
+  // block barriers on the latency-bound path); the other threads wait at the
+  // final barrier
+  const bool warp_only = m <= 8;
+  if (warp_only && threadIdx.x >= 32) {
+    __syncthreads();
+    return 0;
+  }
+  const int tid = threadIdx.x, nt = warp_only ? 32 : (int)blockDim.x;
+  auto sync = [&]() {
+    if (warp_only) __syncwarp();
+    else __syncthreads();
+  };
+  auto total = [&](double v) { return warp_only ? warp_sum(v) : block_sum(v, red); };
+  for (int k = tid; k < m * m; k += nt) E[k] = (k % m == k / m) ? 1.0 : 0.0;
+  sync();
   const int players = m + (m & 1);  // a dummy player for odd m sits out
-  const int half = players / 2;     // rotations per round
-  const int groups = (half + 31) / 32;
-  // round-robin schedule (circle method): slot 0 pairs the fixed player
-  // players-1 with player `round`; slot s >= 1 pairs (round + s) and
-  // (round - s) modulo players-1, so both advance by one each round
-  int sa[GMAX], sb[GMAX];  // this lane's slots g*32 + lane, g < groups
+  const int half = players / 2;     // rotations per round (<= 64)
   const int wrap = players - 1;
-  // this lane's first work item (rotation k, row i) of a group, and the
-  // step between items 32 apart: k += dk, i += di with carry
-  const int dk = 32 / m, di = 32 % m;
-  const int k0 = lane / m, i0 = lane % m;
+  const int work = half * m;
+  // this thread's first work item (rotation k, row i) and the step nt
+  // between its items: k += dk, i += di with carry
+  const int dk = nt / m, di = nt % m;
+  const int k0 = tid / m, i0 = tid % m;
   int sweep = 0;
   double prev = 0.0;
   for (; sweep < max_sweeps && m > 1; ++sweep) {
     double off = 0.0, diag = 0.0;
-    for (int k = lane; k < m * m; k += 32) {
+    for (int k = tid; k < m * m; k += nt) {
       const int i = k % m, j = k / m;
       if (i != j) off += A[k] * A[k];
       else diag += A[k] * A[k];
     }
-    off = warp_sum(off);
-    diag = warp_sum(diag);
+    off = total(off);
+    diag = total(diag);
     if (off <= 1e-30 * diag || off == 0.0) break;
     // at the rounding floor (large m) the off-diagonal mass stops shrinking
     if (sweep > 0 && off <= 1e-24 * diag && off > 0.25 * prev) break;
     prev = off;
-#pragma unroll
-    for (int g = 0; g < GMAX; ++g) {
-      const int slot = g * 32 + lane;
-      sa[g] = slot == 0 ? wrap : slot % wrap;
-      sb[g] = slot == 0 ? 0 : (wrap - slot % wrap) % wrap;
-    }
+    // this thread's slot `tid` (one per thread when nt >= half) advances
+    // incrementally; further slots (nt < half) use the closed form
+    int sa = tid == 0 ? wrap : tid % wrap;
+    int sb = tid == 0 ? 0 : (wrap - tid % wrap) % wrap;
     for (int round = 0; round < wrap; ++round) {
-#pragma unroll
-      for (int g = 0; g < GMAX; ++g) {
-        if (g >= groups) break;
-        const int count = min(32, half - g * 32);
-        int p = 0, q = 0;
-        double c = 1.0, s = 0.0;
-        if (lane < count) {
-          const int a = min(sa[g], sb[g]), b = max(sa[g], sb[g]);
-          if (b < m) {
-            p = a;
-            q = b;
-            const double apq = A[p + q * m];
-            if (apq != 0.0) {
-              // t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)) with
-              // theta = d / e, d = a_qq - a_pp, e = 2 a_pq, written as
-              // sgn(d) e / (|d| + sqrt(d^2 + e^2)): one square root and one
-              // division on the dependent path instead of two of each
-              const double d = A[q + q * m] - A[p + p * m], e = 2.0 * apq;
-              const double tt = (d >= 0 ? e : -e) / (fabs(d) + sqrt(fma(d, d, e * e)));
-              c = rsqrt(fma(tt, tt, 1.0));
-              s = tt * c;
-            }
-          }
+      for (int slot = tid; slot < half; slot += nt) {
+        // circle method: player players-1 fixed, the others rotate
+        int a = slot == tid ? sa : (slot == 0 ? wrap : (round + slot) % wrap);
+        int b = slot == tid ? sb : (slot == 0 ? round : (round - slot + wrap) % wrap);
+        if (a > b) {
+          const int t = a;
+          a = b;
+          b = t;
         }
-        __syncwarp();
-        const int work = count * m;
-        // A <- A J and E <- E J: columns p, q of every rotation of the group
+        double c = 1.0, s = 0.0;
+        if (b < m) {
+          const double apq = A[a + b * m];
+          if (apq != 0.0) {
+            // t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)) with
+            // theta = d / e, d = a_qq - a_pp, e = 2 a_pq, written as
+            // sgn(d) e / (|d| + sqrt(d^2 + e^2)): one square root and one
+            // division on the dependent path instead of two of each
+            const double d = A[b + b * m] - A[a + a * m], e = 2.0 * apq;
+            const double tt = (d >= 0 ? e : -e) / (fabs(d) + sqrt(fma(d, d, e * e)));
+            c = rsqrt(fma(tt, tt, 1.0));
+            s = tt * c;
+          }
+        } else {
+          a = b = 0;
+        }
+        rot_p[slot] = a;
+        rot_q[slot] = b;
+        rot_c[slot] = c;
+        rot_s[slot] = s;
+      }
+      if (tid == 0) {
+        ++sb;
+      } else {
+        sa = sa + 1 == wrap ? 0 : sa + 1;
+        sb = sb + 1 == wrap ? 0 : sb + 1;
+      }
+      sync();
+      // A <- A J and E <- E J: columns p, q of every rotation of the round
+      {
         int k = k0, i = i0;
-        for (int w = lane; w - lane < work; w += 32) {
-          const int kk = w < work ? k : 0;
-          const int pk = __shfl_sync(0xffffffffu, p, kk);
-          const int qk = __shfl_sync(0xffffffffu, q, kk);
-          const double ck = __shfl_sync(0xffffffffu, c, kk);
-          const double sk = __shfl_sync(0xffffffffu, s, kk);
-          if (w < work && sk != 0.0) {
+        for (int w = tid; w < work; w += nt) {
+          const double sk = rot_s[k];
+          if (sk != 0.0) {
+            const int pk = rot_p[k], qk = rot_q[k];
+            const double ck = rot_c[k];
             const double akp = A[i + pk * m], akq = A[i + qk * m];
             A[i + pk * m] = ck * akp - sk * akq;
             A[i + qk * m] = sk * akp + ck * akq;
@@ -108,17 +131,16 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
             ++k;
           }
         }
-        __syncwarp();
-        // A <- J^T A: rows p, q of every rotation of the group
-        k = k0;
-        i = i0;
-        for (int w = lane; w - lane < work; w += 32) {
-          const int kk = w < work ? k : 0;
-          const int pk = __shfl_sync(0xffffffffu, p, kk);
-          const int qk = __shfl_sync(0xffffffffu, q, kk);
-          const double ck = __shfl_sync(0xffffffffu, c, kk);
-          const double sk = __shfl_sync(0xffffffffu, s, kk);
-          if (w < work && sk != 0.0) {
+      }
+      sync();
+      // A <- J^T A: rows p, q of every rotation of the round
+      {
+        int k = k0, i = i0;
+        for (int w = tid; w < work; w += nt) {
+          const double sk = rot_s[k];
+          if (sk != 0.0) {
+            const int pk = rot_p[k], qk = rot_q[k];
+            const double ck = rot_c[k];
             const double apk = A[pk + i * m], aqk = A[qk + i * m];
             A[pk + i * m] = ck * apk - sk * aqk;
             A[qk + i * m] = sk * apk + ck * aqk;
@@ -130,19 +152,11 @@ __device__ inline int jacobi_eigen_warp(double* A, double* E, int m,
             ++k;
           }
         }
-        __syncwarp();
-        // next round: slots >= 1 advance both players by one
-        const int slot = g * 32 + lane;
-        if (slot == 0) {
-          ++sb[g];
-        } else {
-          sa[g] = sa[g] + 1 == wrap ? 0 : sa[g] + 1;
-          sb[g] = sb[g] + 1 == wrap ? 0 : sb[g] + 1;
-        }
       }
+      sync();
     }
   }
-  __syncwarp();
+  __syncthreads();
   return sweep;
 }
 

@@ -196,7 +196,7 @@ __global__ void small_svd_from_gram(const double* __restrict__ G, int l, int k,
   int* order = reinterpret_cast<int*>(E + l * l);
   for (int idx = threadIdx.x; idx < l * l; idx += blockDim.x) A[idx] = G[idx];
   __syncthreads();
-  jacobi_eigen_warp<4>(A, E, l, 60);
+  jacobi_eigen(A, E, l, 60);
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int i = 0; i < l; ++i) order[i] = i;
@@ -373,7 +373,7 @@ class SvdOperator {
     gemm_f64(g, s_);
     if (smem > 48 * 1024)
       FPLS_CHECK(cudaFuncSetAttribute(small_svd_from_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    small_svd_from_gram<<<1, 64, smem, s_>>>(G.get(), l, r, t.d.get(), Ub.get(), Ud.get());
+    small_svd_from_gram<<<1, jacobi_threads(l), smem, s_>>>(G.get(), l, r, t.d.get(), Ub.get(), Ud.get());
     count_launch();
     FPLS_LAUNCH("small_svd_from_gram");
     // U = Q Ub (n x r); V = B^T Ub / d = Z Ud (p x r)
