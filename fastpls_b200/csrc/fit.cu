@@ -132,13 +132,12 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
   jacobi_eigen(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long taken = 0ull;  // m <= 64
     for (int j = 0; j < count; ++j) {
       int best = -1;
       for (int k = 0; k < m; ++k)
-        if (!((taken >> k) & 1ull) && (best < 0 || A[k + k * m] > A[best + best * m])) best = k;
-      taken |= 1ull << best;
+        if (best < 0 || A[k + k * m] > A[best + best * m]) best = k;
       const double lam = A[best + best * m];
+      A[best + best * m] = -INFINITY;  // taken (A is scratch after the solve)
       if (!(lam > 0.0) || !isfinite(lam)) flag_error(flag, 1);
       const double inv = (lam > 0.0 && isfinite(lam)) ? 1.0 / sqrt(lam) : 0.0;
       // deterministic sign: largest-magnitude entry of z positive
@@ -477,7 +476,7 @@ template <class T>
 void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
                 DeviceModel& model, Workspace& ws, cudaStream_t stream, int block) {
-  require(m >= 1 && m <= kMaxResponses, "SIMPLS supports 1..64 responses or classes");
+  require(m >= 1 && m <= kMaxResponses, "SIMPLS supports 1..112 responses or classes");
   const int a_max = components;
   ws.ensure(n, p, m, a_max, stream);
   model.method = kSimpls;

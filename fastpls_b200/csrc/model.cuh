@@ -8,7 +8,9 @@
 
 namespace fpls {
 
-constexpr int kMaxResponses = 64;  // m x m direction eigenproblem in one block
+// m x m direction eigenproblem in one block: 2 m^2 doubles of shared memory
+// (200 KB at 112) and m <= 128 for the block Jacobi
+constexpr int kMaxResponses = 112;
 
 enum Method { kPlssvd = 1, kSimpls = 3, kOpls = 4, kKernelPls = 5 };
 

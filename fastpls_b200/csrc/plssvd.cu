@@ -115,7 +115,7 @@ template <class T>
 void fit_plssvd(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
                 DeviceModel& model, Workspace& ws, cudaStream_t stream) {
-  require(m >= 1 && m <= kMaxResponses, "PLS-SVD supports 1..64 responses or classes");
+  require(m >= 1 && m <= kMaxResponses, "PLS-SVD supports 1..112 responses or classes");
   require(components <= 128, "PLS-SVD supports at most 128 components");
   const int k = components;
   require(k <= std::min(p, m), "fastPLS PLS-SVD component count exceeds cross-covariance rank");
