@@ -95,3 +95,17 @@ def test_fastsvd_small_matrix_is_exact():
     U, S, Vt = np.linalg.svd(x, full_matrices=False)
     assert np.allclose(d, S[:3], rtol=1e-12)
     assert O.rel_err(O.align_signs(u, U[:, :3]), U[:, :3]) < 1e-10
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-8), (32, 2e-3)])
+def test_fastsvd_known_answer(precision, tol):
+    # core/tests/test_core_operator_rsvd.cpp:140-178: a 10 x 8 matrix with
+    # diagonal 8, 7, ..., 1, rank 2, oversample 6, one power step, seed 27
+    x = np.zeros((10, 8))
+    for i in range(8):
+        x[i, i] = 8 - i
+    u, d, v = api.fastsvd(x, 2, oversample=6, power=1, seed=27, precision=precision)
+    assert u.shape == (10, 2) and v.shape == (8, 2)
+    assert abs(d[0] - 8) < tol and abs(d[1] - 7) < tol
+    for j in range(2):
+        assert np.linalg.norm(x @ v[:, j] - d[j] * u[:, j]) / d[j] < tol
