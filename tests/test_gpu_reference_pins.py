@@ -66,3 +66,20 @@ def test_cv_fp32_vs_fp64():
                               store_predictions=True)
     assert np.array_equal(c["predictions"], d["predictions"])
     assert np.allclose(c["metrics"], d["metrics"])
+
+
+def test_label_crossprod_known_answer_on_device():
+    # core/tests/test_core_classification.cpp:13-44 through a PLS-SVD fit: the
+    # autoscaled label cross-product is a = 0.7745967 times [-1, 1] in every
+    # row, so the weight is (1, 1, 1) / sqrt(3) up to sign
+    x = np.array([[1 + r + 10 * c for c in range(3)] for r in range(4)], dtype=np.float64)
+    lab = np.array([1, 2, 1, 2], dtype=np.int32)
+    model = api.fit_resident(x, labels=lab, classes=2, ncomp=1, method="plssvd",
+                             scaling="autoscaling")
+    assert np.allclose(model.export(3), [2.5, 12.5, 22.5], atol=1e-12)
+    assert np.allclose(model.export(4), 1.2909944, atol=1e-6)
+    assert np.allclose(model.export(5), [0.5, 0.5], atol=1e-12)
+    R = model.export(0)[:, 0]
+    assert np.allclose(np.abs(R), 1 / np.sqrt(3), atol=1e-12)
+    assert np.all(np.sign(R) == np.sign(R[0]))
+    model.close()

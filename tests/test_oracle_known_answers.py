@@ -70,3 +70,27 @@ def test_permutation_pvalue():
     assert O.permutation_pvalue([0.1, 0.5, np.nan, 0.9], 0.5) == (2 + 1) / (3 + 1)
     assert O.permutation_pvalue([0.1, 0.5, 0.9], 0.5, lower_tail=True) == 3 / 4
     assert np.isnan(O.permutation_pvalue([np.nan], 0.5))
+
+
+def label_fixture():
+    # core/tests/test_core_classification.cpp:13-19: x(row, col) = 1 + row + 10 col
+    # (4 x 3), classes 0, 1, 0, 1 (one-based here: 1, 2, 1, 2)
+    x = np.array([[1 + r + 10 * c for c in range(3)] for r in range(4)], dtype=np.float64)
+    return x, np.array([1, 2, 1, 2])
+
+
+def test_label_crossprod_known_answers():
+    x, lab = label_fixture()
+    # centred label cross-product without scaling (:20-31): class sums minus
+    # half the column total
+    _, s, _, _, _, _ = O._prepare(x, None, lab, 2, 3)
+    for c in range(3):
+        zero, one = x[0, c] + x[2, c], x[1, c] + x[3, c]
+        assert abs(s[c, 0] - (zero - 0.5 * (zero + one))) < 1e-12
+        assert abs(s[c, 1] - (one - 0.5 * (zero + one))) < 1e-12
+    # autoscaled (:33-44)
+    _, s, centre, scale, ymean, _ = O._prepare(x, None, lab, 2, 2)
+    assert abs(centre[0] - 2.5) < 1e-12
+    assert abs(scale[0] - 1.2909944) < 1e-6
+    assert abs(ymean[0] - 0.5) < 1e-12
+    assert abs(s[0, 0] + 0.7745967) < 1e-6 and abs(s[0, 1] - 0.7745967) < 1e-6
