@@ -1,6 +1,6 @@
 // FP64 FMA throughput probe: the roofline denominator for the FP64-bound
-// kernels of this library, measured on the running device (the driver's
-// peak file carries HBM copy and BF16 GEMM figures only).
+// kernels of this library, measured on the running device (the measured
+// peak file holds HBM copy and BF16 GEMM figures only).
 #include "common.cuh"
 #include "kernels.cuh"
 
