@@ -211,7 +211,7 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
     throw std::invalid_argument("invalid batched CUDA classification CV input");
   int folds_n = 0;
   for (int i = 0; i < n; ++i) {
-    if (labels[i] < 1 || labels[i] > classes || folds[i] < 0)
+    if (labels[i] < 1 || labels[i] > classes || folds[i] < 1)
       throw std::invalid_argument("invalid batched CUDA classification CV input");
     folds_n = std::max(folds_n, folds[i]);
   }
