@@ -477,10 +477,15 @@ void xr_launch(const T* X, int n, int p, long ld, const double* R, long ldr,
   chunks = (int)ceil_div(p, cc);
   scratch.reserve((size_t)chunks * n * nb, stream);
   const size_t smem = (size_t)cc * NB * sizeof(double);
-  if (vec)
-    xr_vec_kernel<T, NB><<<dim3(ceil_div(n, kThreads * Vec16<T>::V), chunks), kThreads, smem, stream>>>(
-        X, n, p, ld, R, ldr, nb, cc, scratch.get());
-  else
+  bool launched = false;
+  if constexpr (NB <= 2) {
+    if (vec) {
+      xr_vec_kernel<T, NB><<<dim3(ceil_div(n, kThreads * Vec16<T>::V), chunks), kThreads, smem,
+                             stream>>>(X, n, p, ld, R, ldr, nb, cc, scratch.get());
+      launched = true;
+    }
+  }
+  if (!launched)
     xr_kernel<T, NB><<<dim3(ceil_div(n, 2 * kThreads), chunks), kThreads, smem, stream>>>(
         X, n, p, ld, R, ldr, nb, cc, scratch.get());
   count_launch();
