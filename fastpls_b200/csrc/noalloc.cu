@@ -13,7 +13,11 @@
 // loads the library keeps it for the lifetime of the process. Its address is
 // looked up once per device (cudaGetSymbolAddress, on the first call made
 // while that device is current), so that first call should happen before any
-// stream capture starts. All calls share the array and every call overwrites
+// stream capture starts. The looked-up address is kept for the process: after
+// cudaDeviceReset the module is loaded again and the array may move, so a
+// process that resets a device must not call this entry point again. Each
+// call waits for its stream before returning. All calls share the array and
+// every call overwrites
 // the slots it uses before reading them (nothing has to start at zero), so
 // calls that overlap on the GPU -- on different streams, or from different
 // host threads -- race on it and must be serialised by the caller.
@@ -118,7 +122,8 @@ void crossprod_noalloc(const T* X, int n, int p, long ld, const double* V,
   double* scratch = scratch_address();
   const int rc = 1024;
   int chunks = (int)ceil_div(n, rc);
-  const long fit = kNoAllocScratchDoubles / per_chunk;
+  // chunks run along gridDim.y (at most 65535), and their partials must fit
+  const long fit = std::min(kNoAllocScratchDoubles / per_chunk, 65535L);
   int rows_per_chunk = rc;
   if (chunks > fit) {  // fewer, taller chunks so the partials fit
     rows_per_chunk = (int)ceil_div(n, fit);

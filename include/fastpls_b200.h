@@ -402,11 +402,13 @@ FASTPLS_B200_API int fastpls_b200_server_stats(void* server, size_t* bytes_in_us
  * reference ABI. Partial sums live in one file-scope device array of
  * 2097152 doubles (16 MiB) that every GPU loading the library keeps until
  * exit; requests with p * nb above that size, or nb above 32, are rejected
- * with an error. The array's address is looked up on the first call made on
- * each device, so make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU race and must be serialised
- * by the caller. Runs on `stream` (a cudaStream_t, NULL = default stream)
- * and returns after the work completes. */
+ * with an error; any row count is accepted (rows are grouped into at most
+ * 65535 chunks). The array's address is looked up on the first call made on
+ * each device, so make that first call before any stream capture; the address
+ * is kept for the process, so do not call again after cudaDeviceReset. All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. Runs on `stream` (a cudaStream_t, NULL = default
+ * stream) and waits for that stream before returning. */
 FASTPLS_B200_API int fastpls_b200_crossprod_noalloc(
     const void* x, int precision, int n, int p, long ldx, const double* v,
     long ldv, int nb, double* out, long ldo, void* stream, char* error,

@@ -23,8 +23,11 @@ _D = np.ctypeslib.ndpointer(dtype=np.float64, flags="F_CONTIGUOUS")
 _I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 
-def build(reference_root="/root/reference"):
-    """Compile the reference core harness (needs the reference tree)."""
+def build(reference_root=None):
+    """Compile the reference core harness (needs the reference tree, found at
+    ``reference_root`` or the FASTPLS_REFERENCE_ROOT environment variable)."""
+    if reference_root is None:
+        reference_root = os.environ.get("FASTPLS_REFERENCE_ROOT", "/root/reference")
     subprocess.run(["make", "-s", f"REF={reference_root}"], cwd=_HERE,
                    check=True)
 

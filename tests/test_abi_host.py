@@ -90,3 +90,35 @@ def test_error_buffer_truncates_safely(lib):
 
 def test_device_count_without_gpu_is_nonnegative(lib):
     assert lib.fastpls_b200_device_count() >= 0
+
+
+def _reference_header():
+    root = os.environ.get("FASTPLS_REFERENCE_ROOT", "/root/reference")
+    path = os.path.join(root, "src", "cuda_resident_api.h")
+    return path if os.path.exists(path) else None
+
+
+@pytest.mark.parametrize("lang,compiler", [("c++", "g++"), ("c", "gcc")])
+def test_header_compiles_together_with_reference_header(tmp_path, lang, compiler):
+    """One translation unit includes the reference's C ABI header
+    (src/cuda_resident_api.h) and this library's header: a function whose
+    name matches but whose signature differs is a conflicting extern "C"
+    redeclaration and fails the compile. Each reference entry point is also
+    bound to a pointer of the reference's type through this header's
+    declaration."""
+    import shutil
+    import subprocess
+
+    ref = _reference_header()
+    if ref is None:
+        pytest.skip("reference tree not present (set FASTPLS_REFERENCE_ROOT)")
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not found")
+    names = re.findall(r"\b(fastpls_\w+)\s*\(", open(ref).read())
+    assert len(names) == 18
+    body = "\n".join(f"__typeof__({n}) *p_{n} = &{n};" for n in names)
+    src = tmp_path / ("abi." + ("cpp" if lang == "c++" else "c"))
+    src.write_text(f'#include "{ref}"\n#include "{HEADER}"\n{body}\n')
+    proc = subprocess.run([compiler, "-x", lang, "-fsyntax-only", "-Wall", "-Werror", str(src)],
+                          capture_output=True, text=True)
+    assert proc.returncode == 0, proc.stderr

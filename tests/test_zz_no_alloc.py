@@ -6,7 +6,9 @@ must not stall on the allocator): they hand over device buffers and the
 library's partial sums live in a fixed file-scope device array. The test
 checks its output against the existing fastpls_cuda_gemm entry point on two
 consecutive calls (the second with new right-hand sides, so stale scratch
-contents would show), and that oversized requests are refused cleanly.
+contents would show), against a host FP64 product on a shape whose partial
+sums only fit as fewer, taller row chunks, and that oversized requests are
+refused cleanly.
 This file is collected last on purpose.
 """
 import ctypes as C
@@ -61,6 +63,32 @@ def test_noalloc_crossprod_matches_gemm_entry_point(precision):
         assert rc == 0, msg
         got = outd.cpu().numpy().T
         want = _reference(lib, x64, v)
+        rel = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert rel < 1e-12, (call, rel)
+
+
+def test_noalloc_tall_chunks_match_host_product():
+    """p * nb = 524288 doubles leaves room for 4 row chunks: 5000 rows run as
+    4 chunks of 1250 rows, each staged through shared memory 192 rows at a
+    time, so every slot is written once and then accumulated into."""
+    import torch
+
+    from fastpls_b200 import _lib
+    lib = _lib.load()
+    n, p, nb = 5000, 16384, 32
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((n, p), dtype=np.float32)
+    dev = torch.device("cuda", 0)
+    xd = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)
+    outd = torch.zeros((nb, p), dtype=torch.float64, device=dev)
+    x64 = x.astype(np.float64)
+    for call in range(2):
+        v = rng.standard_normal((n, nb))
+        vd = torch.from_numpy(np.ascontiguousarray(v.T)).to(dev)
+        rc, msg = _noalloc(lib, xd, 32, n, p, vd, nb, outd)
+        assert rc == 0, msg
+        got = outd.cpu().numpy().T
+        want = x64.T @ v
         rel = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert rel < 1e-12, (call, rel)
 
