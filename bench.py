@@ -62,6 +62,11 @@ def args_parse():
                     help="stream lanes of the batched engine (1..4)")
     ap.add_argument("--fp64-steps", type=int, default=2,
                     help="timed steps with FP64 DMMA products, for comparison")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the single-fit configuration legs (plain FP64 "
+                         "SIMPLS, full-size PLS-SVD + LDA, full-size BF16 SIMPLS)")
+    ap.add_argument("--latency-steps", type=int, default=60,
+                    help="untimed extra steps for the step-latency distribution")
     return ap.parse_args()
 
 
@@ -329,6 +334,201 @@ def int8_peak_tops(torch, dev):
         return 4500.0, f"nominal B200 dense int8 (library GEMM unavailable: {exc})"
 
 
+def measured_peaks():
+    """Roofline denominators: MEASURED_PEAKS.json (written per pod by the
+    driver) when present, else the stated fallback of this GPU pool."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        hbm = float(d.get("hbm_gbs") or d.get("hbm_GBps") or 0) or None
+        bf16 = float(d.get("bf16_tflops") or 0) or None
+        if hbm:
+            return {"hbm_gbs": hbm, "bf16_tflops": bf16, "source": "measured (MEASURED_PEAKS.json)"}
+    except Exception:
+        pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0,
+            "source": "fallback (6.65 TB/s copy, 1.59 PFLOP/s bf16: earlier measurement on this pool)"}
+
+
+def _errors_simpls(R, Q, T, ref, prefixes, pred=None, want_pred=None):
+    from oracle import pls_oracle as O
+    sg = np.where(np.einsum("ij,ij->j", R, ref["R"]) < 0.0, -1.0, 1.0)
+    out = {"R": O.rel_err(R * sg, ref["R"]), "Q": O.rel_err(Q * sg, ref["Q"])}
+    if T is not None:
+        out["T"] = O.rel_err(T * sg, ref["T"])
+    out["B"] = max(O.rel_err(R[:, :k] @ Q[:, :k].T, ref["R"][:, :k] @ ref["Q"][:, :k].T)
+                   for k in prefixes)
+    if pred is not None:
+        out["Yhat"] = max(O.rel_err(pred[j], want_pred[j]) for j in range(len(prefixes)))
+    return {k: float(v) for k, v in out.items()}
+
+
+def _ref_predictions(ref, xp, prefixes):
+    t = (xp - ref["centre"]) / ref["scale"] @ ref["R"]
+    return [ref["ymean"] + t[:, :k] @ ref["Q"][:, :k].T for k in prefixes]
+
+
+def leg_small_fits(fapi, with_ref, fits=100):
+    """The plain FP64 SIMPLS configuration: n 500, p 2000, 3 responses, 10
+    components (latent T 500 x 5, noise 0.5, seed 1): fits/s one fit at a
+    time through fastpls_resident_simpls_create (host buffers), the device
+    time of each fit, and errors against the reference FP64 core."""
+    from fastpls_b200 import workloads as W
+    n, p, m, a = 500, 2000, 3, 10
+    x, y = W.latent_regression(n, p, m, 5, 0.5, 1, dtype=np.float64)
+    pre = [1, 5, 10]
+    for _ in range(5):
+        fapi.fit_resident(x, y, ncomp=a, precision=64).close()
+    dev_ms, lat = [], []
+    t0 = time.perf_counter()
+    for _ in range(fits):
+        s = time.perf_counter()
+        mdl = fapi.fit_resident(x, y, ncomp=a, precision=64)
+        dev_ms.append(fapi.last_fit_times()["fit_ms"])
+        mdl.close()
+        lat.append(1000 * (time.perf_counter() - s))
+    wall = time.perf_counter() - t0
+    mdl = fapi.fit_resident(x, y, ncomp=a, precision=64)
+    R, Q, T = (mdl.export(f).astype(np.float64) for f in (0, 1, 2))
+    pred = mdl.predict_path(x, pre).astype(np.float64)
+    mdl.close()
+    out = {"workload": f"simpls_{n}x{p}_m{m}_ncomp{a}_f64", "fits": fits,
+           "value": 1000.0 / float(np.mean(dev_ms)), "unit": "fits/s",
+           "value_is": "inputs on the device (device time of the fit proper)",
+           "e2e": {"value": fits / wall, "unit": "fits/s",
+                   "p50_ms": float(np.percentile(lat, 50)),
+                   "p99_ms": float(np.percentile(lat, 99)),
+                   "h2d_bytes_per_fit": int(x.nbytes + y.nbytes)}}
+    if with_ref:
+        from oracle import ref
+        cores = os.cpu_count() or 1
+        ref.set_threads(cores)
+        rr = ref.simpls_fit(x, y, ncomp=a)
+        t0 = time.perf_counter()
+        reps = 20
+        for _ in range(reps):
+            ref.simpls_fit(x, y, ncomp=a)
+        dt = time.perf_counter() - t0
+        out["errors_vs_fp64_reference"] = _errors_simpls(
+            R, Q, T, rr, pre, pred, _ref_predictions(rr, x, pre))
+        out["cpu_baseline"] = {"value": reps / dt, "unit": "fits/s", "cores": cores,
+                               "kind": "reference", "sample": f"{reps} reference fits"}
+    return out
+
+
+def leg_plssvd_lda(fapi, peaks, with_ref):
+    """The PLS-SVD + LDA configuration at full size: X 20000 x 50000 FP32
+    (latent k = 20, scales 100 * 0.8^i, noise 0.1), 10 classes, ncomp capped
+    at 9, oversample 10, power 2; LDA on the scores of 2000 rows. Device time
+    of the fit against HBM (algorithmic bytes: the label cross-product pass
+    and the score pass over X, 2 n p 4 bytes); labels against the reference's
+    PLS-SVD + LDA (bit-exact)."""
+    from fastpls_b200 import workloads as W
+    n, p, classes, a = 20_000, 50_000, 10, 9
+    x, lab = W.plssvd_lda_config(seed=2, n=n, p=p, k=20, classes=classes)
+    pre = [1, 3, 5, 9]
+    probe = np.arange(0, n, 10)
+    xp = np.asfortranarray(x[probe])
+    kw = dict(labels=lab, classes=classes, ncomp=a, method="plssvd", precision=32,
+              oversample=10, power=2)
+    fapi.fit_resident(x, **kw).close()
+    fit_ms, copy_ms, walls = [], [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        mdl = fapi.fit_resident(x, **kw)
+        t = fapi.last_fit_times()
+        got = mdl.classify_path(xp, pre, lda=True)
+        walls.append(time.perf_counter() - t0)
+        fit_ms.append(t["fit_ms"])
+        copy_ms.append(t["copy_ms"])
+        mdl.close()
+    fms = float(np.median(fit_ms))
+    alg = 2.0 * n * p * 4
+    achieved = alg / (fms * 1e-3) / 1e9
+    out = {"workload": f"plssvd_lda_{n}x{p}_c{classes}_ncomp{a}_f32",
+           "fit_ms": fms, "copy_ms": float(np.median(copy_ms)),
+           "e2e_ms": 1000 * float(np.median(walls)),
+           "e2e_is": "host buffers: H2D of X (4 GB) and labels, fit, LDA labels of 2000 rows",
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                        "algorithmic_bytes": alg, "peak_source": peaks["source"]}}
+    if with_ref:
+        from oracle import ref
+        cores = os.cpu_count() or 1
+        ref.set_threads(cores)
+        x64 = np.asfortranarray(x, dtype=np.float64)
+        del x
+        t0 = time.perf_counter()
+        rr = ref.plssvd_fit(x64, labels=lab, classes=classes, prefixes=pre, scaling=1,
+                            oversample=10, power=2)
+        tp = (x64[probe] - rr["centre"]) @ rr["R"]
+        _, want = ref.lda(rr["T"], lab, classes, pre, tp)
+        dt = time.perf_counter() - t0
+        del x64
+        out["labels_equal_reference"] = bool(all(
+            np.array_equal(got[j][:, 0], want[:, j]) for j in range(len(pre))))
+        out["label_differences"] = [int(np.sum(got[j][:, 0] != want[:, j]))
+                                    for j in range(len(pre))]
+        out["cpu_baseline"] = {"value": dt, "unit": "s per fit", "cores": cores,
+                               "kind": "reference",
+                               "sample": "one FP64 PLS-SVD fit + LDA labels of 2000 rows"}
+    return out
+
+
+def leg_mixed_precision(fapi, peaks, with_ref):
+    """The mixed-precision configuration at full size: X 100000 x 20000 in
+    BF16 (latent k = 50, column scales logN(0, 1)), 10 responses, 50
+    components. Device time of the fit against HBM (algorithmic bytes:
+    (1 + 2 a) n p 2, the cross-product pass and two passes per component),
+    and the error of R, Q, T, B and predictions against the reference FP64
+    core on the same BF16-rounded values."""
+    from fastpls_b200 import workloads as W
+    n, p, m, a = 100_000, 20_000, 10, 50
+    bits, y = W.mixed_precision_config(seed=4, n=n, p=p, m=m, k=50)
+    pre = [1, 10, 25, 50]
+    rows = np.arange(0, n, 25)[:4000]
+    fapi.fit_resident(bits, y, ncomp=a, precision=16).close()
+    fit_ms, copy_ms, walls = [], [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        mdl = fapi.fit_resident(bits, y, ncomp=a, precision=16)
+        walls.append(time.perf_counter() - t0)
+        t = fapi.last_fit_times()
+        fit_ms.append(t["fit_ms"])
+        copy_ms.append(t["copy_ms"])
+        if len(walls) < 2:
+            mdl.close()
+    pred = mdl.predict_path(bits[rows], pre).astype(np.float64)
+    R, Q, T = (mdl.export(f).astype(np.float64) for f in (0, 1, 2))
+    mdl.close()
+    fms = float(np.median(fit_ms))
+    alg = (1.0 + 2.0 * a) * n * p * 2
+    achieved = alg / (fms * 1e-3) / 1e9
+    out = {"workload": f"simpls_{n}x{p}_m{m}_ncomp{a}_bf16",
+           "fit_ms": fms, "copy_ms": float(np.median(copy_ms)),
+           "e2e_ms": 1000 * float(np.median(walls)),
+           "e2e_is": "host buffers: H2D of X (4 GB BF16) and Y, the fit",
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                        "algorithmic_bytes": alg, "peak_source": peaks["source"]}}
+    if with_ref:
+        from oracle import ref
+        cores = os.cpu_count() or 1
+        ref.set_threads(cores)
+        x64 = W.bf16_to_f64(bits)
+        del bits
+        t0 = time.perf_counter()
+        rr = ref.simpls_fit(x64, y.astype(np.float64), ncomp=a, scaling=1)
+        dt = time.perf_counter() - t0
+        want = _ref_predictions(rr, x64[rows], pre)
+        del x64
+        out["errors_vs_fp64_reference"] = _errors_simpls(R, Q, T, rr, pre, pred, want)
+        out["cpu_baseline"] = {"value": dt, "unit": "s per fit", "cores": cores,
+                               "kind": "reference",
+                               "sample": "one FP64 fit of the same BF16-rounded values"}
+    return out
+
+
 def workload_config(perms, digits=6, lanes=3):
     return {"workload": f"cv{FOLDS}_perm{perms}_ncomp{NCOMP}_{N}x{P}_f32",
             "n": N, "p": P, "q": Q, "folds": FOLDS, "fold_sizes": "480-520",
@@ -442,6 +642,23 @@ def main():
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
     all_q2 = outs[1].reshape(Pn + 1, k).copy()
+    # step-latency distribution over more steps than the timed region (the
+    # same step, device-timed one by one with CUDA events)
+    lat_ms = list(step_ms)
+    if a.latency_steps > 0:
+        lev = [torch.cuda.Event(enable_timing=True) for _ in range(a.latency_steps + 1)]
+        lev[0].record(stream)
+        for s_ in range(a.latency_steps):
+            step_device()
+            lev[s_ + 1].record(stream)
+        barrier()
+        lat_ms += [lev[s_].elapsed_time(lev[s_ + 1]) for s_ in range(a.latency_steps)]
+    sched = {}
+    try:
+        from fastpls_b200 import api as _fapi
+        sched = _fapi.batched_stats()
+    except Exception:
+        pass
 
     # roofline of the dominant kernel: one more step with a single lane (the
     # products run alone, not overlapped with the other lane's kernels), each
@@ -553,9 +770,12 @@ def main():
         "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(Pn, digits, lanes),
-        "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
-                       "p99": float(np.percentile(step_ms, 99)),
-                       "steps": [round(v, 3) for v in step_ms]},
+        "latency_ms": {"p50": float(np.percentile(lat_ms, 50)),
+                       "p99": float(np.percentile(lat_ms, 99)),
+                       "p99_over_p50": float(np.percentile(lat_ms, 99) / np.percentile(lat_ms, 50)),
+                       "steps_measured": len(lat_ms),
+                       "timed_steps": [round(v, 3) for v in step_ms]},
+        "schedule": sched,
         "e2e": {"value": world * fits_per_step / (e2e_ms / 1000.0), "unit": "fits/s",
                 "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -600,6 +820,16 @@ def main():
                                 "queue behind their model's fit in the server",
             sweep=sweep, **plain,
             saturated_served_over_plain=sweep[-1]["fits_per_s"] / plain["plain_fits_per_s"])
+    if rank == 0 and world == 1 and not a.no_configs:
+        from fastpls_b200 import api as fapi
+        from oracle import ref as _ref
+        with_ref = _ref.available() and not a.no_cpu_baseline
+        peaks = measured_peaks()
+        line["configs"] = {
+            "plain_fp64_simpls": leg_small_fits(fapi, with_ref),
+            "plssvd_lda_full": leg_plssvd_lda(fapi, peaks, with_ref),
+            "mixed_precision_bf16_full": leg_mixed_precision(fapi, peaks, with_ref),
+        }
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu, ref_out = cpu_reference_sample(x, y, folds, prefixes)
         line["cpu_baseline"] = cpu

@@ -84,6 +84,16 @@ SIGNATURES = {
     "fastpls_b200_product_digits": (_i, []),
     "fastpls_b200_set_batch_lanes": (None, [_i]),
     "fastpls_b200_batch_lanes": (_i, []),
+    "fastpls_b200_set_argmax_guard": (None, [_d]),
+    "fastpls_b200_argmax_guard": (_d, []),
+    "fastpls_b200_guard_refits": (_i, []),
+    "fastpls_b200_last_fit_times": (None, [_dp, _dp]),
+    "fastpls_b200_set_persistent": (None, [_i]),
+    "fastpls_b200_persistent": (_i, []),
+    "fastpls_b200_set_autotune": (None, [_i]),
+    "fastpls_b200_autotune": (_i, []),
+    "fastpls_b200_batched_stats": (None, [C.POINTER(C.c_int)] * 6),
+    "fastpls_b200_release_workspace": (None, []),
     "fastpls_b200_profile_int8": (None, [_i]),
     "fastpls_b200_profile_int8_read": (None, [_dp, _dp, C.POINTER(C.c_ulonglong)]),
     "fastpls_b200_int8_crossprod": (

@@ -422,6 +422,63 @@ def batch_lanes() -> int:
     return int(_lib.load().fastpls_b200_batch_lanes())
 
 
+def set_argmax_guard(margin: float) -> None:
+    """Relative top-two score margin under which the batched classification
+    engine refits an instance with FP64 products (0 disables); process-wide."""
+    _lib.load().fastpls_b200_set_argmax_guard(float(margin))
+
+
+def argmax_guard() -> float:
+    return float(_lib.load().fastpls_b200_argmax_guard())
+
+
+def set_persistent(enable: bool) -> None:
+    """Single-fit SIMPLS component loop as one persistent launch (default)
+    or as the per-kernel loop; process-wide."""
+    _lib.load().fastpls_b200_set_persistent(1 if enable else 0)
+
+
+def persistent() -> bool:
+    return bool(_lib.load().fastpls_b200_persistent())
+
+
+def set_autotune(enable: bool) -> None:
+    """Autotuning of the batched engine's group schedule (lanes x tile
+    width); process-wide, on by default."""
+    _lib.load().fastpls_b200_set_autotune(1 if enable else 0)
+
+
+def autotune() -> bool:
+    return bool(_lib.load().fastpls_b200_autotune())
+
+
+def batched_stats() -> dict:
+    """Schedule statistics of the last batched call."""
+    vals = [C.c_int(0) for _ in range(6)]
+    _lib.load().fastpls_b200_batched_stats(*[C.byref(v) for v in vals])
+    keys = ("groups", "graph_replays", "graph_captures", "tuned", "lanes", "tile_n")
+    return {k: v.value for k, v in zip(keys, vals)}
+
+
+def last_fit_times() -> dict:
+    """Device milliseconds of this thread's last resident fit: the input
+    copies and the fit proper."""
+    a, b = C.c_double(0), C.c_double(0)
+    _lib.load().fastpls_b200_last_fit_times(C.byref(a), C.byref(b))
+    return {"copy_ms": a.value, "fit_ms": b.value}
+
+
+def release_workspace() -> None:
+    """Free the batched engine's persistent device workspace."""
+    _lib.load().fastpls_b200_release_workspace()
+
+
+def guard_refits() -> int:
+    """Instances refitted with FP64 products by the last batched
+    classification call."""
+    return int(_lib.load().fastpls_b200_guard_refits())
+
+
 def int8_crossprod(a, b=None, digits=6, tile_n=0, pair=-1):
     """a^T b (b = None: a^T a, symmetric) by the int8 split product on the
     tensor cores; a is k x m, b is k x n (FP64). tile_n: 128, 192, 256 or 0

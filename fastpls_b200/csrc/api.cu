@@ -11,6 +11,7 @@
 #include "ozaki.cuh"
 #include "cv.cuh"
 #include "handle.cuh"
+#include "persistent.cuh"
 
 #include <atomic>
 #include <cstdio>
@@ -20,6 +21,7 @@ namespace fpls {
 
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launch(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 void keep_pool_memory() {
   static thread_local int configured_device = -1;
@@ -622,6 +624,39 @@ int fastpls_b200_product_digits(void) { return ozaki_slices(); }
 void fastpls_b200_set_batch_lanes(int lanes) { batch_lanes() = std::max(1, std::min(lanes, 4)); }
 
 int fastpls_b200_batch_lanes(void) { return batch_lanes(); }
+
+void fastpls_b200_set_argmax_guard(double margin) {
+  argmax_guard() = (margin > 0.0 && std::isfinite(margin)) ? margin : 0.0;
+}
+
+double fastpls_b200_argmax_guard(void) { return argmax_guard(); }
+
+int fastpls_b200_guard_refits(void) { return last_guard_refits(); }
+
+void fastpls_b200_last_fit_times(double* copy_ms, double* fit_ms) {
+  read_last_fit_times(copy_ms, fit_ms);
+}
+
+void fastpls_b200_set_persistent(int enable) { persistent_enabled() = enable ? 1 : 0; }
+
+int fastpls_b200_persistent(void) { return persistent_enabled(); }
+
+void fastpls_b200_set_autotune(int enable) { batch_autotune() = enable ? 1 : 0; }
+
+int fastpls_b200_autotune(void) { return batch_autotune(); }
+
+void fastpls_b200_batched_stats(int* groups, int* graph_replays, int* graph_captures, int* tuned,
+                                int* lanes, int* tile_n) {
+  const BatchedStats& s = last_batched_stats();
+  if (groups) *groups = s.groups;
+  if (graph_replays) *graph_replays = s.graph_replays;
+  if (graph_captures) *graph_captures = s.graph_captures;
+  if (tuned) *tuned = s.tuned;
+  if (lanes) *lanes = s.lanes;
+  if (tile_n) *tile_n = s.tile_n;
+}
+
+void fastpls_b200_release_workspace(void) { release_batched_workspace(); }
 
 void fastpls_b200_profile_int8(int enable) { ozaki_profile_enable(enable != 0); }
 

@@ -31,7 +31,13 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
 #include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 namespace fpls {
@@ -56,6 +62,10 @@ struct InstanceView {
   const double* Y;          // n x q base responses (FP64)
   const int* labels;        // n zero-based classes of the base rows, or null
                             // (regression); classification counts hits
+  int* amb;                 // per instance: set to 1 when a held-out argmax
+                            // decision fell inside the int8-product margin
+                            // (null: FP64 products, no margin)
+  double guard;             // relative argmax margin (argmax_guard())
 };
 
 __device__ __forceinline__ int src_row(const InstanceView& v, int perm, int r) {
@@ -72,17 +82,27 @@ __device__ __forceinline__ double heldout_term(const InstanceView& v, int i, int
   const int q = v.q;
   if (v.labels) {
     int best = -1;
-    double bv = 0.0;
+    double bv = 0.0, sv = 0.0;
+    bool second = false;
     for (int c = 0; c < q; ++c) {
       const double ym = ymean[(long)i * q + c];
       if (ym > 0.0) {
         const double score = ym + yh[(long)c * ld];
         if (best < 0 || score > bv) {
+          if (best >= 0) {
+            sv = bv;
+            second = true;
+          }
           best = c;
           bv = score;
+        } else if (!second || score > sv) {
+          sv = score;
+          second = true;
         }
       }
     }
+    if (v.amb && second && !(bv - sv > v.guard * fmax(fabs(bv), fabs(sv))))
+      v.amb[i] = 1;
     return best == v.labels[src_row(v, b, r)] ? 1.0 : 0.0;
   }
   double err = 0.0;
@@ -584,6 +604,32 @@ int& batch_lanes() {
   return lanes;
 }
 
+// Relative margin of the argmax guard. The int8 digit products (6 digits)
+// move held-out scores by well under 1e-6 of their magnitude (worst case seen
+// in the kernel-form simulation at the benchmark size: 3.9e-7 on
+// predictions); a decision whose top-two gap is within this fraction of the
+// score magnitude is not trusted, and its instance is refitted with FP64
+// products, so the labels equal those of the FP64 path.
+double& argmax_guard() {
+  static double margin = 1e-5;
+  return margin;
+}
+
+int& last_guard_refits() {
+  static int count = 0;
+  return count;
+}
+
+int& batch_autotune() {
+  static int on = 1;
+  return on;
+}
+
+BatchedStats& last_batched_stats() {
+  static BatchedStats stats;
+  return stats;
+}
+
 namespace {
 
 // Rows per thread of the register-resident score kernel for n rows (0: too
@@ -598,36 +644,213 @@ int rows_per_thread(int n) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Persistent per-device workspace. Every buffer a group's component sequence
+// touches lives here, with a stable address across calls (buffers only
+// grow), so the sequence can be captured once as a CUDA graph and replayed
+// by later calls of the same shape. The engine runs on the workspace's own
+// streams: `main` (joined to the caller's stream by events) and one stream
+// per lane.
+struct LaneState {
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  int off = 0, cnt = 0;
+  InstanceView v{};
+  OzakiOperand rhs;  // int8 digits of this lane's right-hand sides
+};
+
+struct GroupGraph {
+  std::vector<long long> key;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long launches = 0;
+};
+
+struct TuneDecision {
+  int lanes = 1, tile_n = 0;
+  double ms = 0.0;
+};
+
+struct BatchedWorkspace {
+  int device = -1;
+  cudaStream_t main = nullptr;
+  cudaEvent_t fork = nullptr, joined = nullptr, t0 = nullptr, t1 = nullptr;
+  LaneState lanes[kMaxLanes];
+  // group-wide instance arrays; lane l works on instances [off, off + cnt)
+  DeviceArray<int> d_if, d_ip, amb;
+  DeviceArray<double> C0, C, G, ym, sst, sse, yhat, Wb, KWb, Ws, U, Y1, KC0;
+  // per-call inputs and the shared Gram
+  OzakiOperand gram_split, x_split;
+  DeviceArray<double> gram, Y64, x64;
+  DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag, perms, labels;
+  std::vector<GroupGraph> graphs;
+
+  BatchedWorkspace() {
+    FPLS_CHECK(cudaGetDevice(&device));
+    FPLS_CHECK(cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking));
+    FPLS_CHECK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    FPLS_CHECK(cudaEventCreateWithFlags(&joined, cudaEventDisableTiming));
+    FPLS_CHECK(cudaEventCreate(&t0));
+    FPLS_CHECK(cudaEventCreate(&t1));
+    for (LaneState& L : lanes) {
+      FPLS_CHECK(cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking));
+      FPLS_CHECK(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+    }
+  }
+  BatchedWorkspace(const BatchedWorkspace&) = delete;
+  BatchedWorkspace& operator=(const BatchedWorkspace&) = delete;
+  ~BatchedWorkspace() {
+    cudaStreamSynchronize(main);
+    for (LaneState& L : lanes) cudaStreamSynchronize(L.st);
+    drop_graphs();
+    // free every buffer while the streams it was allocated on still exist
+    for (LaneState& L : lanes) {
+      L.rhs.digits.release();
+      L.rhs.scale.release();
+    }
+    for (auto* a : {&d_if, &d_ip, &amb, &d_fold, &d_ntrain, &d_test_rows, &d_test_off, &d_slot,
+                    &flag, &perms, &labels})
+      a->release();
+    for (auto* a : {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram,
+                    &Y64, &x64})
+      a->release();
+    for (OzakiOperand* o : {&gram_split, &x_split}) {
+      o->digits.release();
+      o->scale.release();
+    }
+    cudaStreamSynchronize(main);
+    for (LaneState& L : lanes) {
+      cudaStreamSynchronize(L.st);
+      cudaEventDestroy(L.done);
+      cudaStreamDestroy(L.st);
+    }
+    for (cudaEvent_t e : {fork, joined, t0, t1}) cudaEventDestroy(e);
+    cudaStreamDestroy(main);
+  }
+  void drop_graphs() {
+    for (GroupGraph& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
+  // Device bytes held by the instance arrays and the Gram (reused by the
+  // next call, so they count as available when a group is sized).
+  size_t held_bytes() const {
+    size_t b = (d_if.size() + d_ip.size() + amb.size()) * sizeof(int);
+    for (const auto* a :
+         {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram})
+      b += a->size() * sizeof(double);
+    return b + gram_split.digits.size();
+  }
+};
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr size_t kMaxGraphs = 16;
+
+std::mutex& workspace_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+
+BatchedWorkspace*& workspace_slot(int device) {
+  static BatchedWorkspace* slots[kMaxDevices] = {};
+  return slots[device];
+}
+
+// Grow-only buffer sizing (the address is kept while it is large enough).
+template <class U>
+void grow(DeviceArray<U>& a, size_t count, cudaStream_t s) {
+  if (count == 0) count = 1;
+  if (count > a.size() || !a) a.allocate(count, s);
+}
+
+// Schedule decisions of the autotuner, keyed on the group shape; optionally
+// persisted in the file named by FASTPLS_B200_TUNE_FILE (one decision per
+// line: n p q instances components digits classification lanes tile ms).
+struct Tuner {
+  std::mutex mu;
+  std::map<std::vector<long long>, TuneDecision> decisions;
+  bool loaded = false;
+
+  const char* path() const { return std::getenv("FASTPLS_B200_TUNE_FILE"); }
+  void load() {
+    if (loaded) return;
+    loaded = true;
+    const char* f = path();
+    if (!f) return;
+    std::ifstream in(f);
+    std::vector<long long> k(7);
+    TuneDecision d;
+    while (in >> k[0] >> k[1] >> k[2] >> k[3] >> k[4] >> k[5] >> k[6] >> d.lanes >> d.tile_n >> d.ms)
+      if (d.lanes >= 1 && d.lanes <= kMaxLanes && (d.tile_n == 192 || d.tile_n == 256))
+        decisions[k] = d;
+  }
+  bool find(const std::vector<long long>& key, TuneDecision* out) {
+    std::lock_guard<std::mutex> lock(mu);
+    load();
+    auto it = decisions.find(key);
+    if (it == decisions.end()) return false;
+    *out = it->second;
+    return true;
+  }
+  void store(const std::vector<long long>& key, const TuneDecision& d) {
+    std::lock_guard<std::mutex> lock(mu);
+    load();
+    decisions[key] = d;
+    if (const char* f = path()) {
+      std::ofstream out(f, std::ios::app);
+      for (long long v : key) out << v << ' ';
+      out << d.lanes << ' ' << d.tile_n << ' ' << d.ms << '\n';
+    }
+  }
+};
+
+Tuner& tuner() {
+  static Tuner t;
+  return t;
+}
+
+}  // namespace
+
+void release_batched_workspace() {
+  std::lock_guard<std::mutex> lock(workspace_mutex());
+  for (int d = 0; d < kMaxDevices; ++d) {
+    delete workspace_slot(d);
+    workspace_slot(d) = nullptr;
+  }
+}
+
+// ---------------------------------------------------------------------------
 template <class T>
 void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
-  gram.reserve((size_t)n * n, s);
+  grow(ws->gram, (size_t)n * n, s);
   if (digits > 0) {
     // int8 digits of the rows of X D^1/2, the symmetric product on the int8
     // tensor cores (lower tiles + mirror), then the digits of K's rows for
-    // every later product with K
-    ozaki_split_colmajor<T>(X, n, p, n, kscale, digits, x_split, flag.get(), s);
-    ozaki_gemm(x_split, x_split, gram.get(), n, true, flag.get(), s);
-    ozaki_split_rows(gram.get(), n, n, n, digits, gram_split, flag.get(), s);
+    // every later product with K; X's digits are freed once K is formed
+    ozaki_split_colmajor<T>(X, n, p, n, kscale, digits, ws->x_split, ws->flag.get(), s);
+    ozaki_gemm(ws->x_split, ws->x_split, ws->gram.get(), n, true, ws->flag.get(), s);
+    ozaki_split_rows(ws->gram.get(), n, n, n, digits, ws->gram_split, ws->flag.get(), s);
+    ws->x_split.digits.release();
+    ws->x_split.scale.release();
     return;
   }
   // FP64 copy of X with the scaling folded in (X D^1/2), then the symmetric
   // product on the FP64 tensor-core path (lower tiles + mirror).
-  x64.reserve((size_t)n * p, s);
+  grow(ws->x64, (size_t)n * p, s);
   const long total = (long)n * p;
   scale_columns_f64<T><<<(unsigned)std::min<long>((total + 255) / 256, 16L * num_sms()), 256, 0, s>>>(
-      X, n, p, kscale, x64.get());
+      X, n, p, kscale, ws->x64.get());
   count_launch();
   FPLS_LAUNCH("scale_columns_f64");
   GemmArgs g;
   g.M = n;
   g.N = n;
   g.K = p;
-  g.A = x64.get();
+  g.A = ws->x64.get();
   g.lda = n;
-  g.B = x64.get();
+  g.B = ws->x64.get();
   g.ldb = n;
   g.trans_b = true;
-  g.C = gram.get();
+  g.C = ws->gram.get();
   g.ldc = n;
   g.lower = gemm_mma_supported(g);
   gemm_f64(g, s);
@@ -635,18 +858,18 @@ void BatchedCv<T>::form_gram(const double* kscale, cudaStream_t s) {
 
 template <class T>
 void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out,
-                                OzakiOperand& rhs_split, cudaStream_t s) {
+                                OzakiOperand& rhs_split, int tile_n, cudaStream_t s) {
   if (digits > 0) {
     // K is symmetric: its rows are its columns (contiguous, ld n)
-    ozaki_split_rows(rhs, n, cols, n, digits, rhs_split, flag.get(), s);
-    ozaki_gemm(gram_split, rhs_split, out, n, false, flag.get(), s);
+    ozaki_split_rows(rhs, n, cols, n, digits, rhs_split, ws->flag.get(), s);
+    ozaki_gemm(ws->gram_split, rhs_split, out, n, false, ws->flag.get(), s, tile_n);
     return;
   }
   GemmArgs g;
   g.M = n;
   g.N = cols;
   g.K = n;
-  g.A = gram.get();
+  g.A = ws->gram.get();
   g.lda = n;
   g.B = rhs;
   g.ldb = n;
@@ -655,124 +878,66 @@ void BatchedCv<T>::gram_product(const double* rhs, int cols, double* out,
   gemm_f64(g, s);
 }
 
-// The instances of a group run in lanes of their own CUDA stream, enqueued
-// component by component in turn, so that the memory-bound score and
-// deflation kernels of one lane overlap the tensor-core products of the
-// other. Lanes share the Gram and its digits (read only).
+// The whole component sequence of one group. The instances run in lanes of
+// their own CUDA stream, enqueued component by component in turn, so that
+// the memory-bound score and deflation kernels of one lane overlap the
+// tensor-core products of another. Lanes share the Gram and its digits
+// (read only). Fork from s at the start, join into s at the end; nothing in
+// here allocates, synchronises or reads back, so it can be captured.
 template <class T>
-void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
-                             const std::vector<int>& inst_perm,
-                             cudaStream_t s) {
-  const int I = (int)inst_fold.size();
-  if (I == 0) return;
-  const int q = this->q, kmax = this->kmax;
-  const size_t nq = (size_t)n * q;
-  const int nlanes = std::max(1, std::min(batch_lanes(), I / kLaneMinInstances));
-  struct OwnStream {
-    cudaStream_t st = nullptr;
-    bool own = false;
-    ~OwnStream() {
-      if (own) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-      }
-    }
-  };
-  struct Lane {
-    OwnStream hold;  // destroyed last: every array below is freed on it first
-    int off = 0, cnt = 0;
-    InstanceView v;
-    DeviceArray<int> d_if, d_ip;
-    DeviceArray<double> C0, C, G, ym, sst, sse, yhat, Wb, KWb, Ws, U, Y1, KC0;
-    OzakiOperand rhs;
-  };
-  std::vector<Lane> lanes(nlanes);
-  cudaEvent_t ready = nullptr;
-  FPLS_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-  struct EventGuard {
-    cudaEvent_t e;
-    ~EventGuard() { cudaEventDestroy(e); }
-  } ready_guard{ready};
-  FPLS_CHECK(cudaEventRecord(ready, s));
-
+void BatchedCv<T>::enqueue_group(int I, int nlanes, int tile_n, cudaStream_t s) {
   const size_t smem_dir = 2 * (size_t)q * q * sizeof(double);
+  const size_t smem_defl = (2 * (size_t)q * q + 2 * (size_t)kmax + q) * sizeof(double);
+  const size_t nq = (size_t)n * q;
   const int rpt = rows_per_thread(n);
+  FPLS_CHECK(cudaEventRecord(ws->fork, s));
   for (int l = 0; l < nlanes; ++l) {
-    Lane& L = lanes[l];
-    L.off = l * (I / nlanes);
-    L.cnt = l + 1 == nlanes ? I - L.off : I / nlanes;
-    if (nlanes == 1) {
-      L.hold.st = s;
-    } else {
-      FPLS_CHECK(cudaStreamCreateWithFlags(&L.hold.st, cudaStreamNonBlocking));
-      L.hold.own = true;
-      FPLS_CHECK(cudaStreamWaitEvent(L.hold.st, ready, 0));
-    }
-    const cudaStream_t st = L.hold.st;
+    LaneState& L = ws->lanes[l];
+    const cudaStream_t st = L.st;
     const int c = L.cnt;
-    L.d_if.allocate(c, st);
-    L.d_ip.allocate(c, st);
-    FPLS_CHECK(cudaMemcpyAsync(L.d_if.get(), inst_fold.data() + L.off, sizeof(int) * c,
-                               cudaMemcpyHostToDevice, st));
-    FPLS_CHECK(cudaMemcpyAsync(L.d_ip.get(), inst_perm.data() + L.off, sizeof(int) * c,
-                               cudaMemcpyHostToDevice, st));
-    InstanceView& v = L.v;
-    v.n = n;
-    v.q = q;
-    v.kmax = kmax;
-    v.B = 0;
-    v.center = center ? 1 : 0;
-    v.fold_of_row = d_fold.get();
-    v.inst_fold = L.d_if.get();
-    v.inst_perm = L.d_ip.get();
-    v.perms = perms;
-    v.ntrain = d_ntrain.get();
-    v.test_rows = d_test_rows.get();
-    v.test_off = d_test_off.get();
-    v.Y = Y64.get();
-    v.labels = class_labels;
-    L.C0.allocate(nq * c, st);
-    L.C.allocate(nq * c, st);
-    L.G.allocate((size_t)c * q * (q + 1) / 2, st);
-    L.ym.allocate((size_t)c * q, st);
-    L.sst.allocate(c, st);
-    L.sse.allocate((size_t)c * prefix_count, st);
-    L.yhat.allocate((size_t)c * max_test * q, st);
-    L.Wb.allocate((size_t)c * n * kmax, st);
-    L.KWb.allocate((size_t)c * n * kmax, st);
-    L.Ws.allocate((size_t)c * kmax, st);
-    L.U.allocate((size_t)n * c, st);
-    L.Y1.allocate((size_t)n * c, st);
-    L.KC0.allocate(nq * c, st);
-
-    init_instances<<<c, BT, 0, st>>>(v, L.C0.get(), L.C.get(), L.ym.get(), L.sst.get(),
-                                     L.yhat.get(), max_test, L.sse.get(), prefix_count);
+    const size_t o = L.off;
+    const InstanceView& v = L.v;
+    FPLS_CHECK(cudaStreamWaitEvent(st, ws->fork, 0));
+    if (v.amb) FPLS_CHECK(cudaMemsetAsync(v.amb, 0, sizeof(int) * c, st));
+    init_instances<<<c, BT, 0, st>>>(v, ws->C0.get() + o * nq, ws->C.get() + o * nq,
+                                     ws->ym.get() + o * q, ws->sst.get() + o,
+                                     ws->yhat.get() + o * max_test * q, max_test,
+                                     ws->sse.get() + o * prefix_count, prefix_count);
     count_launch();
     FPLS_LAUNCH("init_instances");
     // G0 = C0^T K C0 via one product over all instances' C0 columns
-    gram_product(L.C0.get(), q * c, L.KC0.get(), L.rhs, st);
-    initial_gram<<<c, BT, 0, st>>>(v, L.C0.get(), L.KC0.get(), L.G.get());
+    gram_product(ws->C0.get() + o * nq, q * c, ws->KC0.get() + o * nq, L.rhs, tile_n, st);
+    initial_gram<<<c, BT, 0, st>>>(v, ws->C0.get() + o * nq, ws->KC0.get() + o * nq,
+                                   ws->G.get() + o * q * (q + 1) / 2);
     count_launch();
     FPLS_LAUNCH("initial_gram");
     // first direction; K u comes from K C0 (no GEMM)
-    direction_batched<<<c, BT, smem_dir, st>>>(v, L.G.get(), L.C.get(), L.U.get(), L.KC0.get(),
-                                               L.Y1.get(), flag.get());
+    direction_batched<<<c, BT, smem_dir, st>>>(v, ws->G.get() + o * q * (q + 1) / 2,
+                                               ws->C.get() + o * nq, ws->U.get() + o * n,
+                                               ws->KC0.get() + o * nq, ws->Y1.get() + o * n,
+                                               ws->flag.get());
     count_launch();
     FPLS_LAUNCH("direction_batched");
-    L.KC0.release();
   }
   for (int a = 0; a < kmax; ++a) {
-    for (Lane& L : lanes) {
-      const cudaStream_t st = L.hold.st;
+    for (int l = 0; l < nlanes; ++l) {
+      LaneState& L = ws->lanes[l];
+      const cudaStream_t st = L.st;
       const int c = L.cnt;
+      const size_t o = L.off;
       const InstanceView& v = L.v;
-      if (a > 0) gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);  // Y1 = K u
+      double* U = ws->U.get() + o * n;
+      double* Y1 = ws->Y1.get() + o * n;
+      double* C0 = ws->C0.get() + o * nq;
+      double* ym = ws->ym.get() + o * q;
+      double* yhat = ws->yhat.get() + o * max_test * q;
+      double* sse = ws->sse.get() + o * prefix_count;
+      if (a > 0) gram_product(U, c, Y1, L.rhs, tile_n, st);  // Y1 = K u
       switch (rpt) {
-#define FPLS_SCORES(R)                                                                         \
-  case R:                                                                                      \
-    scores_rows<R><<<c, BT, 0, st>>>(v, L.Y1.get(), L.U.get(), L.C0.get(), L.ym.get(),         \
-                                     L.yhat.get(), max_test, a, d_slot.get(), prefix_count,    \
-                                     L.sse.get(), flag.get());                                 \
+#define FPLS_SCORES(R)                                                                  \
+  case R:                                                                               \
+    scores_rows<R><<<c, BT, 0, st>>>(v, Y1, U, C0, ym, yhat, max_test, a, ws->d_slot.get(), \
+                                     prefix_count, sse, ws->flag.get());                \
     break;
         FPLS_SCORES(8)
         FPLS_SCORES(16)
@@ -781,49 +946,236 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
         FPLS_SCORES(32)
 #undef FPLS_SCORES
         default:
-          scores_batched<<<c, BT, 0, st>>>(v, L.Y1.get(), L.U.get(), L.C0.get(), L.ym.get(),
-                                           L.yhat.get(), max_test, a, d_slot.get(),
-                                           prefix_count, L.sse.get(), nullptr, flag.get());
+          scores_batched<<<c, BT, 0, st>>>(v, Y1, U, C0, ym, yhat, max_test, a, ws->d_slot.get(),
+                                           prefix_count, sse, nullptr, ws->flag.get());
       }
       count_launch();
       FPLS_LAUNCH("scores_batched");
       if (a + 1 == kmax) continue;  // the last deflation is never used
       // Y1 = K t~ (U holds the masked training scores)
-      gram_product(L.U.get(), c, L.Y1.get(), L.rhs, st);
-      const size_t smem_defl = (2 * (size_t)q * q + 2 * (size_t)kmax + q) * sizeof(double);
+      gram_product(U, c, Y1, L.rhs, tile_n, st);
+      double* Wb = ws->Wb.get() + o * n * kmax;
+      double* KWb = ws->KWb.get() + o * n * kmax;
+      double* Ws = ws->Ws.get() + o * kmax;
+      double* C = ws->C.get() + o * nq;
+      double* G = ws->G.get() + o * q * (q + 1) / 2;
       if (q <= 4)
-        deflate_batched<4><<<c, DEFL_BT, smem_defl, st>>>(v, L.Y1.get(), L.U.get(), L.Wb.get(),
-                                                     L.KWb.get(), L.Ws.get(), L.C.get(),
-                                                     L.G.get(), a, flag.get());
+        deflate_batched<4><<<c, DEFL_BT, smem_defl, st>>>(v, Y1, U, Wb, KWb, Ws, C, G, a,
+                                                          ws->flag.get());
       else
         deflate_batched<kBatchMaxResponses><<<c, DEFL_BT, smem_defl, st>>>(
-            v, L.Y1.get(), L.U.get(), L.Wb.get(), L.KWb.get(), L.Ws.get(), L.C.get(), L.G.get(),
-            a, flag.get());
+            v, Y1, U, Wb, KWb, Ws, C, G, a, ws->flag.get());
       count_launch();
       FPLS_LAUNCH("deflate_batched");
     }
   }
-  // collect per-instance sums
-  std::vector<double> h_sse((size_t)I * prefix_count), h_sst(I);
-  for (Lane& L : lanes) {
-    FPLS_CHECK(cudaMemcpyAsync(h_sse.data() + (size_t)L.off * prefix_count, L.sse.get(),
-                               sizeof(double) * L.cnt * prefix_count, cudaMemcpyDeviceToHost,
-                               L.hold.st));
-    FPLS_CHECK(cudaMemcpyAsync(h_sst.data() + L.off, L.sst.get(), sizeof(double) * L.cnt,
-                               cudaMemcpyDeviceToHost, L.hold.st));
+  for (int l = 0; l < nlanes; ++l) {
+    FPLS_CHECK(cudaEventRecord(ws->lanes[l].done, ws->lanes[l].st));
+    FPLS_CHECK(cudaStreamWaitEvent(s, ws->lanes[l].done, 0));
   }
-  for (Lane& L : lanes) {
-    FPLS_CHECK(cudaStreamSynchronize(L.hold.st));
-    if (L.hold.own) {
-      // later work on the caller's stream follows this lane
-      cudaEvent_t done = nullptr;
-      FPLS_CHECK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-      FPLS_CHECK(cudaEventRecord(done, L.hold.st));
-      FPLS_CHECK(cudaStreamWaitEvent(s, done, 0));
-      cudaEventDestroy(done);
+}
+
+// One group of instances: lay the lanes out over the group-wide arrays, pick
+// the schedule (autotuned on the first group of a new shape), run the
+// component sequence (a replayed CUDA graph when the products are int8), and
+// collect each instance's sums.
+template <class T>
+void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
+                             const std::vector<int>& inst_perm, cudaStream_t s) {
+  const int I = (int)inst_fold.size();
+  if (I == 0) return;
+  BatchedStats& stats = last_batched_stats();
+  const size_t nq = (size_t)n * q;
+  const size_t cI = (size_t)I;
+  grow(ws->d_if, cI, s);
+  grow(ws->d_ip, cI, s);
+  grow(ws->amb, cI, s);
+  grow(ws->C0, nq * cI, s);
+  grow(ws->C, nq * cI, s);
+  grow(ws->G, cI * q * (q + 1) / 2, s);
+  grow(ws->ym, cI * q, s);
+  grow(ws->sst, cI, s);
+  grow(ws->sse, cI * prefix_count, s);
+  grow(ws->yhat, cI * max_test * q, s);
+  grow(ws->Wb, cI * n * kmax, s);
+  grow(ws->KWb, cI * n * kmax, s);
+  grow(ws->Ws, cI * kmax, s);
+  grow(ws->U, (size_t)n * cI, s);
+  grow(ws->Y1, (size_t)n * cI, s);
+  grow(ws->KC0, nq * cI, s);
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_if.get(), inst_fold.data(), sizeof(int) * I,
+                             cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_ip.get(), inst_perm.data(), sizeof(int) * I,
+                             cudaMemcpyHostToDevice, s));
+  const bool guard = class_labels && digits > 0 && argmax_guard() > 0.0;
+
+  // candidate schedules: lanes (each at least kLaneMinInstances instances)
+  // x tile widths 192 / 256, which combine the digit diagonals in the same
+  // FP64 order, so every candidate gives bit-identical results
+  const int max_lanes = std::max(1, std::min(kMaxLanes, I / kLaneMinInstances));
+  std::vector<TuneDecision> cands;
+  TuneDecision chosen;
+  chosen.lanes = std::max(1, std::min(batch_lanes(), max_lanes));
+  chosen.tile_n = digits > 0 ? ozaki_wide_tile(n, ceil_div(I, chosen.lanes)) : 0;
+  const std::vector<long long> key = {n, p, q, I, kmax, digits, class_labels ? 1 : 0};
+  bool tune = false;
+  if (digits > 0 && batch_autotune() && !ozaki_profile_enabled()) {
+    TuneDecision d;
+    if (tuner().find(key, &d) && d.lanes <= max_lanes) {
+      chosen = d;
+    } else {
+      tune = true;
+      for (int nl = 1; nl <= max_lanes; ++nl)
+        for (int tn : {192, 256}) cands.push_back({nl, tn, 0.0});
     }
   }
+  if (!tune) cands.assign(1, chosen);
+
+  auto layout = [&](int nlanes, int tile_n) {
+    for (int l = 0; l < nlanes; ++l) {
+      LaneState& L = ws->lanes[l];
+      L.off = l * (I / nlanes);
+      L.cnt = l + 1 == nlanes ? I - L.off : I / nlanes;
+      InstanceView& v = L.v;
+      v.n = n;
+      v.q = q;
+      v.kmax = kmax;
+      v.B = 0;
+      v.center = center ? 1 : 0;
+      v.fold_of_row = ws->d_fold.get();
+      v.inst_fold = ws->d_if.get() + L.off;
+      v.inst_perm = ws->d_ip.get() + L.off;
+      v.perms = perms;
+      v.ntrain = ws->d_ntrain.get();
+      v.test_rows = ws->d_test_rows.get();
+      v.test_off = ws->d_test_off.get();
+      v.Y = ws->Y64.get();
+      v.labels = class_labels;
+      v.guard = argmax_guard();
+      v.amb = guard ? ws->amb.get() + L.off : nullptr;
+      if (digits > 0) {
+        // size the digits of the largest right-hand side (K C0: q columns
+        // per instance) so the products inside the sequence never allocate
+        ozaki_reserve(L.rhs, std::max(q, 1) * L.cnt, n, digits, L.st);
+      }
+    }
+    (void)tile_n;
+  };
+
+  const bool use_graph = digits > 0 && !ozaki_profile_enabled();
+  auto run_schedule = [&](const TuneDecision& d, bool timed) -> double {
+    layout(d.lanes, d.tile_n);
+    if (timed) FPLS_CHECK(cudaEventRecord(ws->t0, s));
+    if (use_graph) {
+      std::vector<long long> gkey = {n, q, I, kmax, prefix_count, max_test, digits, center,
+                                     d.lanes, d.tile_n, class_labels ? 1 : 0, guard ? 1 : 0};
+      long long gbits = 0;
+      const double gv = argmax_guard();
+      std::memcpy(&gbits, &gv, sizeof(gbits));
+      gkey.push_back(gbits);
+      for (const void* ptr :
+           {(const void*)ws->d_if.get(), (const void*)ws->d_ip.get(), (const void*)ws->amb.get(),
+            (const void*)ws->C0.get(), (const void*)ws->C.get(), (const void*)ws->G.get(),
+            (const void*)ws->ym.get(), (const void*)ws->sst.get(), (const void*)ws->sse.get(),
+            (const void*)ws->yhat.get(), (const void*)ws->Wb.get(), (const void*)ws->KWb.get(),
+            (const void*)ws->Ws.get(), (const void*)ws->U.get(), (const void*)ws->Y1.get(),
+            (const void*)ws->KC0.get(), (const void*)ws->gram_split.digits.get(),
+            (const void*)ws->gram_split.scale.get(), (const void*)ws->Y64.get(),
+            (const void*)ws->d_fold.get(), (const void*)ws->d_ntrain.get(),
+            (const void*)ws->d_test_rows.get(), (const void*)ws->d_test_off.get(),
+            (const void*)ws->d_slot.get(), (const void*)ws->flag.get(), (const void*)perms,
+            (const void*)class_labels})
+        gkey.push_back((long long)(uintptr_t)ptr);
+      for (int l = 0; l < d.lanes; ++l) {
+        gkey.push_back((long long)(uintptr_t)ws->lanes[l].rhs.digits.get());
+        gkey.push_back((long long)(uintptr_t)ws->lanes[l].rhs.scale.get());
+      }
+      GroupGraph* found = nullptr;
+      for (GroupGraph& g : ws->graphs)
+        if (g.key == gkey) found = &g;
+      if (!found) {
+        const unsigned long long before = launch_count();
+        cudaGraph_t graph = nullptr;
+        FPLS_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue_group(I, d.lanes, d.tile_n, s);
+        } catch (...) {
+          cudaStreamEndCapture(s, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          cudaGetLastError();
+          throw;
+        }
+        FPLS_CHECK(cudaStreamEndCapture(s, &graph));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        FPLS_CHECK(rc);
+        if (ws->graphs.size() >= kMaxGraphs) {
+          cudaGraphExecDestroy(ws->graphs.front().exec);
+          ws->graphs.erase(ws->graphs.begin());
+        }
+        GroupGraph g;
+        g.key = gkey;
+        g.exec = exec;
+        // nothing ran during the capture: count the kernels when replayed
+        g.launches = launch_count() - before;
+        uncount_launch(g.launches);
+        ws->graphs.push_back(std::move(g));
+        found = &ws->graphs.back();
+        ++stats.graph_captures;
+      }
+      FPLS_CHECK(cudaGraphLaunch(found->exec, s));
+      count_launch((unsigned)found->launches);
+      ++stats.graph_replays;
+    } else {
+      enqueue_group(I, d.lanes, d.tile_n, s);
+    }
+    if (!timed) return 0.0;
+    FPLS_CHECK(cudaEventRecord(ws->t1, s));
+    FPLS_CHECK(cudaEventSynchronize(ws->t1));
+    float ms = 0.f;
+    FPLS_CHECK(cudaEventElapsedTime(&ms, ws->t0, ws->t1));
+    return ms;
+  };
+
+  if (tune) {
+    // every candidate computes the full group (identical results); the
+    // first run of each also captures its graph, so time a second replay
+    TuneDecision best;
+    best.ms = -1.0;
+    for (TuneDecision& c : cands) {
+      run_schedule(c, false);
+      c.ms = run_schedule(c, true);
+      if (best.ms < 0.0 || c.ms < best.ms) best = c;
+    }
+    tuner().store(key, best);
+    chosen = best;
+    ++stats.tuned;
+    // the last candidate's results are in place; when it is not the chosen
+    // schedule the results are the same, bit for bit
+  } else {
+    run_schedule(chosen, false);
+  }
+  ++stats.groups;
+  stats.lanes = chosen.lanes;
+  stats.tile_n = chosen.tile_n;
+
+  // collect per-instance sums
+  std::vector<double> h_sse((size_t)I * prefix_count), h_sst(I);
+  std::vector<int> h_amb(I, 0);
+  if (guard)
+    FPLS_CHECK(cudaMemcpyAsync(h_amb.data(), ws->amb.get(), sizeof(int) * I,
+                               cudaMemcpyDeviceToHost, s));
+  FPLS_CHECK(cudaMemcpyAsync(h_sse.data(), ws->sse.get(), sizeof(double) * I * prefix_count,
+                             cudaMemcpyDeviceToHost, s));
+  FPLS_CHECK(cudaMemcpyAsync(h_sst.data(), ws->sst.get(), sizeof(double) * I,
+                             cudaMemcpyDeviceToHost, s));
+  FPLS_CHECK(cudaStreamSynchronize(s));
   for (int k = 0; k < I; ++k) {
+    if (h_amb[k]) {
+      amb_fold.push_back(inst_fold[k]);
+      amb_perm.push_back(inst_perm[k]);
+    }
     const int f = inst_fold[k];
     const int b = inst_perm[k] + 1;  // 0 = observed responses
     for (int j = 0; j < prefix_count; ++j)
@@ -836,12 +1188,11 @@ template <class T>
 void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
                        const int* folds_host, const int* perms_dev,
                        int perm_count, const int* prefixes_, int count,
-                       int scaling_, cudaStream_t s) {
+                       int scaling_, cudaStream_t caller) {
   X = X_;
   n = n_;
   p = p_;
   q = q_;
-  perms = perms_dev;
   P = perm_count;
   prefix_count = count;
   scaling = scaling_;
@@ -876,25 +1227,70 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   for (int f = 0; f < folds; ++f) heldout[f] = (int)test[f].size();
   std::vector<int> slot(kmax + 1, -1);
   for (int j = 0; j < count; ++j) slot[prefixes_[j] - 1] = j;
-  d_fold.allocate(n, s);
-  d_ntrain.allocate(folds, s);
-  d_test_rows.allocate(std::max(1, (int)test_rows.size()), s);
-  d_test_off.allocate(folds + 1, s);
-  d_slot.allocate(kmax + 1, s);
-  flag.allocate(1, s);
-  FPLS_CHECK(cudaMemsetAsync(flag.get(), 0, sizeof(int), s));
-  FPLS_CHECK(cudaMemcpyAsync(d_fold.get(), folds_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
-  FPLS_CHECK(cudaMemcpyAsync(d_ntrain.get(), ntrain.data(), sizeof(int) * folds, cudaMemcpyHostToDevice, s));
-  FPLS_CHECK(cudaMemcpyAsync(d_test_rows.get(), test_rows.data(), sizeof(int) * test_rows.size(), cudaMemcpyHostToDevice, s));
-  FPLS_CHECK(cudaMemcpyAsync(d_test_off.get(), test_off.data(), sizeof(int) * (folds + 1), cudaMemcpyHostToDevice, s));
-  FPLS_CHECK(cudaMemcpyAsync(d_slot.get(), slot.data(), sizeof(int) * (kmax + 1), cudaMemcpyHostToDevice, s));
-  Y64.allocate((size_t)n * q, s);
-  to_f64<T><<<std::min<unsigned>(ceil_div((size_t)n * q, 256), 4 * num_sms()), 256, 0, s>>>(Y_, (long)n * q, Y64.get());
+
+  // One batched call at a time uses the device's persistent workspace;
+  // a concurrent call (another host thread) gets a private one.
+  int dev = 0;
+  FPLS_CHECK(cudaGetDevice(&dev));
+  require(dev >= 0 && dev < kMaxDevices, "device index beyond the batched workspace table");
+  std::unique_lock<std::mutex> lock(workspace_mutex(), std::try_to_lock);
+  std::unique_ptr<BatchedWorkspace> own;
+  if (lock.owns_lock()) {
+    if (!workspace_slot(dev)) workspace_slot(dev) = new BatchedWorkspace();
+    ws = workspace_slot(dev);
+  } else {
+    own.reset(new BatchedWorkspace());
+    ws = own.get();
+  }
+  last_batched_stats() = BatchedStats{};
+  const cudaStream_t s = ws->main;
+  // the caller's earlier work (input copies) before ours; ours before its later work
+  FPLS_CHECK(cudaEventRecord(ws->fork, caller));
+  FPLS_CHECK(cudaStreamWaitEvent(s, ws->fork, 0));
+  struct Join {
+    BatchedWorkspace* ws;
+    cudaStream_t caller;
+    ~Join() {
+      if (cudaEventRecord(ws->joined, ws->main) == cudaSuccess)
+        cudaStreamWaitEvent(caller, ws->joined, 0);
+    }
+  } join{ws, caller};
+
+  grow(ws->d_fold, n, s);
+  grow(ws->d_ntrain, folds, s);
+  grow(ws->d_test_rows, test_rows.size(), s);
+  grow(ws->d_test_off, folds + 1, s);
+  grow(ws->d_slot, kmax + 1, s);
+  grow(ws->flag, 1, s);
+  FPLS_CHECK(cudaMemsetAsync(ws->flag.get(), 0, sizeof(int), s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_fold.get(), folds_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_ntrain.get(), ntrain.data(), sizeof(int) * folds, cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_test_rows.get(), test_rows.data(), sizeof(int) * test_rows.size(), cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_test_off.get(), test_off.data(), sizeof(int) * (folds + 1), cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_slot.get(), slot.data(), sizeof(int) * (kmax + 1), cudaMemcpyHostToDevice, s));
+  // permutations and labels are copied in, so that captured groups always
+  // read them at the workspace's addresses
+  perms = nullptr;
+  if (P > 0) {
+    grow(ws->perms, (size_t)P * n, s);
+    FPLS_CHECK(cudaMemcpyAsync(ws->perms.get(), perms_dev, sizeof(int) * (size_t)P * n,
+                               cudaMemcpyDeviceToDevice, s));
+    perms = ws->perms.get();
+  }
+  const int* caller_labels = class_labels;
+  if (caller_labels) {
+    grow(ws->labels, n, s);
+    FPLS_CHECK(cudaMemcpyAsync(ws->labels.get(), caller_labels, sizeof(int) * n,
+                               cudaMemcpyDeviceToDevice, s));
+    class_labels = ws->labels.get();
+  }
+  grow(ws->Y64, (size_t)n * q, s);
+  to_f64<T><<<std::min<unsigned>(ceil_div((size_t)n * q, 256), 4 * num_sms()), 256, 0, s>>>(Y_, (long)n * q, ws->Y64.get());
   count_launch();
   FPLS_LAUNCH("to_f64");
   {
     DeviceArray<double> cs((size_t)2 * q, s);
-    response_moments<<<q, 256, 0, s>>>(Y64.get(), n, cs.get());
+    response_moments<<<q, 256, 0, s>>>(ws->Y64.get(), n, cs.get());
     count_launch();
     FPLS_LAUNCH("response_moments");
     std::vector<double> h(2 * q);
@@ -910,11 +1306,14 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   inst_sst.assign((size_t)B * folds, 0.0);
 
   // instances per group bounded by device memory (per instance: C0, C, W,
-  // KW, U, Y1 and held-out predictions)
+  // KW, U, Y1 and held-out predictions); the workspace's instance arrays are
+  // reused, so they count as available
   size_t free_b = 0, total_b = 0;
   FPLS_CHECK(cudaMemGetInfo(&free_b, &total_b));
-  const size_t per_inst = sizeof(double) * ((size_t)n * (2 * q + 2 * kmax + 2 + q) + (size_t)max_test * q + 64);
-  const size_t budget = free_b > ((size_t)n * n * 8 + (1ull << 30)) ? free_b - (size_t)n * n * 8 - (1ull << 30) : per_inst;
+  free_b += ws->held_bytes();
+  const size_t per_inst = sizeof(double) * ((size_t)n * (3 * q + 2 * kmax + 2) + (size_t)max_test * q + 64);
+  const size_t gram_b = (size_t)n * n * 8 + (digits > 0 ? (size_t)digits * n * n : 0);
+  const size_t budget = free_b > gram_b + (1ull << 30) ? free_b - gram_b - (1ull << 30) : per_inst;
   const int max_group = std::max(1, (int)std::min<size_t>(budget * 7 / 10 / per_inst, 1 << 20));
 
   auto run_instances = [&](const std::vector<int>& fl, const std::vector<int>& pl) {
@@ -925,6 +1324,26 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
       run_group(a, b, s);
     }
   };
+  // Classification with int8 products: instances with a held-out decision
+  // inside the argmax margin are refitted with FP64 products (FP64 Gram and
+  // DMMA products), replacing their hit counts.
+  amb_fold.clear();
+  amb_perm.clear();
+  refitted = 0;
+  auto refit_ambiguous = [&](const double* kscale) {
+    if (amb_fold.empty()) return;
+    const int saved = digits;
+    std::vector<int> fl, pl;
+    fl.swap(amb_fold);
+    pl.swap(amb_perm);
+    refitted += (int)fl.size();
+    digits = 0;
+    form_gram(kscale, s);
+    run_instances(fl, pl);
+    digits = saved;
+    amb_fold.clear();
+    amb_perm.clear();
+  };
 
   if (scaling == 2) {
     // autoscaling: one Gram per fold with that fold's training-row scales
@@ -934,7 +1353,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
     for (int f = 0; f < folds; ++f) {
       if (test[f].empty()) continue;
       heldout_moments<T><<<std::min(p, 8 * num_sms()), 256, 0, s>>>(
-          X, n, p, d_test_rows.get() + test_off[f], (int)test[f].size(), hmom.get(), hmom.get() + p);
+          X, n, p, ws->d_test_rows.get() + test_off[f], (int)test[f].size(), hmom.get(), hmom.get() + p);
       fold_kscale<<<std::min<unsigned>(ceil_div(p, 256), 4 * num_sms()), 256, 0, s>>>(
           mom.get(), mom.get() + p, hmom.get(), hmom.get() + p, p, ntrain[f], ks.get());
       count_launch(2);
@@ -946,6 +1365,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
         pl.push_back(b - 1);
       }
       run_instances(fl, pl);
+      refit_ambiguous(ks.get());
     }
   } else {
     form_gram(nullptr, s);
@@ -957,10 +1377,13 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
         pl.push_back(b - 1);
       }
     run_instances(fl, pl);
+    refit_ambiguous(nullptr);
   }
+  last_guard_refits() = refitted;
   int bad = 0;
-  FPLS_CHECK(cudaMemcpyAsync(&bad, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  FPLS_CHECK(cudaMemcpyAsync(&bad, ws->flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
   FPLS_CHECK(cudaStreamSynchronize(s));
+  class_labels = caller_labels;
   if (bad) throw std::runtime_error("resident SIMPLS failed: invalid labels, decomposition or component norm");
 }
 

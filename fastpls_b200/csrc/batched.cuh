@@ -13,7 +13,32 @@ constexpr int kBatchMaxResponses = 32;
 // Instance groups run as up to batch_lanes() interleaved stream lanes of at
 // least kLaneMinInstances instances each (process-wide setting, 1..4).
 constexpr int kLaneMinInstances = 32;
+constexpr int kMaxLanes = 4;
 int& batch_lanes();
+// Relative top-two margin under which a held-out class decision made with
+// int8 products is refitted with FP64 products (process-wide; 0 disables),
+// and the number of instances the last batched classification run refitted.
+double& argmax_guard();
+int& last_guard_refits();
+// Autotuning of the group schedule (lanes x tile width), keyed on
+// (n, p, q, instances, components, digits): 1 = time the candidates on the
+// first group of a new key and keep the fastest (default), 0 = the fixed
+// rule (batch_lanes() lanes, tile width from the wave count).
+int& batch_autotune();
+// Group statistics of the last batched call, for benchmarks and tests.
+struct BatchedStats {
+  int groups = 0;             // instance groups run
+  int graph_replays = 0;      // group runs that replayed a captured CUDA graph
+  int graph_captures = 0;     // graphs captured (first use of a group shape)
+  int tuned = 0;              // groups whose schedule was chosen by timing
+  int lanes = 0, tile_n = 0;  // schedule of the last group
+};
+BatchedStats& last_batched_stats();
+// Frees the persistent per-device workspace of the batched engine (device
+// buffers, lane streams and captured graphs); the next call rebuilds it.
+void release_batched_workspace();
+
+struct BatchedWorkspace;
 
 template <class T>
 struct BatchedCv {
@@ -40,26 +65,30 @@ struct BatchedCv {
   std::vector<double> inst_sst;     // (P+1) x folds
   std::vector<int> heldout;         // held-out rows per fold
   long double total_ss = 0.0L;
+  int refitted = 0;                 // classification instances refitted with
+                                    // FP64 products by the argmax guard
 
  private:
   void form_gram(const double* kscale, cudaStream_t s);
   void run_group(const std::vector<int>& inst_fold,
                  const std::vector<int>& inst_perm, cudaStream_t s);
+  // Enqueues the whole component sequence of one group (all lanes) on the
+  // workspace's lane streams, forked from and joined back into s.
+  void enqueue_group(int I, int nlanes, int tile_n, cudaStream_t s);
   // out (n x cols) = K rhs, rhs n x cols column-major (ld n): FP64 DMMA or,
   // when digits > 0, the int8 split product with the digits of K prepared by
-  // form_gram (rhs_split receives the digits of rhs).
+  // form_gram (rhs_split receives the digits of rhs), tile width tile_n.
   void gram_product(const double* rhs, int cols, double* out, OzakiOperand& rhs_split,
-                    cudaStream_t s);
+                    int tile_n, cudaStream_t s);
 
+  BatchedWorkspace* ws = nullptr;
   const T* X = nullptr;
   const int* perms = nullptr;
   int n = 0, p = 0, q = 0, P = 0, prefix_count = 0, scaling = 1, kmax = 0;
   int folds = 0, max_test = 1;
   bool center = true;
   int digits = 0;                 // int8 digits per FP64 value (0: FP64 DMMA)
-  OzakiOperand gram_split, x_split;
-  DeviceArray<double> gram, Y64, x64;
-  DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag;
+  std::vector<int> amb_fold, amb_perm;  // instances flagged by the argmax guard
 };
 
 }  // namespace fpls

@@ -91,6 +91,9 @@ class DeviceArray {
 // Launch accounting: every kernel launch of this library goes through
 // count_launch() so callers (benchmarks) can report how many ran.
 void count_launch(unsigned n = 1);
+// Takes back launches counted while a CUDA graph was being captured (they
+// are counted again each time the graph is replayed).
+void uncount_launch(unsigned long long n);
 unsigned long long launch_count();
 
 inline int num_sms() {

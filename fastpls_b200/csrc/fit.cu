@@ -22,6 +22,7 @@
 //    deterministic, no atomics on data, no spin-waits.
 #include "kernels.cuh"
 #include "model.cuh"
+#include "persistent.cuh"
 #include "reduce.cuh"
 #include "small.cuh"
 
@@ -516,6 +517,10 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
   gram_of_columns(S.get(), p, m, gpk, ws, stream);
+
+  // one direction per component: the whole loop as one persistent launch
+  if (block <= 1 && fit_simpls_persistent<T>(X, n, p, ld, m, a_max, model, S.get(), gpk, ws, stream))
+    return;
 
   // Candidate blocks (the reference's block refresh): the directions of
   // `use` consecutive components are the leading left singular vectors of S

@@ -200,6 +200,44 @@ void check_path(const int* prefixes, int count, int a) {
 // T: storage type of the predictors (float, double, or bf16 for precision
 // 16); TO: type of responses and of every result written back (T, or float
 // for bf16 predictors).
+// Device time of the calling thread's last fit: input copies, then the fit
+// proper (CUDA events on the handle's stream, read once the fit finished).
+struct FitTimes {
+  double copy_ms = 0.0, fit_ms = 0.0;
+};
+FitTimes& last_fit_times() {
+  thread_local FitTimes t;
+  return t;
+}
+
+class FitTimer {
+ public:
+  explicit FitTimer(cudaStream_t s) : s_(s) {
+    for (cudaEvent_t& e : ev_) FPLS_CHECK(cudaEventCreate(&e));
+    FPLS_CHECK(cudaEventRecord(ev_[0], s_));
+  }
+  ~FitTimer() {
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+  }
+  FitTimer(const FitTimer&) = delete;
+  FitTimer& operator=(const FitTimer&) = delete;
+  void mark() { FPLS_CHECK(cudaEventRecord(ev_[++marks_], s_)); }
+  // after the stream has finished the fit
+  void finish() {
+    if (marks_ != 2) return;
+    float a = 0.f, b = 0.f;
+    FPLS_CHECK(cudaEventSynchronize(ev_[2]));
+    FPLS_CHECK(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+    FPLS_CHECK(cudaEventElapsedTime(&b, ev_[1], ev_[2]));
+    last_fit_times() = {a, b};
+  }
+
+ private:
+  cudaStream_t s_;
+  cudaEvent_t ev_[3] = {};
+  int marks_ = 0;
+};
+
 template <class T>
 class TypedHandle final : public ResidentHandle {
   using TO = typename io_type<T>::type;
@@ -407,6 +445,7 @@ class TypedHandle final : public ResidentHandle {
       throw std::invalid_argument(rq_.method == kPlssvd ? "invalid resident PLS-SVD dimensions"
                                                         : "invalid resident SIMPLS dimensions");
     if (cls && q < 2) throw std::invalid_argument("classification requires at least two classes");
+    FitTimer timer(stream_);
     xtrain_.allocate((size_t)n * p, stream_);
     FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
     DeviceArray<TO> y;
@@ -421,6 +460,7 @@ class TypedHandle final : public ResidentHandle {
       FPLS_CHECK(cudaMemcpyAsync(y.get(), rq_.y, sizeof(TO) * n * q, cudaMemcpyHostToDevice, stream_));
     }
     model_.classification = cls;
+    timer.mark();  // inputs on the device: the fit proper starts here
     ws_.ensure(n, p, q, a, stream_);
     FPLS_CHECK(cudaMemsetAsync(ws_.flag.get(), 0, sizeof(int), stream_));
     DeviceArray<double> yc((size_t)n * q, stream_);
@@ -439,10 +479,12 @@ class TypedHandle final : public ResidentHandle {
     else
       fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_,
                     simpls_block_size(n, p, q, a, cls, std::is_same<T, float>::value));
+    timer.mark();
     raise_on_flag(ws_, stream_, rq_.method == kPlssvd
         ? "resident PLS-SVD failed: invalid labels, decomposition or score Gram"
         : rq_.method == kOpls ? "resident CUDA OPLS filtering failed"
         : "resident SIMPLS failed: invalid labels, decomposition or component norm");
+    timer.finish();
   }
 
   void load(const ImportRequest& im) {
@@ -635,6 +677,12 @@ ResidentHandle* import_handle(int precision, const ImportRequest& im) {
   if (precision == 64) return new TypedHandle<double>(im);
   if (precision == 16) return new TypedHandle<bf16>(im);
   throw std::invalid_argument("invalid resident matrix or precision");
+}
+
+void read_last_fit_times(double* copy_ms, double* fit_ms) {
+  const FitTimes& t = last_fit_times();
+  if (copy_ms) *copy_ms = t.copy_ms;
+  if (fit_ms) *fit_ms = t.fit_ms;
 }
 
 ResidentHandle* make_handle(int precision, const FitRequest& rq) {

@@ -69,4 +69,10 @@ struct ImportRequest {
 
 ResidentHandle* import_handle(int precision, const ImportRequest& request);
 
+// Device time of the calling thread's last resident fit (CUDA events on the
+// handle's stream): the input copies and the fit proper, in milliseconds.
+struct FitTimes;
+FitTimes& last_fit_times();
+void read_last_fit_times(double* copy_ms, double* fit_ms);
+
 }  // namespace fpls

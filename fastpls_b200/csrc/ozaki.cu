@@ -952,8 +952,12 @@ void launch_gemm(const OzakiOperand& a, const OzakiOperand& b, OzArgs args, long
   args.stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
   require(args.stages >= 2, "int8 split product: stages do not fit shared memory");
   const size_t smem = (size_t)args.stages * stage_bytes + 1024;
-  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel<BN>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+  static const bool configured = [] {
+    FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel<BN>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+    return true;
+  }();
+  (void)configured;
   // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
   const int kb_total = a.k_p / OZ_BK;
   const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
@@ -988,8 +992,12 @@ void launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, OzArgs args,
   args.stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
   require(args.stages >= 2, "int8 split product: stages do not fit shared memory");
   const size_t smem = (size_t)args.stages * stage_bytes + 1024;
-  FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_pair_kernel<BN>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+  static const bool configured = [] {
+    FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_pair_kernel<BN>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+    return true;
+  }();
+  (void)configured;
   const int kb_total = a.k_p / OZ_BK;
   const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
   const int kb_seg = seg_bytes / OZ_BK;
@@ -1007,6 +1015,23 @@ void launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, OzArgs args,
 }  // namespace
 
 void ozaki_profile_enable(bool on) { oz_timing().enabled = on; }
+
+bool ozaki_profile_enabled() { return oz_timing().enabled; }
+
+void ozaki_reserve(OzakiOperand& out, int rows, int k, int slices, cudaStream_t stream) {
+  prepare(out, rows, k, slices, stream);
+}
+
+int ozaki_wide_tile(int a_rows, int b_rows) {
+  // waves of tiles x the measured clocks of one 128 x BN x 32 step (the
+  // single-CTA candidates of pick_tile)
+  const int sms = num_sms();
+  auto cost = [&](int bn, double step_clk) {
+    const long tiles = (long)ceil_div(a_rows, OZ_BM) * ceil_div(b_rows, bn);
+    return (double)((tiles + sms - 1) / sms) * step_clk;
+  };
+  return cost(256, 288.0) <= cost(192, 276.0) ? 256 : 192;
+}
 
 void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launches) {
   OzTiming& t = oz_timing();

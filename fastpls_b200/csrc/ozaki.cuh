@@ -60,12 +60,23 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C,
                 long ldc, bool lower, int* flag, cudaStream_t stream, int tile_n = 0,
                 int pair = -1);
 
+// Sizes out's buffers for `rows` x k digits (as the split would), so that a
+// later split of at most that many rows does not allocate (e.g. inside a
+// captured CUDA graph).
+void ozaki_reserve(OzakiOperand& out, int rows, int k, int slices, cudaStream_t stream);
+
+// The tile width (192 or 256) of a rectangular product of a_rows x b_rows
+// with the fewer waves of measured step cost. Both widths combine the digit
+// diagonals in the same FP64 order, so the choice never changes results.
+int ozaki_wide_tile(int a_rows, int b_rows);
+
 // Digit count used by the batched CV engine for its products with the
 // shared Gram (0 selects the FP64 DMMA path). Process-wide setting.
 int& ozaki_slices();
 
 // Timing of the last ozaki_gemm launches (CUDA events), for benchmarks.
 void ozaki_profile_enable(bool on);
+bool ozaki_profile_enabled();
 void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launches);
 
 }  // namespace fpls

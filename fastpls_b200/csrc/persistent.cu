@@ -1,0 +1,674 @@
+// Persistent single-fit SIMPLS: every component of a fit in one cooperative
+// launch.
+//
+// The per-component step of the p-space SIMPLS loop (the reference's
+// ComponentWorkspace::step, src/cuda_resident_component.cuh:94-130, and the
+// FP64 CPU body, inst/include/fastpls/core/simpls.hpp:588-756) is two
+// HBM-streaming passes over X (t = X r, p = X^T t) plus O(p (a + m)) vector
+// work whose reductions are grid-wide. As separate kernels that is about ten
+// launches per component, most of them tiny and latency-bound. Here one
+// grid of CTAs stays resident for the whole fit and walks through the
+// phases of each component, separated by group barriers:
+//
+//   B0  (last CTA) reduce the Gram of the deflated S, Jacobi -> z / sqrt(lambda)
+//   P1  r = S z, rt = r / scale, partial  c = mean . rt             -> B1: c
+//   P2  t partials over column chunks: sum_j X[i, j] rt[j]          -> B2
+//   P3  t = sum of partials - c, partial |t|^2 and sum t            -> B3: |t|, sum t
+//   P4  loading partials over row chunks: sum_i X[i, j] t[i]        -> B4
+//   P5  p = (X^T t - mean sum t) / (scale |t|), R[:, a] = r / |t|,
+//       partial V^T p and S0^T R[:, a]                              -> B5: h, q
+//   P6  v = p - V h, partial v.v and S^T v                          -> B6: |v|, S^T v
+//   P7  V[:, a] = v / |v|, S -= V[:, a] (S^T v / |v|)^T, partial Gram
+//       of S, T[:, a] /= |t|
+//
+// At each barrier the last CTA to arrive adds the per-CTA partials in CTA
+// order (deterministic) and publishes the result before releasing the
+// others. Chunk sizes depend only on (n, p), so the result does not depend
+// on the storage type of X: BF16 storage gives the same bits as FP32
+// storage of the same values. All arithmetic is FP64.
+//
+// Every barrier wait is bounded (about 2 s): on expiry the CTA sets the
+// error flag (5) and returns, so a fit never hangs. Blocks of one fit wait on
+// each other only inside this one cooperative launch (all of its CTAs are
+// co-resident).
+#include "kernels.cuh"
+#include "model.cuh"
+#include "persistent.cuh"
+#include "small.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace fpls {
+
+namespace {
+
+constexpr int PT = 256;                       // threads per CTA
+constexpr int kMaxXrCols = 2048;              // columns of rt staged per item
+constexpr int kMaxXtvRows = 4096;             // rows of t staged per item
+constexpr int kGramRows = 64;                 // S rows staged per Gram step
+constexpr int kSmemDoubles = 4096;            // 32 KB of dynamic shared memory
+constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s
+
+// scalar slots of a fit (global, FP64)
+constexpr int SC_Z = 0;            // z / sqrt(lambda): kPersistMaxResponses
+constexpr int SC_C = 32;           // mean . rt
+constexpr int SC_T2 = 33;          // |t|^2
+constexpr int SC_ST = 34;          // sum t
+constexpr int SC_VV = 35;          // |v|^2
+constexpr int SC_Q = 40;           // q (m)
+constexpr int SC_SV = 72;          // S^T v (m)
+constexpr int SC_H = 104;          // V^T p (a)
+
+struct Fit {
+  const void* X;
+  long ld;
+  int n, p, m, a;
+  const double* mean;
+  const double* scale;
+  const double* S0;
+  double *S, *R, *V, *Q, *T;
+  double* gpk;     // packed Gram of S (m (m + 1) / 2)
+  double *r, *rt, *pv, *v;  // p
+  double* tpart;   // kt x n
+  double* ppart;   // kp x p
+  double* cpart;   // C x cslots
+  double* scal;    // scalar slots
+  unsigned* bar;   // [count, generation]
+  int cta0, C;     // CTA range of this fit
+  int cc, kt;      // t pass: columns per chunk, chunks
+  int rc, kp;      // loading pass: rows per chunk, chunks
+  int vec;         // rows per 16-byte load in the t pass (1: scalar)
+  int pair;        // row pairs per lane in the loading pass
+  int cslots;      // per-CTA partial slots
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Barrier of the fit's CTAs. Every thread of the CTA calls it after writing
+// its partials. The last CTA to arrive runs reduce() (whole CTA, reading the
+// other CTAs' partials with L1-bypassing loads) before releasing the rest.
+// Returns false when a wait ran out (flag set to 5); the caller returns.
+template <class F>
+__device__ bool group_sync(const Fit& f, int* flag, F&& reduce) {
+  __shared__ int last_s, ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned gen = ld_acquire(f.bar + 1);
+    __threadfence();
+    const unsigned ticket = atomicAdd(f.bar, 1u);
+    last_s = ticket == (unsigned)f.C - 1u;
+    ok_s = 1;
+    if (!last_s) {
+      const long long t0 = clock64();
+      while (ld_acquire(f.bar + 1) == gen) {
+        if (clock64() - t0 > kBarrierCycles) {
+          flag_error(flag, 5);
+          ok_s = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  __syncthreads();
+  if (last_s) {
+    __threadfence();
+    reduce();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicExch(f.bar, 0u);
+      __threadfence();
+      atomicAdd(f.bar + 1, 1u);
+    }
+  }
+  __syncthreads();
+  __threadfence();
+  return ok_s != 0;
+}
+
+// CTA-level sum; every thread receives it.
+__device__ __forceinline__ double cta_sum(double v, double* red) { return block_sum(v, red); }
+
+// Contiguous column range [j0, j1) of CTA `c` out of C over p columns.
+__device__ __forceinline__ void col_range(int p, int C, int c, int& j0, int& j1) {
+  const int per = (p + C - 1) / C;
+  j0 = min(p, c * per);
+  j1 = min(p, j0 + per);
+}
+
+// Sum over the C per-CTA partials of slot `k` (stride cslots), CTA order.
+__device__ __forceinline__ double sum_slots(const Fit& f, int k) {
+  double s = 0.0;
+  for (int c = 0; c < f.C; ++c) s += __ldcg(f.cpart + (long)c * f.cslots + k);
+  return s;
+}
+
+template <class T> struct Vec16;
+template <> struct Vec16<float> {
+  static constexpr int N = 4;
+  using type = float4;
+  static __device__ __forceinline__ void get(const type& v, double (&o)[4]) {
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+};
+template <> struct Vec16<double> {
+  static constexpr int N = 2;
+  using type = double2;
+  static __device__ __forceinline__ void get(const type& v, double (&o)[2]) {
+    o[0] = v.x; o[1] = v.y;
+  }
+};
+template <> struct Vec16<bf16> {
+  static constexpr int N = 8;
+  using type = uint4;
+  static __device__ __forceinline__ void get(const type& v, double (&o)[8]) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      o[2 * k] = (double)__uint_as_float(w[k] << 16);
+      o[2 * k + 1] = (double)__uint_as_float(w[k] & 0xffff0000u);
+    }
+  }
+};
+
+template <class T> struct Pair2;
+template <> struct Pair2<float> {
+  using type = float2;
+  static __device__ __forceinline__ double lo(type v) { return v.x; }
+  static __device__ __forceinline__ double hi(type v) { return v.y; }
+};
+template <> struct Pair2<double> {
+  using type = double2;
+  static __device__ __forceinline__ double lo(type v) { return v.x; }
+  static __device__ __forceinline__ double hi(type v) { return v.y; }
+};
+template <> struct Pair2<bf16> {
+  using type = __nv_bfloat162;
+  static __device__ __forceinline__ double lo(type v) { return __low2float(v); }
+  static __device__ __forceinline__ double hi(type v) { return __high2float(v); }
+};
+
+// P2: partial scores of one item (row tile x column chunk k): thread rows
+// i .. i + VEC - 1, columns of the chunk in order.
+template <class T>
+__device__ void xr_item(const Fit& f, const T* X, int tile, int k, double* rts) {
+  constexpr int VN = Vec16<T>::N;
+  const int c0 = k * f.cc;
+  const int cols = min(f.cc, f.p - c0);
+  __syncthreads();
+  for (int j = threadIdx.x; j < cols; j += PT) rts[j] = __ldcg(f.rt + c0 + j);
+  __syncthreads();
+  const int vec = f.vec;  // VN or 1
+  const int rows_tile = PT * vec;
+  const int i = tile * rows_tile + threadIdx.x * vec;
+  if (i >= f.n) return;
+  double* out = f.tpart + (long)k * f.n;
+  const T* base = X + (long)c0 * f.ld + i;
+  if (vec == VN && i + VN <= f.n) {
+    using V = typename Vec16<T>::type;
+    double acc[VN];
+#pragma unroll
+    for (int u = 0; u < VN; ++u) acc[u] = 0.0;
+    int j = 0;
+    for (; j + 3 < cols; j += 4) {
+      V x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        x[u] = __ldg(reinterpret_cast<const V*>(base + (long)(j + u) * f.ld));
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        double e[VN];
+        Vec16<T>::get(x[u], e);
+        const double w = rts[j + u];
+#pragma unroll
+        for (int q = 0; q < VN; ++q) acc[q] = fma(e[q], w, acc[q]);
+      }
+    }
+    for (; j < cols; ++j) {
+      double e[VN];
+      Vec16<T>::get(__ldg(reinterpret_cast<const V*>(base + (long)j * f.ld)), e);
+      const double w = rts[j];
+#pragma unroll
+      for (int q = 0; q < VN; ++q) acc[q] = fma(e[q], w, acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < VN; ++q) out[i + q] = acc[q];
+  } else {
+    // scalar rows (unaligned storage, or the last rows of X)
+    const int cnt = min(vec, f.n - i);
+    for (int q = 0; q < cnt; ++q) {
+      double acc = 0.0;
+      for (int j = 0; j < cols; ++j) acc = fma(as_f64(base[q + (long)j * f.ld]), rts[j], acc);
+      out[i + q] = acc;
+    }
+  }
+}
+
+// P4: loading partials of one item (row chunk kc x 32 columns from jt*32):
+// warp per column, lanes over row pairs (or rows), t rows staged in shared
+// memory.
+template <class T>
+__device__ void xtv_item(const Fit& f, const T* X, int kc, int jt, const double* tcol,
+                         double* ts) {
+  const int r0 = kc * f.rc;
+  const int rows = min(f.rc, f.n - r0);
+  __syncthreads();
+  for (int r = threadIdx.x; r < rows; r += PT) ts[r] = __ldcg(tcol + r0 + r);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int jj = warp; jj < 32; jj += PT / 32) {
+    const int j = jt * 32 + jj;
+    if (j >= f.p) break;
+    const T* col = X + (long)j * f.ld + r0;
+    double acc = 0.0;
+    if (f.pair) {
+      using P = Pair2<T>;
+      const typename P::type* col2 = reinterpret_cast<const typename P::type*>(col);
+      const int pairs = rows >> 1;
+      int q = lane;
+      for (; q + 96 < pairs; q += 128) {
+        typename P::type x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = __ldg(col2 + q + 32 * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = 2 * (q + 32 * u);
+          acc = fma(P::lo(x[u]), ts[r], acc);
+          acc = fma(P::hi(x[u]), ts[r + 1], acc);
+        }
+      }
+      for (; q < pairs; q += 32) {
+        const typename P::type x = __ldg(col2 + q);
+        acc = fma(P::lo(x), ts[2 * q], acc);
+        acc = fma(P::hi(x), ts[2 * q + 1], acc);
+      }
+      if ((rows & 1) && lane == 0) acc = fma(as_f64(col[rows - 1]), ts[rows - 1], acc);
+    } else {
+      for (int r = lane; r < rows; r += 32) acc = fma(as_f64(col[r]), ts[r], acc);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) f.ppart[(long)kc * f.p + j] = acc;
+  }
+}
+
+// Dominant eigenpair of the packed m x m Gram (whole CTA): zs = s z / sqrt(lambda),
+// sign fixed so the largest |z| entry is positive (as direction_kernel).
+__device__ void direction_step(const Fit& f, double* sm, int* flag) {
+  const int m = f.m;
+  double* A = sm;
+  double* E = sm + m * m;
+  for (int c = threadIdx.x; c < m; c += blockDim.x)
+    for (int d = 0; d <= c; ++d) {
+      const double v = __ldcg(f.gpk + c * (c + 1) / 2 + d);
+      A[c + d * m] = v;
+      A[d + c * m] = v;
+    }
+  __syncthreads();
+  jacobi_eigen(A, E, m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int best = 0;
+    for (int k = 1; k < m; ++k)
+      if (A[k + k * m] > A[best + best * m]) best = k;
+    const double lam = A[best + best * m];
+    const bool ok = lam > 0.0 && isfinite(lam);
+    if (!ok) flag_error(flag, 1);
+    const double inv = ok ? 1.0 / sqrt(lam) : 0.0;
+    int arg = 0;
+    for (int k = 1; k < m; ++k)
+      if (fabs(E[k + best * m]) > fabs(E[arg + best * m])) arg = k;
+    const double sgn = E[arg + best * m] < 0.0 ? -1.0 : 1.0;
+    for (int k = 0; k < m; ++k) f.scal[SC_Z + k] = sgn * E[k + best * m] * inv;
+  }
+  __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(PT, 2)
+    persistent_simpls(const Fit* __restrict__ fits, int nfits, int* flag) {
+  extern __shared__ double psm[];
+  __shared__ double red[32];
+  __shared__ double zs[kPersistMaxResponses];
+  __shared__ double hs[kPersistMaxComponents];
+  __shared__ double sv[kPersistMaxResponses];
+  __shared__ double scal_s[4];
+  int fi = 0;
+  while (fi + 1 < nfits && (int)blockIdx.x >= fits[fi + 1].cta0) ++fi;
+  const Fit f = fits[fi];
+  const int cta = (int)blockIdx.x - f.cta0;
+  const T* X = static_cast<const T*>(f.X);
+  const int n = f.n, p = f.p, m = f.m, C = f.C;
+  const int tid = threadIdx.x;
+  int j0, j1;
+  col_range(p, C, cta, j0, j1);
+
+  for (int a = 0; a < f.a; ++a) {
+    // B0: Gram of the deflated S (after the first component) and direction
+    if (!group_sync(f, flag, [&] {
+          if (a > 0) {
+            const int G = m * (m + 1) / 2;
+            for (int k = tid; k < G; k += PT) f.gpk[k] = sum_slots(f, k);
+            __syncthreads();
+            __threadfence();
+          }
+          direction_step(f, psm, flag);
+        }))
+      return;
+    for (int c = tid; c < m; c += PT) zs[c] = __ldcg(f.scal + SC_Z + c);
+    __syncthreads();
+    // P1: r = S z, rt = r / scale, partial mean . rt
+    double acc = 0.0;
+    for (int j = cta * PT + tid; j < p; j += C * PT) {
+      double rv = 0.0;
+      for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + j + (long)c * p), zs[c], rv);
+      const double w = rv / f.scale[j];
+      f.r[j] = rv;
+      f.rt[j] = w;
+      acc = fma(f.mean[j], w, acc);
+    }
+    acc = cta_sum(acc, red);
+    if (tid == 0) f.cpart[(long)cta * f.cslots] = acc;
+    if (!group_sync(f, flag, [&] {
+          if (tid == 0) f.scal[SC_C] = sum_slots(f, 0);
+        }))
+      return;
+    // P2: score partials, items (row tile, column chunk)
+    {
+      const int tiles = (n + PT * f.vec - 1) / (PT * f.vec);
+      const int items = tiles * f.kt;
+      for (int it = cta; it < items; it += C) xr_item<T>(f, X, it % tiles, it / tiles, psm);
+    }
+    if (!group_sync(f, flag, [] {})) return;
+    // P3: t = sum of the chunk partials - c; |t|^2 and sum t
+    {
+      const double cc = __ldcg(f.scal + SC_C);
+      double* tcol = f.T + (long)a * n;
+      double s2 = 0.0, s1 = 0.0;
+      for (int i = cta * PT + tid; i < n; i += C * PT) {
+        double s = 0.0;
+        for (int k = 0; k < f.kt; ++k) s += __ldcg(f.tpart + (long)k * n + i);
+        const double t = s - cc;
+        tcol[i] = t;
+        s2 = fma(t, t, s2);
+        s1 += t;
+      }
+      s2 = cta_sum(s2, red);
+      s1 = cta_sum(s1, red);
+      if (tid == 0) {
+        f.cpart[(long)cta * f.cslots] = s2;
+        f.cpart[(long)cta * f.cslots + 1] = s1;
+      }
+    }
+    if (!group_sync(f, flag, [&] {
+          if (tid == 0) {
+            f.scal[SC_T2] = sum_slots(f, 0);
+            f.scal[SC_ST] = sum_slots(f, 1);
+          }
+        }))
+      return;
+    // P4: loading partials, items (row chunk, 32-column tile)
+    {
+      const int jtiles = (p + 31) / 32;
+      const int items = jtiles * f.kp;
+      const double* tcol = f.T + (long)a * n;
+      for (int it = cta; it < items; it += C) xtv_item<T>(f, X, it % f.kp, it / f.kp, tcol, psm);
+    }
+    if (!group_sync(f, flag, [] {})) return;
+    // P5: p, R[:, a]; partial V^T p (a) and S0^T R[:, a] (m)
+    if (tid == 0) {
+      const double t2 = __ldcg(f.scal + SC_T2);
+      const double tn = sqrt(t2);
+      const bool ok = tn > 0.0 && isfinite(tn);
+      if (!ok && cta == 0) flag_error(flag, 1);
+      scal_s[0] = ok ? 1.0 / tn : 0.0;
+      scal_s[1] = __ldcg(f.scal + SC_ST);
+    }
+    __syncthreads();
+    const double inv_t = scal_s[0], sum_t = scal_s[1];
+    double* ps = psm;          // p values of this CTA's columns (<= 4096)
+    double* rs = psm + 2048;   // R values
+    for (int jl = tid; jl < j1 - j0; jl += PT) {
+      const int j = j0 + jl;
+      double pr = 0.0;
+      for (int k = 0; k < f.kp; ++k) pr += __ldcg(f.ppart + (long)k * p + j);
+      const double pj = (pr - f.mean[j] * sum_t) / f.scale[j] * inv_t;
+      const double rj = __ldcg(f.r + j) * inv_t;
+      f.pv[j] = pj;
+      f.R[j + (long)a * p] = rj;
+      ps[jl] = pj;
+      rs[jl] = rj;
+    }
+    __syncthreads();
+    {
+      const int lane = tid & 31, warp = tid >> 5;
+      const int cols = j1 - j0;
+      for (int k = warp; k < a + m; k += PT / 32) {
+        double s = 0.0;
+        if (k < a) {
+          const double* vk = f.V + (long)k * p + j0;
+          for (int jl = lane; jl < cols; jl += 32) s = fma(__ldcg(vk + jl), ps[jl], s);
+        } else {
+          const double* sk = f.S0 + (long)(k - a) * p + j0;
+          for (int jl = lane; jl < cols; jl += 32) s = fma(sk[jl], rs[jl], s);
+        }
+        s = warp_sum(s);
+        if (lane == 0) f.cpart[(long)cta * f.cslots + k] = s;
+      }
+    }
+    if (!group_sync(f, flag, [&] {
+          for (int k = tid; k < a + m; k += PT) {
+            const double s = sum_slots(f, k);
+            if (k < a) f.scal[SC_H + k] = s;
+            else {
+              f.scal[SC_Q + k - a] = s;
+              f.Q[(k - a) + (long)a * m] = s;
+            }
+          }
+        }))
+      return;
+    // P6: v = p - V h; partial v.v and S^T v
+    for (int k = tid; k < a; k += PT) hs[k] = __ldcg(f.scal + SC_H + k);
+    __syncthreads();
+    double* vs = psm;  // v of this CTA's columns
+    double vvp = 0.0;
+    for (int jl = tid; jl < j1 - j0; jl += PT) {
+      const int j = j0 + jl;
+      double vj = __ldcg(f.pv + j);
+      for (int k = 0; k < a; ++k) vj = fma(-__ldcg(f.V + j + (long)k * p), hs[k], vj);
+      f.v[j] = vj;
+      vs[jl] = vj;
+      vvp = fma(vj, vj, vvp);
+    }
+    vvp = cta_sum(vvp, red);  // (synchronises: vs complete)
+    {
+      const int lane = tid & 31, warp = tid >> 5;
+      const int cols = j1 - j0;
+      for (int c = warp; c < m; c += PT / 32) {
+        const double* sc = f.S + (long)c * p + j0;
+        double s = 0.0;
+        for (int jl = lane; jl < cols; jl += 32) s = fma(__ldcg(sc + jl), vs[jl], s);
+        s = warp_sum(s);
+        if (lane == 0) f.cpart[(long)cta * f.cslots + 1 + c] = s;
+      }
+      if (tid == 0) f.cpart[(long)cta * f.cslots] = vvp;
+    }
+    if (!group_sync(f, flag, [&] {
+          for (int k = tid; k < 1 + m; k += PT) {
+            const double s = sum_slots(f, k);
+            if (k == 0) f.scal[SC_VV] = s;
+            else f.scal[SC_SV + k - 1] = s;
+          }
+        }))
+      return;
+    // P7: V[:, a], deflate S, partial Gram of the deflated S; T[:, a] /= |t|
+    if (tid == 0) {
+      const double vn = sqrt(__ldcg(f.scal + SC_VV));
+      const bool ok = vn > 0.0 && isfinite(vn);
+      if (!ok && cta == 0) flag_error(flag, 1);
+      scal_s[2] = ok ? 1.0 / vn : 0.0;
+    }
+    for (int c = tid; c < m; c += PT) sv[c] = __ldcg(f.scal + SC_SV + c);
+    __syncthreads();
+    const double inv_v = scal_s[2];
+    {
+      const int G = m * (m + 1) / 2;
+      const int lane = tid & 31, warp = tid >> 5;
+      double* ss = psm;  // kGramRows x m
+      double* gacc = psm + kGramRows * kPersistMaxResponses;  // G running sums (warp-owned)
+      for (int k = tid; k < G; k += PT) gacc[k] = 0.0;
+      for (int g0 = j0; g0 < j1; g0 += kGramRows) {
+        const int rows = min(kGramRows, j1 - g0);
+        __syncthreads();
+        for (int idx = tid; idx < rows * m; idx += PT) {
+          const int jl = idx % rows, c = idx / rows;
+          const int j = g0 + jl;
+          const double vj = __ldcg(f.v + j) * inv_v;
+          if (c == 0) f.V[j + (long)a * p] = vj;
+          const double s = fma(-vj, sv[c] * inv_v, __ldcg(f.S + j + (long)c * p));
+          f.S[j + (long)c * p] = s;
+          ss[jl + c * kGramRows] = s;
+        }
+        __syncthreads();
+        for (int k = warp; k < G; k += PT / 32) {
+          int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+          while (c * (c + 1) / 2 > k) --c;
+          while ((c + 1) * (c + 2) / 2 <= k) ++c;
+          const int d = k - c * (c + 1) / 2;
+          double s = 0.0;
+          for (int jl = lane; jl < rows; jl += 32)
+            s = fma(ss[jl + c * kGramRows], ss[jl + d * kGramRows], s);
+          s = warp_sum(s);
+          if (lane == 0) gacc[k] += s;
+        }
+      }
+      __syncthreads();
+      for (int k = tid; k < G; k += PT) f.cpart[(long)cta * f.cslots + k] = gacc[k];
+      double* tcol = f.T + (long)a * n;
+      for (int i = cta * PT + tid; i < n; i += C * PT) tcol[i] = __ldcg(tcol + i) * inv_t;
+    }
+  }
+}
+
+int round_up(long v, long m) { return (int)((v + m - 1) / m * m); }
+
+}  // namespace
+
+int& persistent_enabled() {
+  static int on = 1;
+  return on;
+}
+
+bool persistent_supported(int m, int a) {
+  return m >= 1 && m <= kPersistMaxResponses && a >= 1 && a <= kPersistMaxComponents;
+}
+
+template <class T>
+bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, DeviceModel& model,
+                           double* S, double* gpk, Workspace& ws, cudaStream_t stream) {
+  if (!persistent_enabled() || !persistent_supported(m, a) || n < 2 || p < 1) return false;
+  static const int max_per_sm = [] {
+    int v = 0;
+    if (cudaFuncSetAttribute(persistent_simpls<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSmemDoubles * (int)sizeof(double)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, persistent_simpls<T>, PT,
+                                                      kSmemDoubles * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return v;
+  }();
+  int coop = 0, dev = 0;
+  FPLS_CHECK(cudaGetDevice(&dev));
+  FPLS_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  // CTAs of the fit: from (n, p) only (never from the storage type), at most
+  // two per SM
+  const int sms = num_sms();
+  const long elems = (long)n * p;
+  const int C = (int)std::max(1L, std::min<long>(2L * sms, (elems + (1L << 17) - 1) >> 17));
+  if (!coop || max_per_sm < 2 || C > max_per_sm * sms) return false;
+
+  Fit f{};
+  f.X = X;
+  f.ld = ld;
+  f.n = n;
+  f.p = p;
+  f.m = m;
+  f.a = a;
+  f.mean = model.mean.get();
+  f.scale = model.scale.get();
+  f.S0 = model.S0.get();
+  f.S = S;
+  f.R = model.R.get();
+  f.V = model.V.get();
+  f.Q = model.Q.get();
+  f.T = model.T.get();
+  f.gpk = gpk;
+  f.r = ws.vec_p[0].get();
+  f.rt = ws.vec_p[1].get();
+  f.pv = ws.vec_p[2].get();
+  f.v = ws.vec_p[3].get();
+  f.cta0 = 0;
+  f.C = C;
+  // t pass: chunks of columns so that (row tiles of 1024) x chunks gives
+  // about four items per CTA; loading pass: 32-column tiles x row chunks
+  const int target = 4 * C;
+  const long row_tiles = (n + 1023) / 1024;
+  f.cc = std::max(32, std::min(kMaxXrCols, round_up((p * row_tiles + target - 1) / target, 32)));
+  f.kt = (p + f.cc - 1) / f.cc;
+  const int jtiles = (p + 31) / 32;
+  int kp = std::max((target + jtiles - 1) / jtiles, (n + kMaxXtvRows - 1) / kMaxXtvRows);
+  kp = std::max(1, std::min(kp, (n + 63) / 64));
+  f.rc = std::min(kMaxXtvRows, round_up((n + kp - 1) / kp, 64));
+  f.kp = (n + f.rc - 1) / f.rc;
+  constexpr int VN = sizeof(T) == 2 ? 8 : (sizeof(T) == 4 ? 4 : 2);
+  const bool aligned16 = reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % VN == 0;
+  f.vec = aligned16 ? VN : 1;
+  f.pair = (reinterpret_cast<uintptr_t>(X) % (2 * sizeof(T)) == 0 && ld % 2 == 0) ? 1 : 0;
+  f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2));
+  // per-CTA column ranges must fit the shared staging of P5/P6 (2048 each)
+  if ((p + C - 1) / C > 2048) return false;
+
+  // scratch of this launch (stream-ordered, freed behind the kernel); the
+  // workspace's own scalar arrays hold the Gram of S and stay untouched
+  ws.stream_partial.reserve((size_t)f.kt * n + (size_t)f.kp * p, stream);
+  f.tpart = ws.stream_partial.get();
+  f.ppart = f.tpart + (size_t)f.kt * n;
+  DeviceArray<double> cpart((size_t)C * f.cslots, stream);
+  DeviceArray<double> scal((size_t)SC_H + kPersistMaxComponents + 8, stream);
+  DeviceArray<unsigned> bar(2, stream);
+  bar.zero(stream);
+  f.cpart = cpart.get();
+  f.scal = scal.get();
+  f.bar = bar.get();
+
+  DeviceArray<Fit> d_fit(1, stream);
+  FPLS_CHECK(cudaMemcpyAsync(d_fit.get(), &f, sizeof(Fit), cudaMemcpyHostToDevice, stream));
+  const Fit* fp = d_fit.get();
+  int nfits = 1;
+  int* flag = ws.flag.get();
+  void* args[] = {(void*)&fp, (void*)&nfits, (void*)&flag};
+  FPLS_CHECK(cudaLaunchCooperativeKernel((const void*)persistent_simpls<T>, dim3(C), dim3(PT), args,
+                                         kSmemDoubles * sizeof(double), stream));
+  count_launch();
+  FPLS_LAUNCH("persistent_simpls");
+  // the descriptor must outlive the launch: release it stream-ordered
+  d_fit.release();
+  model.a = a;
+  return true;
+}
+
+template bool fit_simpls_persistent<float>(const float*, int, int, long, int, int, DeviceModel&,
+                                           double*, double*, Workspace&, cudaStream_t);
+template bool fit_simpls_persistent<double>(const double*, int, int, long, int, int, DeviceModel&,
+                                            double*, double*, Workspace&, cudaStream_t);
+template bool fit_simpls_persistent<bf16>(const bf16*, int, int, long, int, int, DeviceModel&,
+                                          double*, double*, Workspace&, cudaStream_t);
+
+}  // namespace fpls

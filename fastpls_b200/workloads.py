@@ -96,3 +96,68 @@ def config_cv_permutation(n=5000, p=10000, dtype=np.float32):
     x, y = latent_regression(n, p, 3, 10, 0.3, 3, dtype=dtype)
     folds = uneven_folds(n, 10, 3)
     return x, y, folds
+
+
+# ---------------------------------------------------------------------------
+# Full-size configurations, drawn on the device (torch's CUDA Philox
+# generator, seeded) because the host generator is far slower at these sizes.
+# The same host arrays then feed the device fit and the FP64 reference.
+
+def mixed_precision_config(seed=4, n=100_000, p=20_000, m=10, k=50, noise=0.5):
+    """The mixed-precision SIMPLS configuration: X = T W^T diag(s) + noise
+    (n x p, column-centred, column scales s ~ logN(0, 1)), rounded to BF16;
+    Y = T C + 0.1 noise (n x m). Returns (bits, y): bits the BF16 bit
+    patterns of X as an n x p Fortran-ordered uint16 array, y float32 n x m
+    Fortran-ordered."""
+    import torch
+
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev).manual_seed(seed)
+    t = torch.randn(n, k, generator=g, device=dev)
+    w = torch.randn(p, k, generator=g, device=dev)
+    scale = torch.exp(torch.randn(p, generator=g, device=dev))
+    c = torch.randn(k, m, generator=g, device=dev)
+    xt = (w * scale[:, None]) @ t.T            # p x n row-major = n x p column-major
+    xt += noise * torch.randn(p, n, generator=g, device=dev)
+    xt -= xt.mean(dim=1, keepdim=True)
+    xb = xt.to(torch.bfloat16)
+    del xt
+    y = (t @ c + 0.1 * torch.randn(n, m, generator=g, device=dev)).T.contiguous()
+    bits = xb.view(torch.int16).cpu().numpy().view(np.uint16).T
+    yh = y.cpu().numpy().T
+    del xb, t, w, y, c
+    torch.cuda.empty_cache()
+    return bits, yh
+
+
+def bf16_to_f64(bits, rows=None):
+    """FP64 values of BF16 bit patterns (exact), optionally of some rows."""
+    b = bits if rows is None else bits[rows]
+    out = np.empty(b.shape, dtype=np.float64, order="F")
+    step = 4096
+    for j0 in range(0, b.shape[1], step):
+        blk = np.ascontiguousarray(b[:, j0:j0 + step]).astype(np.uint32) << 16
+        out[:, j0:j0 + step] = blk.view(np.float32)
+    return out
+
+
+def plssvd_lda_config(seed=2, n=20_000, p=50_000, k=20, classes=10):
+    """The PLS-SVD + LDA configuration: X = T W^T + N(0, 0.1^2) (n x p FP32,
+    column-centred) with factor scales 100 * 0.8^i; labels = argmax(T C) + 1
+    with C ~ N(0, 1) k x classes. Returns (x, labels), x Fortran-ordered."""
+    import torch
+
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev).manual_seed(seed)
+    sigma = 100.0 * 0.8 ** torch.arange(k, device=dev, dtype=torch.float32)
+    t = torch.randn(n, k, generator=g, device=dev) * sigma
+    w = torch.randn(p, k, generator=g, device=dev)
+    c = torch.randn(k, classes, generator=g, device=dev)
+    xt = w @ t.T
+    xt += 0.1 * torch.randn(p, n, generator=g, device=dev)
+    xt -= xt.mean(dim=1, keepdim=True)
+    lab = (torch.argmax(t @ c, dim=1) + 1).to(torch.int32).cpu().numpy()
+    x = xt.cpu().numpy().T
+    del xt, t, w, c
+    torch.cuda.empty_cache()
+    return x, lab

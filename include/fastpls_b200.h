@@ -224,6 +224,51 @@ FASTPLS_B200_API int fastpls_b200_product_digits(void);
 FASTPLS_B200_API void fastpls_b200_set_batch_lanes(int lanes);
 FASTPLS_B200_API int fastpls_b200_batch_lanes(void);
 
+/* Argmax guard of the batched classification engine (no reference
+ * counterpart). With int8 digit products, a held-out row whose top two class
+ * scores differ by no more than `margin` times their magnitude marks its
+ * (fold, permutation) instance, and every marked instance is refitted with
+ * FP64 products, so predicted labels equal those of the FP64 path (the
+ * reference's argmax, first index on ties:
+ * inst/include/fastpls/core/classification.hpp:401-425). Default 1e-5;
+ * 0 disables the guard. Process-wide. fastpls_b200_guard_refits returns the
+ * number of instances the last batched classification call refitted. */
+FASTPLS_B200_API void fastpls_b200_set_argmax_guard(double margin);
+/* Group schedule of the batched engine (no reference counterpart). Every
+ * buffer of a group lives in a per-device workspace kept between calls, and
+ * a group's whole component sequence (all lanes, all components) is captured
+ * once as a CUDA graph and replayed by later calls of the same shape. With
+ * autotuning on (default), the first group of a new (n, p, q, instances,
+ * components, digits) key times every schedule -- lanes 1..4 x tile width
+ * 192 / 256, which give bit-identical results -- and keeps the fastest; the
+ * decisions persist in the file named by the FASTPLS_B200_TUNE_FILE
+ * environment variable when it is set. 0 selects the fixed rule
+ * (fastpls_b200_set_batch_lanes lanes, width from the wave count).
+ * fastpls_b200_batched_stats reports the last call: groups run, groups run by
+ * graph replay, graphs captured, groups tuned, and the last schedule.
+ * fastpls_b200_release_workspace frees the workspaces (the next call
+ * rebuilds them). Process-wide. */
+/* Device time of the calling thread's last resident fit (any of the four
+ * _create functions), from CUDA events on the handle's stream: the copies of
+ * the inputs to the device, and the fit proper (no reference counterpart;
+ * benchmark instrumentation). Milliseconds. */
+FASTPLS_B200_API void fastpls_b200_last_fit_times(double* copy_ms, double* fit_ms);
+/* Single-fit SIMPLS component loop (no reference counterpart): 1 (default)
+ * runs every component of a fit in one cooperative persistent launch where
+ * it applies (one direction per component, 1..32 responses, 1..256
+ * components); 0 runs the per-kernel loop. Results agree to rounding.
+ * Process-wide. */
+FASTPLS_B200_API void fastpls_b200_set_persistent(int enable);
+FASTPLS_B200_API int fastpls_b200_persistent(void);
+FASTPLS_B200_API void fastpls_b200_set_autotune(int enable);
+FASTPLS_B200_API int fastpls_b200_autotune(void);
+FASTPLS_B200_API void fastpls_b200_batched_stats(int* groups, int* graph_replays,
+                                                 int* graph_captures, int* tuned, int* lanes,
+                                                 int* tile_n);
+FASTPLS_B200_API void fastpls_b200_release_workspace(void);
+FASTPLS_B200_API double fastpls_b200_argmax_guard(void);
+FASTPLS_B200_API int fastpls_b200_guard_refits(void);
+
 /* Benchmark instrumentation of the int8 split products, as for
  * fastpls_b200_profile_gemm; the operation count is the int8 multiply-adds
  * issued (2 M N k per digit pair, M (M + 1) k for a symmetric product). */

@@ -142,11 +142,53 @@ def test_batched_classification_permutations(digits, scaling):
     for b in range(4):
         lb = lab if b == 0 else lab[perms[b - 1]]
         want = O.cv_classification(x64, lb, classes, folds, pre, scaling=scaling)["metrics"]
-        if digits == 0:
-            assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
-        else:   # int8 products: at most one borderline row may flip
-            assert np.all(np.abs(got["accuracy"][b] - want) <= 1.0 / n + 1e-12)
+        # labels are bit-exact with int8 products too: the argmax guard
+        # refits instances with near-tied held-out scores in FP64
+        assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
     assert list(got["status"]) == [1] * 5
+
+
+@pytest.mark.parametrize("scaling", [1, 2])
+def test_argmax_guard_refits_every_marked_instance(scaling):
+    """A margin of 1e30 marks every instance with two or more active classes, so
+    the whole run is refitted with FP64 products: the accuracies must then be
+    identical to the FP64-product run, and the refit count must be every
+    instance."""
+    n, p, classes = 240, 120, 3
+    x, lab = W.latent_classification(n, p, classes, 3, 0.5, 43, dtype=np.float64)
+    folds = W.uneven_folds(n, 4, 43)
+    perms = W.permutations(n, 5, 43)
+    pre = [1, 2, 5]
+    fp64 = api.cv_permutation_classification(x, lab, classes, folds, perms, pre,
+                                             scaling=scaling, digits=0)
+    assert api.guard_refits() == 0
+    old = api.argmax_guard()
+    api.set_argmax_guard(1e30)
+    try:
+        got = api.cv_permutation_classification(x, lab, classes, folds, perms, pre,
+                                                scaling=scaling, digits=6)
+        refits = api.guard_refits()
+    finally:
+        api.set_argmax_guard(old)
+    assert refits == 6 * 4
+    assert np.array_equal(got["accuracy"], fp64["accuracy"])
+
+
+def test_batched_classification_ten_classes_bit_exact():
+    """The PLS-SVD + LDA configuration's label shape (10 classes from the
+    argmax of latent scores) at a reduced size, 6-digit products: held-out
+    accuracies equal the FP64 oracle's for every permutation and prefix."""
+    n, p, classes = 600, 400, 10
+    x, lab = W.latent_classification(n, p, classes, 20, 0.1, 2, dtype=np.float32)
+    folds = W.uneven_folds(n, 5, 2)
+    perms = W.permutations(n, 4, 2)
+    pre = [1, 3, 6, 9]
+    got = api.cv_permutation_classification(x, lab, classes, folds, perms, pre, digits=6)
+    x64 = x.astype(np.float64)
+    for b in range(5):
+        lb = lab if b == 0 else lab[perms[b - 1]]
+        want = O.cv_classification(x64, lb, classes, folds, pre)["metrics"]
+        assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
 
 
 def test_batched_classification_rejects_single_class_folds():
@@ -157,3 +199,45 @@ def test_batched_classification_rejects_single_class_folds():
     lab[folds == 1] = 2          # class 2 only in fold 1: its training rows hold one class
     with pytest.raises(api._lib.FastplsError, match="two classes"):
         api.cv_permutation_classification(x, lab, 2, folds, None, [1, 2])
+
+
+def test_batched_graph_replay_and_schedules_bit_identical():
+    """The second call of a shape replays the group's captured CUDA graph
+    (no new capture); the tuned schedule, every fixed lane count and the
+    FP64-free default give bit-identical results, since the candidate tile
+    widths (192, 256) combine the digit diagonals in one FP64 order and
+    lanes only partition the instances."""
+    n, p = 300, 160
+    x, y = W.latent_regression(n, p, 3, 4, 0.3, 61, dtype=np.float32)
+    folds = W.uneven_folds(n, 5, 61)
+    perms = W.permutations(n, 99, 61)      # 500 instances: up to 4 lanes of 125
+    pre = [1, 2, 4, 7]
+    api.release_workspace()
+    first = api.cv_permutation(x, y, folds, perms, pre, precision=32, digits=6)
+    s1 = api.batched_stats()
+    assert s1["groups"] == 1 and s1["graph_captures"] >= 1
+    second = api.cv_permutation(x, y, folds, perms, pre, precision=32, digits=6)
+    s2 = api.batched_stats()
+    assert s2["graph_replays"] == 1 and s2["graph_captures"] == 0 and s2["tuned"] == 0
+    for key in ("q2", "rmsd", "observed_r2"):
+        assert np.array_equal(first[key], second[key]), key
+    old_tune, old_lanes = api.autotune(), api.batch_lanes()
+    try:
+        api.set_autotune(False)
+        for lanes in (1, 2, 3, 4):
+            api.set_batch_lanes(lanes)
+            got = api.cv_permutation(x, y, folds, perms, pre, precision=32, digits=6)
+            assert api.batched_stats()["lanes"] == lanes
+            for key in ("q2", "rmsd", "observed_r2"):
+                assert np.array_equal(first[key], got[key]), (lanes, key)
+    finally:
+        api.set_autotune(old_tune)
+        api.set_batch_lanes(old_lanes)
+    # new inputs of the same shape replay the same graph and match the oracle
+    x2, y2 = W.latent_regression(n, p, 3, 4, 0.3, 62, dtype=np.float32)
+    got = api.cv_permutation(x2, y2, folds, perms, pre, precision=32, digits=6)
+    assert api.batched_stats()["graph_captures"] == 0
+    for b in (0, 50, 99):
+        yb = y2 if b == 0 else y2[perms[b - 1]]
+        ref = O.cv_regression(x2.astype(np.float64), yb.astype(np.float64), folds, pre)
+        assert np.allclose(got["q2"][b], ref["q2"], rtol=1e-5, atol=1e-7), b
