@@ -65,6 +65,9 @@ def args_parse():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the single-fit configuration legs (plain FP64 "
                          "SIMPLS, full-size PLS-SVD + LDA, full-size BF16 SIMPLS)")
+    ap.add_argument("--served-spec-requests", type=int, default=40,
+                    help="requests in the served leg at the configuration's stated "
+                         "sizes (n, p up to 50000; 0 = skip)")
     ap.add_argument("--latency-steps", type=int, default=60,
                     help="untimed extra steps for the step-latency distribution")
     return ap.parse_args()
@@ -240,6 +243,70 @@ def served_workload(count, seed=11):
                  classes=m if cls else None, ncomp=a, p=p, q=m)
         reqs.append(r)
         fitted.append(r)
+    return reqs
+
+
+def served_spec_workload(count, seed=12):
+    """The served mixed workload at its stated sizes: n log-uniform in
+    [200, 50000], p log-uniform in [500, 50000], m uniform in 1..10, ncomp
+    uniform in [2, 30]; SIMPLS 50%, PLS-SVD 20%, OPLS 15%, kernel PLS (RBF,
+    n <= 5000) 15%; 30% classification (2-20 classes); 70% fits and 30%
+    predictions (100-2000 rows) against the models fitted so far. Inputs come
+    from the latent-factor generator seeded by request id, drawn on the
+    device (torch's Philox generator) and copied to host memory."""
+    import torch
+    dev = torch.device("cuda")
+    g = np.random.default_rng(seed)
+    reqs, fitted = [], []
+
+    def latent(n, p, k, rid):
+        gen = torch.Generator(device=dev).manual_seed(rid)
+        t = torch.randn(n, k, generator=gen, device=dev)
+        w = torch.randn(p, k, generator=gen, device=dev)
+        xt = w @ t.T + 0.4 * torch.randn(p, n, generator=gen, device=dev)
+        xt -= xt.mean(dim=1, keepdim=True)
+        x = xt.cpu().numpy().T          # n x p, Fortran order
+        return x, t, gen
+    for rid in range(count):
+        if fitted and g.random() < 0.3:
+            src = fitted[int(g.integers(len(fitted)))]
+            rows = int(g.integers(100, 2001))
+            x, _, _ = latent(rows, src["p"], 5, 900000 + rid)
+            reqs.append(dict(kind="predict", src=src, x=x))
+            continue
+        method = str(g.choice(["simpls", "plssvd", "opls", "kernelpls"], p=[0.5, 0.2, 0.15, 0.15]))
+        n = int(np.exp(g.uniform(np.log(200), np.log(50000))))
+        p = int(np.exp(g.uniform(np.log(500), np.log(50000))))
+        if method == "kernelpls":
+            n = min(n, 5000)
+        m = int(g.integers(1, 11))
+        cls = g.random() < 0.3
+        x, t, gen = latent(n, p, 5, rid)
+        if cls:
+            m = int(g.integers(2, 21))
+            c = torch.randn(5, m, generator=gen, device=t.device)
+            lab = (torch.argmax(t @ c, dim=1)).cpu().numpy()
+            present, lab = np.unique(lab, return_inverse=True)
+            lab = (lab + 1).astype(np.int32)
+            m = int(present.size)
+            if m < 2:
+                continue
+            y = None
+        else:
+            c = torch.randn(5, m, generator=gen, device=t.device)
+            y = (t @ c + 0.1 * torch.randn(n, m, generator=gen, device=t.device)).cpu().numpy()
+            y = np.asfortranarray(y)
+            lab = None
+        cap = min(n - 1, p) if method != "kernelpls" else n - 1
+        a = int(min(int(g.integers(2, 31)), cap))
+        if method == "plssvd":
+            a = max(1, min(a, m - 1 if cls else m))
+        r = dict(kind="fit", method=method, x=x, y=y, labels=lab,
+                 classes=m if cls else None, ncomp=a, p=p, q=m)
+        reqs.append(r)
+        fitted.append(r)
+    del t
+    torch.cuda.empty_cache()
     return reqs
 
 
@@ -820,6 +887,26 @@ def main():
                                 "queue behind their model's fit in the server",
             sweep=sweep, **plain,
             saturated_served_over_plain=sweep[-1]["fits_per_s"] / plain["plain_fits_per_s"])
+    if rank == 0 and a.served_spec_requests > 0:
+        from fastpls_b200 import api as fapi
+        reqs = served_spec_workload(a.served_spec_requests)
+        nbytes = sum(r["x"].nbytes for r in reqs)
+        plain_s = run_plain(fapi, reqs)
+        sweep_s = [run_served(fapi, reqs, mean_gap_ms=g_, workers=8) for g_ in (20.0, 0.0)]
+        fits_ = [r for r in reqs if r["kind"] == "fit"]
+        line["served_spec"] = dict(
+            requests=len(reqs), fits=len(fits_),
+            input_gb=nbytes / 1e9,
+            n_range=[int(min(r["x"].shape[0] for r in fits_)), int(max(r["x"].shape[0] for r in fits_))],
+            p_range=[int(min(r["p"] for r in fits_)), int(max(r["p"] for r in fits_))],
+            methods={m_: sum(1 for r in fits_ if r["method"] == m_)
+                     for m_ in ("simpls", "plssvd", "opls", "kernelpls")},
+            classification=sum(1 for r in fits_ if r["labels"] is not None),
+            budget_gb=150, workers=8,
+            arrivals="Poisson; mean gap 20 ms, then all at once",
+            sweep=sweep_s, **plain_s,
+            saturated_served_over_plain=sweep_s[-1]["fits_per_s"] / plain_s["plain_fits_per_s"])
+        del reqs
     if rank == 0 and world == 1 and not a.no_configs:
         from fastpls_b200 import api as fapi
         from oracle import ref as _ref

@@ -714,6 +714,12 @@ class Server:
         self._lib.fastpls_b200_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c))
         return dict(bytes_in_use=a.value, queued=b.value, resident_models=c.value)
 
+    def batch_stats(self):
+        """Persistent launches that carried batches of fits, and those fits."""
+        a, b = C.c_size_t(0), C.c_size_t(0)
+        self._lib.fastpls_b200_server_batch_stats(self._h, C.byref(a), C.byref(b))
+        return dict(launches=a.value, fits=b.value)
+
     def close(self):
         if self._h:
             self._lib.fastpls_b200_server_destroy(self._h)

@@ -73,7 +73,8 @@ void fit_method(int method, const T* X, int n, int p, const double* Yc,
                 DeviceModel& model, Workspace& ws, cudaStream_t s) {
   if (method == kPlssvd) fit_plssvd<T>(X, n, p, n, Yc, ycsum, m, a, scaling, model, ws, s);
   else fit_simpls<T>(X, n, p, n, Yc, ycsum, m, a, scaling, model, ws, s,
-                     simpls_block_size(n, p, m, a, model.classification, std::is_same<T, float>::value));
+                     simpls_block_size(n, p, m, a, model.classification, std::is_same<T, float>::value),
+                     simpls_gram_route(n, p, a, model.classification));
 }
 
 }  // namespace

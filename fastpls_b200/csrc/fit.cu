@@ -27,6 +27,7 @@
 #include "small.cuh"
 
 #include <algorithm>
+#include <memory>
 
 namespace fpls {
 
@@ -216,6 +217,7 @@ __device__ inline void block_dots(const double* __restrict__ M, long ldm,
 
 // p = (praw - mean * sum t) / (scale * ||t||) ; R[:,a] = r / ||t||
 // out (last block): h = V^T p (a_cur), q = S0^T R[:,a] (m)
+// When `loading` is given (cached-Gram route) p = loading / ||t|| directly.
 __global__ void tail1_kernel(const double* __restrict__ praw,
                              const double* __restrict__ mean,
                              const double* __restrict__ scale,
@@ -225,7 +227,7 @@ __global__ void tail1_kernel(const double* __restrict__ praw,
                              const double* __restrict__ V, int p, int m,
                              int a_cur, double* pvec, double* Rcol,
                              double* partial, unsigned* counter, double* hq,
-                             int* flag) {
+                             int* flag, const double* __restrict__ loading = nullptr) {
   extern __shared__ double sm[];
   double* ps = sm;            // TB
   double* rs = sm + TB;       // TB
@@ -240,7 +242,7 @@ __global__ void tail1_kernel(const double* __restrict__ praw,
   const int t = threadIdx.x;
   if (t < rows) {
     const int j = j0 + t;
-    const double pj = (praw[j] - mean[j] * scal[2]) / scale[j] * inv;
+    const double pj = loading ? loading[j] * inv : (praw[j] - mean[j] * scal[2]) / scale[j] * inv;
     const double rj = r[j] * inv;
     pvec[j] = pj;
     Rcol[j] = rj;
@@ -378,6 +380,35 @@ __global__ void fill_rows_mean(double* out, int rows, int m, long ldo,
   }
 }
 
+// Gs[j, k] = (G[j, k] - n mean_j mean_k) / (scale_j scale_k): the Gram of
+// the standardised predictors from the raw X^T X.
+__global__ void standardize_gram(double* G, int p, int n, const double* __restrict__ mean,
+                                 const double* __restrict__ scale) {
+  const long total = (long)p * p;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(idx % p), k = (int)(idx / p);
+    G[idx] = (G[idx] - (double)n * mean[j] * mean[k]) / (scale[j] * scale[k]);
+  }
+}
+
+// scal[1] = r . loading (= ||X_s r||^2), scal[2] = 0 (sum t unused on this route)
+__global__ void gram_tstats(const double* __restrict__ r, const double* __restrict__ loading,
+                            int p, double* partial, unsigned* counter, double* scal) {
+  __shared__ double scratch[32];
+  __shared__ double vals[2];
+  double a = 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p; j += gridDim.x * blockDim.x)
+    a = fma(r[j], loading[j], a);
+  a = block_sum(a, scratch);
+  if (threadIdx.x == 0) {
+    vals[0] = a;
+    vals[1] = 0.0;
+  }
+  __syncthreads();
+  last_block_reduce(vals, 2, partial, counter, scal + 1);
+}
+
 int tail3_block(int m) { return m <= 16 ? 256 : (m <= 32 ? 128 : 64); }
 
 }  // namespace
@@ -476,7 +507,8 @@ void gram_of_columns(double* S, int p, int m, double* gpk, Workspace& ws,
 template <class T>
 void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
-                DeviceModel& model, Workspace& ws, cudaStream_t stream, int block) {
+                DeviceModel& model, Workspace& ws, cudaStream_t stream, int block,
+                bool gram_route) {
   require(m >= 1 && m <= kMaxResponses, "SIMPLS supports 1..112 responses or classes");
   const int a_max = components;
   ws.ensure(n, p, m, a_max, stream);
@@ -518,9 +550,46 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
   gram_of_columns(S.get(), p, m, gpk, ws, stream);
 
+  // cached-Gram route (FP32 / FP64 storage): Gs = X_s^T X_s once
+  gram_route = gram_route && !std::is_same<T, bf16>::value;
+  DeviceArray<double> Gs, loading;
+  if (gram_route) {
+    Gs.allocate((size_t)p * p, stream);
+    loading.allocate(p, stream);
+    GemmArgs g;
+    g.M = p;
+    g.N = p;
+    g.K = n;
+    g.A = X;
+    g.lda = ld;
+    g.trans_a = true;
+    g.a_f32 = std::is_same<T, float>::value;
+    g.B = X;
+    g.ldb = ld;
+    g.b_f32 = std::is_same<T, float>::value;
+    g.C = Gs.get();
+    g.ldc = p;
+    gemm_f64(g, stream);
+    const long total = (long)p * p;
+    standardize_gram<<<(unsigned)std::min<long>((total + 255) / 256, 8L * num_sms()), 256, 0, stream>>>(
+        Gs.get(), p, n, model.mean.get(), model.scale.get());
+    count_launch();
+    FPLS_LAUNCH("standardize_gram");
+  }
+
   // one direction per component: the whole loop as one persistent launch
-  if (block <= 1 && fit_simpls_persistent<T>(X, n, p, ld, m, a_max, model, S.get(), gpk, ws, stream))
-    return;
+  // (or handed to the caller's batch when it collects plans)
+  if (block <= 1 && !gram_route) {
+    std::unique_ptr<PersistentPlan> plan(new PersistentPlan());
+    if (plan_simpls_persistent<T>(X, n, p, ld, m, a_max, model, S, gpk, ws, stream, *plan)) {
+      if (std::unique_ptr<PersistentPlan>* sink = persistent_deferral()) {
+        *sink = std::move(plan);
+      } else {
+        launch_persistent({plan.get()}, stream);
+      }
+      return;
+    }
+  }
 
   // Candidate blocks (the reference's block refresh): the directions of
   // `use` consecutive components are the leading left singular vectors of S
@@ -553,28 +622,45 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
     count_launch();
     FPLS_LAUNCH("rvec_kernel");
     double* tcol = model.T.get() + (size_t)a * n;
-    xr_product<T>(X, n, p, ld, rt, p, 1, scal, tcol, n, ws.stream_partial, stream);
-    tstats_kernel<<<std::min<unsigned>(ceil_div(n, TB), 2 * num_sms()), TB, 0, stream>>>(
-        tcol, n, part, ctr + 1, scal);
-    count_launch();
-    FPLS_LAUNCH("tstats");
-    xtv_product<T>(X, n, p, ld, tcol, n, 1, praw, p, ws.stream_partial, stream);
+    if (gram_route) {
+      // loading = Gs r (Gs symmetric: its columns dot r), ||t||^2 = r . loading
+      xtv_product<double>(Gs.get(), p, p, p, r, p, 1, loading.get(), p, ws.stream_partial, stream);
+      gram_tstats<<<std::min<unsigned>(ceil_div(p, TB), 2 * num_sms()), TB, 0, stream>>>(
+          r, loading.get(), p, part, ctr + 1, scal);
+      count_launch();
+      FPLS_LAUNCH("gram_tstats");
+    } else {
+      xr_product<T>(X, n, p, ld, rt, p, 1, scal, tcol, n, ws.stream_partial, stream);
+      tstats_kernel<<<std::min<unsigned>(ceil_div(n, TB), 2 * num_sms()), TB, 0, stream>>>(
+          tcol, n, part, ctr + 1, scal);
+      count_launch();
+      FPLS_LAUNCH("tstats");
+      xtv_product<T>(X, n, p, ld, tcol, n, 1, praw, p, ws.stream_partial, stream);
+    }
     tail1_kernel<<<g1, TB, (2 * TB + a + m) * sizeof(double), stream>>>(
         praw, model.mean.get(), model.scale.get(), scal, r, model.S0.get(),
         model.V.get(), p, m, a, pvec, model.R.get() + (size_t)a * p, part,
-        ctr + 2, hq, ws.flag.get());
+        ctr + 2, hq, ws.flag.get(), gram_route ? loading.get() : nullptr);
     tail2_kernel<<<g1, TB, (TB + 1 + m) * sizeof(double), stream>>>(
         pvec, model.V.get(), hq, S.get(), p, m, a, v, part, ctr + 3, vr);
     tail3_kernel<<<g3, jb3, smem3, stream>>>(v, vr, S.get(), p, m,
                                              model.V.get() + (size_t)a * p,
                                              true, part, ctr + 4, gpk,
                                              ws.flag.get());
-    finish_component<<<std::min<unsigned>(ceil_div(n, TB), 2 * num_sms()), TB, 0, stream>>>(
-        tcol, n, scal, hq, a, m, model.Q.get() + (size_t)a * m);
+    if (!gram_route)
+      finish_component<<<std::min<unsigned>(ceil_div(n, TB), 2 * num_sms()), TB, 0, stream>>>(
+          tcol, n, scal, hq, a, m, model.Q.get() + (size_t)a * m);
+    else
+      finish_component<<<1, TB, 0, stream>>>(tcol, 0, scal, hq, a, m,
+                                             model.Q.get() + (size_t)a * m);
     count_launch(4);
     FPLS_LAUNCH("simpls component");
   }
   model.a = a_max;
+  if (gram_route) {
+    // training scores T = X_s R (normalised: R holds r / ||t||), one pass
+    project_rows<T>(model, X, n, ld, a_max, model.T.get(), n, ws, stream);
+  }
 }
 
 template <class T>
@@ -631,7 +717,7 @@ template void prepare_responses<double>(const double*, const int*, int, int, dou
 #define FPLS_INSTANTIATE(T)                                                    \
   template void fit_simpls<T>(const T*, int, int, long, const double*,        \
                               const double*, int, int, int, DeviceModel&,     \
-                              Workspace&, cudaStream_t, int);                 \
+                              Workspace&, cudaStream_t, int, bool);           \
   template void project_rows<T>(const DeviceModel&, const T*, int, long, int, \
                                 double*, long, Workspace&, cudaStream_t);   \
   template void compute_crossprod<T>(const T*, int, int, long, const double*, \

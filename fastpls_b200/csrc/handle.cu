@@ -3,6 +3,7 @@
 // reference (validation order, error strings, field sizes, synchronous
 // calls on a per-handle non-blocking stream).
 #include "handle.cuh"
+#include "persistent.cuh"
 #include "lda.cuh"
 #include "reduce.cuh"
 
@@ -243,10 +244,23 @@ class TypedHandle final : public ResidentHandle {
   using TO = typename io_type<T>::type;
 
  public:
-  explicit TypedHandle(const FitRequest& rq) : rq_(rq) {
+  // defer: a SIMPLS fit that plans a persistent launch leaves it pending
+  // (pending_plan()); the caller launches the plans of several handles
+  // together, orders this handle's stream after that launch and calls
+  // complete_fit().
+  explicit TypedHandle(const FitRequest& rq, bool defer = false) : rq_(rq) {
     try {
       FPLS_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-      fit();
+      if (defer && rq_.method == kSimpls) {
+        struct Sink {
+          explicit Sink(std::unique_ptr<PersistentPlan>* s) { persistent_deferral() = s; }
+          ~Sink() { persistent_deferral() = nullptr; }
+        } sink(&pending_);
+        fit_begin();
+      } else {
+        fit_begin();
+      }
+      if (!pending_) fit_end();
     } catch (...) {
       release();
       throw;
@@ -262,6 +276,14 @@ class TypedHandle final : public ResidentHandle {
     }
   }
   ~TypedHandle() override { release(); }
+
+  PersistentPlan* pending_plan() override { return pending_.get(); }
+  cudaStream_t stream() const override { return stream_; }
+  void complete_fit() override {
+    if (!pending_) return;
+    fit_end();
+    pending_.reset();
+  }
 
   void predict_path(const void* x, int rows, const int* prefixes, int count,
                     bool lda, void* out) override {
@@ -407,12 +429,15 @@ class TypedHandle final : public ResidentHandle {
                 int* implicit_operator, int* crossprod_cache) override {
     if (!oversample || !power || !block || !block_limit || !implicit_operator || !crossprod_cache)
       throw std::invalid_argument("null resident control output");
+    // the requested sketch controls (directions are exact here), the
+    // candidate block and the cached-Gram route this fit took; the
+    // cross-covariance is always explicit (no implicit operator)
     *oversample = rq_.oversample;
     *power = rq_.power;
-    *block = 1;
+    *block = used_block_;
     *block_limit = 0;
     *implicit_operator = 0;
-    *crossprod_cache = 0;
+    *crossprod_cache = used_gram_ ? 1 : 0;
   }
 
   void compact(bool prepare_lda) override {
@@ -430,7 +455,7 @@ class TypedHandle final : public ResidentHandle {
   }
 
  private:
-  void fit() {
+  void fit_begin() {
     const int n = rq_.n, p = rq_.p, q = rq_.q, a = rq_.components;
     const bool cls = rq_.labels != nullptr;
     if (!rq_.x) throw std::invalid_argument("invalid resident matrix or precision");
@@ -445,7 +470,8 @@ class TypedHandle final : public ResidentHandle {
       throw std::invalid_argument(rq_.method == kPlssvd ? "invalid resident PLS-SVD dimensions"
                                                         : "invalid resident SIMPLS dimensions");
     if (cls && q < 2) throw std::invalid_argument("classification requires at least two classes");
-    FitTimer timer(stream_);
+    timer_.reset(new FitTimer(stream_));
+    FitTimer& timer = *timer_;
     xtrain_.allocate((size_t)n * p, stream_);
     FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
     DeviceArray<TO> y;
@@ -477,14 +503,23 @@ class TypedHandle final : public ResidentHandle {
       fit_kernelpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, rq_.kernel,
                        rq_.gamma, rq_.degree, rq_.coef0, model_, ws_, design_, stream_);
     else
+    {
+      used_block_ = simpls_block_size(n, p, q, a, cls, std::is_same<T, float>::value);
+      used_gram_ = simpls_gram_route(n, p, a, cls) && !std::is_same<T, bf16>::value;
       fit_simpls<T>(xtrain_.get(), n, p, n, yc.get(), ycsum.get(), q, a, rq_.scaling, model_, ws_, stream_,
-                    simpls_block_size(n, p, q, a, cls, std::is_same<T, float>::value));
-    timer.mark();
+                    used_block_, used_gram_);
+    }
+  }
+
+  // after the fit's kernels (or its pending persistent launch) are enqueued
+  void fit_end() {
+    timer_->mark();
     raise_on_flag(ws_, stream_, rq_.method == kPlssvd
         ? "resident PLS-SVD failed: invalid labels, decomposition or score Gram"
         : rq_.method == kOpls ? "resident CUDA OPLS filtering failed"
         : "resident SIMPLS failed: invalid labels, decomposition or component norm");
-    timer.finish();
+    timer_->finish();
+    timer_.reset();
   }
 
   void load(const ImportRequest& im) {
@@ -641,6 +676,8 @@ class TypedHandle final : public ResidentHandle {
 
   void release() noexcept {
     if (stream_) cudaStreamSynchronize(stream_);
+    pending_.reset();
+    timer_.reset();
     lda_.reset();
     model_ = DeviceModel();
     ws_ = Workspace();
@@ -670,6 +707,10 @@ class TypedHandle final : public ResidentHandle {
   DeviceArray<double> scores_, pred_, disc_, loadings_, var_ss_, design_;
   DeviceArray<int> top_;
   std::unique_ptr<LdaState> lda_;
+  std::unique_ptr<PersistentPlan> pending_;
+  std::unique_ptr<FitTimer> timer_;
+  int used_block_ = 1;
+  bool used_gram_ = false;
 };
 
 ResidentHandle* import_handle(int precision, const ImportRequest& im) {
@@ -685,10 +726,10 @@ void read_last_fit_times(double* copy_ms, double* fit_ms) {
   if (fit_ms) *fit_ms = t.fit_ms;
 }
 
-ResidentHandle* make_handle(int precision, const FitRequest& rq) {
-  if (precision == 32) return new TypedHandle<float>(rq);
-  if (precision == 64) return new TypedHandle<double>(rq);
-  if (precision == 16) return new TypedHandle<bf16>(rq);
+ResidentHandle* make_handle(int precision, const FitRequest& rq, bool defer) {
+  if (precision == 32) return new TypedHandle<float>(rq, defer);
+  if (precision == 64) return new TypedHandle<double>(rq, defer);
+  if (precision == 16) return new TypedHandle<bf16>(rq, defer);
   throw std::invalid_argument("invalid resident matrix or precision");
 }
 

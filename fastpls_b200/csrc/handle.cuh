@@ -14,7 +14,8 @@
 
 namespace fpls {
 
-struct LdaState;  // lda.cu
+struct LdaState;        // lda.cu
+struct PersistentPlan;  // persistent.cuh
 
 class ResidentHandle {
  public:
@@ -33,6 +34,12 @@ class ResidentHandle {
                         int* crossprod_cache) = 0;
   virtual void compact(bool prepare_lda) = 0;
   virtual void vip(double* out, std::size_t size) = 0;
+  // A fit made with make_handle(..., defer = true) may leave its persistent
+  // launch pending: the plan to launch (with others), the handle's stream
+  // (to order after that launch), and the step that finishes the fit.
+  virtual PersistentPlan* pending_plan() { return nullptr; }
+  virtual cudaStream_t stream() const { return nullptr; }
+  virtual void complete_fit() {}
 };
 
 struct FitRequest {
@@ -48,7 +55,7 @@ struct FitRequest {
   double gamma = 0.0, coef0 = 1.0;
 };
 
-ResidentHandle* make_handle(int precision, const FitRequest& request);
+ResidentHandle* make_handle(int precision, const FitRequest& request, bool defer = false);
 
 // A fitted SIMPLS or OPLS model rebuilt from its exported fields (R, Q, the
 // predictor means and scales, the response means; optionally the training

@@ -58,11 +58,23 @@ void prepare_responses(const T* Y, const int* labels, int n, int m,
 
 // SIMPLS fit on raw X (n x p, ld) with centred responses Yc (n x m).
 // Fills model.{mean, scale, ymean (caller), R, Q, V, T, S0, a}.
+// gram_route: loadings from the cached p x p Gram of the standardised
+// predictors instead of two passes over X per component (simpls_gram_route).
 template <class T>
 void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
                 const double* ycsum, int m, int components, int scaling,
                 DeviceModel& model, Workspace& ws, cudaStream_t stream,
-                int block = 1);
+                int block = 1, bool gram_route = false);
+
+// The reference's cached predictor cross-product route
+// (src/cuda_resident_simpls.cuh:135, step_crossprod in
+// src/cuda_resident_component.cuh:131-167): classification fits with at
+// least 8 components and n >= 8 p form X_s^T X_s once and take each
+// component's loadings from it; the scores are X_s R at the end. FP32 and
+// FP64 storage.
+inline bool simpls_gram_route(int n, int p, int components, bool classification) {
+  return classification && components >= 8 && (long)n >= 8L * p;
+}
 
 // Candidate block size of a SIMPLS fit (src/cuda_resident_simpls.cuh:144-153):
 // a classification fit with q <= 2048 classes, at least 4 components and

@@ -28,12 +28,25 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace fpls {
 
 int& ozaki_slices() {
   static int slices = 6;
   return slices;
+}
+
+// MMA issue order of the int8 product within a stage: 1 = digit-major
+// (consecutive MMAs alternate between the diagonals' accumulators), 0 =
+// diagonal-major. Bit-identical results either way; the environment
+// variable FASTPLS_B200_INT8_ORDER (0 or 1) overrides the default.
+int ozaki_mma_order() {
+  static const int order = [] {
+    const char* e = std::getenv("FASTPLS_B200_INT8_ORDER");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return order;
 }
 
 namespace {
@@ -71,6 +84,7 @@ struct OzArgs {
   int kb0, kblocks;  // k-block range of this launch
   int rows_pa, rows_pb;  // padded rows of the digit layouts of A and B
   int slices, stages, lower, accumulate;
+  int interleave;    // MMA order within a stage (1: digit-major across diagonals)
   long ldc;
   double* C;
   const double* scale_a;
@@ -340,14 +354,28 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
           tc_fence_after();
           const uint32_t a0 = smem_u32(smem + st * stage_bytes);
           const uint32_t b0 = a0 + S * OZ_A_PLANE;
-          for (int q = 0; q < nk; ++q)
-            for (int d = dlo; d <= dhi; ++d)
-              for (int s = 0; s <= d; ++s) {
-                const uint64_t ad = core_desc(a0 + (q * ns + s) * OZ_A_PLANE);
-                const uint64_t bd = core_desc(b0 + (q * ns + d - s) * Shape::B_PLANE);
-                const uint32_t acc = (kb + q > 0 || s > 0) ? 1u : 0u;
-                tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
-              }
+          for (int q = 0; q < nk; ++q) {
+            if (args.interleave) {
+              // digit s outer, diagonal inner: consecutive MMAs write
+              // different accumulators (the int32 sums are exact, so the
+              // order does not change any result)
+              for (int s = 0; s <= dhi; ++s)
+                for (int d = max(dlo, s); d <= dhi; ++d) {
+                  const uint64_t ad = core_desc(a0 + (q * ns + s) * OZ_A_PLANE);
+                  const uint64_t bd = core_desc(b0 + (q * ns + d - s) * Shape::B_PLANE);
+                  const uint32_t acc = (kb + q > 0 || s > 0) ? 1u : 0u;
+                  tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
+                }
+            } else {
+              for (int d = dlo; d <= dhi; ++d)
+                for (int s = 0; s <= d; ++s) {
+                  const uint64_t ad = core_desc(a0 + (q * ns + s) * OZ_A_PLANE);
+                  const uint64_t bd = core_desc(b0 + (q * ns + d - s) * Shape::B_PLANE);
+                  const uint32_t acc = (kb + q > 0 || s > 0) ? 1u : 0u;
+                  tc_mma_i8(tmem + (uint32_t)((d - dlo) * BN), ad, bd, Shape::IDESC, acc);
+                }
+            }
+          }
           tc_commit(&empty_bar[st]);
           ++it;
         }
@@ -1115,6 +1143,7 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   args.flag = flag;
   args.rows_pa = a.rows_p;
   args.rows_pb = b.rows_p;
+  args.interleave = ozaki_mma_order();
   const int tiles_n = ceil_div(b.rows, bn);
   args.tiles_n = tiles_n;
   if (tc.pair) {

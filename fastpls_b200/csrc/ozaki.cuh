@@ -73,6 +73,7 @@ int ozaki_wide_tile(int a_rows, int b_rows);
 // Digit count used by the batched CV engine for its products with the
 // shared Gram (0 selects the FP64 DMMA path). Process-wide setting.
 int& ozaki_slices();
+int ozaki_mma_order();
 
 // Timing of the last ozaki_gemm launches (CUDA events), for benchmarks.
 void ozaki_profile_enable(bool on);

@@ -37,6 +37,7 @@
 #include "small.cuh"
 
 #include <algorithm>
+#include <memory>
 #include <vector>
 
 namespace fpls {
@@ -60,28 +61,7 @@ constexpr int SC_Q = 40;           // q (m)
 constexpr int SC_SV = 72;          // S^T v (m)
 constexpr int SC_H = 104;          // V^T p (a)
 
-struct Fit {
-  const void* X;
-  long ld;
-  int n, p, m, a;
-  const double* mean;
-  const double* scale;
-  const double* S0;
-  double *S, *R, *V, *Q, *T;
-  double* gpk;     // packed Gram of S (m (m + 1) / 2)
-  double *r, *rt, *pv, *v;  // p
-  double* tpart;   // kt x n
-  double* ppart;   // kp x p
-  double* cpart;   // C x cslots
-  double* scal;    // scalar slots
-  unsigned* bar;   // [count, generation]
-  int cta0, C;     // CTA range of this fit
-  int cc, kt;      // t pass: columns per chunk, chunks
-  int rc, kp;      // loading pass: rows per chunk, chunks
-  int vec;         // rows per 16-byte load in the t pass (1: scalar)
-  int pair;        // row pairs per lane in the loading pass
-  int cslots;      // per-CTA partial slots
-};
+using Fit = PersistentFit;
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -332,7 +312,7 @@ __device__ void direction_step(const Fit& f, double* sm, int* flag) {
 
 template <class T>
 __global__ void __launch_bounds__(PT, 2)
-    persistent_simpls(const Fit* __restrict__ fits, int nfits, int* flag) {
+    persistent_simpls(const Fit* __restrict__ fits, int nfits) {
   extern __shared__ double psm[];
   __shared__ double red[32];
   __shared__ double zs[kPersistMaxResponses];
@@ -342,6 +322,7 @@ __global__ void __launch_bounds__(PT, 2)
   int fi = 0;
   while (fi + 1 < nfits && (int)blockIdx.x >= fits[fi + 1].cta0) ++fi;
   const Fit f = fits[fi];
+  int* const flag = f.flag;
   const int cta = (int)blockIdx.x - f.cta0;
   const T* X = static_cast<const T*>(f.X);
   const int n = f.n, p = f.p, m = f.m, C = f.C;
@@ -569,32 +550,56 @@ bool persistent_supported(int m, int a) {
   return m >= 1 && m <= kPersistMaxResponses && a >= 1 && a <= kPersistMaxComponents;
 }
 
+std::unique_ptr<PersistentPlan>*& persistent_deferral() {
+  thread_local std::unique_ptr<PersistentPlan>* sink = nullptr;
+  return sink;
+}
+
+int persistent_ctas(int n, int p) {
+  // from (n, p) only, never from the storage type: at most two per SM
+  const long elems = (long)n * p;
+  return (int)std::max(1L, std::min<long>(2L * num_sms(), (elems + (1L << 17) - 1) >> 17));
+}
+
+namespace {
+
 template <class T>
-bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, DeviceModel& model,
-                           double* S, double* gpk, Workspace& ws, cudaStream_t stream) {
-  if (!persistent_enabled() || !persistent_supported(m, a) || n < 2 || p < 1) return false;
-  static const int max_per_sm = [] {
-    int v = 0;
-    if (cudaFuncSetAttribute(persistent_simpls<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+int capacity_of() {
+  static const int cap = [] {
+    int v = 0, coop = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+        cudaFuncSetAttribute(persistent_simpls<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSmemDoubles * (int)sizeof(double)) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, persistent_simpls<T>, PT,
                                                       kSmemDoubles * sizeof(double)) != cudaSuccess) {
       cudaGetLastError();
       return 0;
     }
-    return v;
+    return v >= 2 ? v * num_sms() : 0;
   }();
-  int coop = 0, dev = 0;
-  FPLS_CHECK(cudaGetDevice(&dev));
-  FPLS_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  // CTAs of the fit: from (n, p) only (never from the storage type), at most
-  // two per SM
-  const int sms = num_sms();
-  const long elems = (long)n * p;
-  const int C = (int)std::max(1L, std::min<long>(2L * sms, (elems + (1L << 17) - 1) >> 17));
-  if (!coop || max_per_sm < 2 || C > max_per_sm * sms) return false;
+  return cap;
+}
 
-  Fit f{};
+}  // namespace
+
+int persistent_capacity(int elem) {
+  return elem == 2 ? capacity_of<bf16>() : elem == 4 ? capacity_of<float>() : capacity_of<double>();
+}
+
+template <class T>
+bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, DeviceModel& model,
+                            DeviceArray<double>& S, double* gpk, Workspace& ws, cudaStream_t stream,
+                            PersistentPlan& plan) {
+  if (!persistent_enabled() || !persistent_supported(m, a) || n < 2 || p < 1) return false;
+  const int C = persistent_ctas(n, p);
+  const int cap = capacity_of<T>();
+  if (cap == 0 || C > cap) return false;
+  // per-CTA column ranges must fit the shared staging of P5/P6 (2048 each)
+  if ((p + C - 1) / C > 2048) return false;
+
+  Fit& f = plan.fit;
+  f = Fit{};
   f.X = X;
   f.ld = ld;
   f.n = n;
@@ -604,7 +609,6 @@ bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Devi
   f.mean = model.mean.get();
   f.scale = model.scale.get();
   f.S0 = model.S0.get();
-  f.S = S;
   f.R = model.R.get();
   f.V = model.V.get();
   f.Q = model.Q.get();
@@ -614,7 +618,7 @@ bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Devi
   f.rt = ws.vec_p[1].get();
   f.pv = ws.vec_p[2].get();
   f.v = ws.vec_p[3].get();
-  f.cta0 = 0;
+  f.flag = ws.flag.get();
   f.C = C;
   // t pass: chunks of columns so that (row tiles of 1024) x chunks gives
   // about four items per CTA; loading pass: 32-column tiles x row chunks
@@ -632,43 +636,63 @@ bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Devi
   f.vec = aligned16 ? VN : 1;
   f.pair = (reinterpret_cast<uintptr_t>(X) % (2 * sizeof(T)) == 0 && ld % 2 == 0) ? 1 : 0;
   f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2));
-  // per-CTA column ranges must fit the shared staging of P5/P6 (2048 each)
-  if ((p + C - 1) / C > 2048) return false;
 
-  // scratch of this launch (stream-ordered, freed behind the kernel); the
+  // scratch of this fit (stream-ordered, freed behind the launch); the
   // workspace's own scalar arrays hold the Gram of S and stay untouched
-  ws.stream_partial.reserve((size_t)f.kt * n + (size_t)f.kp * p, stream);
-  f.tpart = ws.stream_partial.get();
+  plan.elem = (int)sizeof(T);
+  plan.S = std::move(S);
+  f.S = plan.S.get();
+  plan.part.allocate((size_t)f.kt * n + (size_t)f.kp * p, stream);
+  f.tpart = plan.part.get();
   f.ppart = f.tpart + (size_t)f.kt * n;
-  DeviceArray<double> cpart((size_t)C * f.cslots, stream);
-  DeviceArray<double> scal((size_t)SC_H + kPersistMaxComponents + 8, stream);
-  DeviceArray<unsigned> bar(2, stream);
-  bar.zero(stream);
-  f.cpart = cpart.get();
-  f.scal = scal.get();
-  f.bar = bar.get();
-
-  DeviceArray<Fit> d_fit(1, stream);
-  FPLS_CHECK(cudaMemcpyAsync(d_fit.get(), &f, sizeof(Fit), cudaMemcpyHostToDevice, stream));
-  const Fit* fp = d_fit.get();
-  int nfits = 1;
-  int* flag = ws.flag.get();
-  void* args[] = {(void*)&fp, (void*)&nfits, (void*)&flag};
-  FPLS_CHECK(cudaLaunchCooperativeKernel((const void*)persistent_simpls<T>, dim3(C), dim3(PT), args,
-                                         kSmemDoubles * sizeof(double), stream));
-  count_launch();
-  FPLS_LAUNCH("persistent_simpls");
-  // the descriptor must outlive the launch: release it stream-ordered
-  d_fit.release();
+  plan.cpart.allocate((size_t)C * f.cslots, stream);
+  plan.scal.allocate((size_t)SC_H + kPersistMaxComponents + 8, stream);
+  plan.bar.allocate(2, stream);
+  plan.bar.zero(stream);
+  f.cpart = plan.cpart.get();
+  f.scal = plan.scal.get();
+  f.bar = plan.bar.get();
   model.a = a;
   return true;
 }
 
-template bool fit_simpls_persistent<float>(const float*, int, int, long, int, int, DeviceModel&,
-                                           double*, double*, Workspace&, cudaStream_t);
-template bool fit_simpls_persistent<double>(const double*, int, int, long, int, int, DeviceModel&,
-                                            double*, double*, Workspace&, cudaStream_t);
-template bool fit_simpls_persistent<bf16>(const bf16*, int, int, long, int, int, DeviceModel&,
-                                          double*, double*, Workspace&, cudaStream_t);
+void launch_persistent(const std::vector<PersistentPlan*>& plans, cudaStream_t stream) {
+  if (plans.empty()) return;
+  const int elem = plans[0]->elem;
+  std::vector<Fit> fits;
+  int total = 0;
+  for (PersistentPlan* pl : plans) {
+    require(pl->elem == elem, "one persistent launch takes one storage type");
+    Fit f = pl->fit;
+    f.cta0 = total;
+    total += f.C;
+    fits.push_back(f);
+  }
+  require(total <= persistent_capacity(elem), "persistent launch exceeds the co-resident CTAs");
+  DeviceArray<Fit> d_fits(fits.size(), stream);
+  FPLS_CHECK(cudaMemcpyAsync(d_fits.get(), fits.data(), sizeof(Fit) * fits.size(),
+                             cudaMemcpyHostToDevice, stream));
+  const Fit* fp = d_fits.get();
+  int nfits = (int)fits.size();
+  void* args[] = {(void*)&fp, (void*)&nfits};
+  const void* fn = elem == 2 ? (const void*)persistent_simpls<bf16>
+                 : elem == 4 ? (const void*)persistent_simpls<float>
+                             : (const void*)persistent_simpls<double>;
+  FPLS_CHECK(cudaLaunchCooperativeKernel(fn, dim3(total), dim3(PT), args,
+                                         kSmemDoubles * sizeof(double), stream));
+  count_launch();
+  FPLS_LAUNCH("persistent_simpls");
+  // the descriptors are freed stream-ordered, behind the launch
+}
+
+template bool plan_simpls_persistent<float>(const float*, int, int, long, int, int, DeviceModel&,
+                                            DeviceArray<double>&, double*, Workspace&, cudaStream_t,
+                                            PersistentPlan&);
+template bool plan_simpls_persistent<double>(const double*, int, int, long, int, int, DeviceModel&,
+                                             DeviceArray<double>&, double*, Workspace&, cudaStream_t,
+                                             PersistentPlan&);
+template bool plan_simpls_persistent<bf16>(const bf16*, int, int, long, int, int, DeviceModel&,
+                                           DeviceArray<double>&, double*, Workspace&, cudaStream_t,
+                                           PersistentPlan&);
 
 }  // namespace fpls

@@ -1,25 +1,76 @@
-// Persistent single-fit SIMPLS (one cooperative launch per fit; see
-// persistent.cu).
+// Persistent single-fit SIMPLS (one cooperative launch for every component
+// of one or several fits; see persistent.cu).
 #pragma once
 
 #include "model.cuh"
+
+#include <memory>
+#include <vector>
 
 namespace fpls {
 
 constexpr int kPersistMaxResponses = 32;
 constexpr int kPersistMaxComponents = 256;
 
+// Device-side description of one fit of a persistent launch.
+struct PersistentFit {
+  const void* X;
+  long ld;
+  int n, p, m, a;
+  const double* mean;
+  const double* scale;
+  const double* S0;
+  double *S, *R, *V, *Q, *T;
+  double* gpk;              // packed Gram of S (m (m + 1) / 2)
+  double *r, *rt, *pv, *v;  // p
+  double* tpart;            // kt x n
+  double* ppart;            // kp x p
+  double* cpart;            // C x cslots
+  double* scal;             // scalar slots
+  unsigned* bar;            // [count, generation]
+  int* flag;                // the fit's error flag
+  int cta0, C;              // CTA range of this fit in the launch
+  int cc, kt;               // t pass: columns per chunk, chunks
+  int rc, kp;               // loading pass: rows per chunk, chunks
+  int vec;                  // rows per 16-byte load in the t pass (1: scalar)
+  int pair;                 // row pairs per lane in the loading pass
+  int cslots;               // per-CTA partial slots
+};
+
+// One planned fit: its descriptor and the scratch it owns until the launch
+// has finished (every buffer is freed stream-ordered on the fit's stream).
+struct PersistentPlan {
+  PersistentFit fit{};
+  int elem = 0;  // bytes per stored element of X (2 BF16, 4 FP32, 8 FP64)
+  DeviceArray<double> S, part, cpart, scal;
+  DeviceArray<unsigned> bar;
+};
+
 // Whether the persistent path takes a fit with m responses and a components.
 bool persistent_supported(int m, int a);
+// CTAs a fit of n x p gets (a function of the shape only).
+int persistent_ctas(int n, int p);
+// CTAs one launch can hold co-resident for a storage type (0: unavailable).
+int persistent_capacity(int elem);
 
-// Runs the whole component loop of a SIMPLS fit (one direction per
-// component, no candidate blocks) as one cooperative launch, from S (p x m,
-// deflated in place), its packed Gram gpk, and model.{mean, scale, S0};
-// fills model.{R, Q, V, T}. Returns false (nothing enqueued) when the shape
-// or the device does not allow it; the caller then runs the per-kernel loop.
+// Plans the whole component loop of a SIMPLS fit (one direction per
+// component) from S (p x m, deflated in place; the plan takes it over), its
+// packed Gram gpk and model.{mean, scale, S0}, to fill model.{R, Q, V, T}.
+// Returns false (nothing planned, S untouched) when the shape or the device
+// does not allow it.
 template <class T>
-bool fit_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, DeviceModel& model,
-                           double* S, double* gpk, Workspace& ws, cudaStream_t stream);
+bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, DeviceModel& model,
+                            DeviceArray<double>& S, double* gpk, Workspace& ws, cudaStream_t stream,
+                            PersistentPlan& plan);
+
+// One cooperative launch for the planned fits (one storage type, total CTAs
+// within persistent_capacity) on `stream`, which must already be ordered
+// after the work that produced each plan.
+void launch_persistent(const std::vector<PersistentPlan*>& plans, cudaStream_t stream);
+
+// When set on this thread, a SIMPLS fit that plans a persistent launch hands
+// the plan to *sink instead of launching it (the caller batches plans).
+std::unique_ptr<PersistentPlan>*& persistent_deferral();
 
 // Process-wide switch (1 = use the persistent path where it applies).
 int& persistent_enabled();

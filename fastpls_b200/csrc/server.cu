@@ -16,6 +16,7 @@
 // There is no counterpart in the reference (it fits one model per call).
 #include "../../include/fastpls_b200.h"
 #include "handle.cuh"
+#include "persistent.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -84,6 +85,21 @@ size_t resident_footprint(const Request& r) {
   double bytes = 8.0 * (p * (2 * a + q + 2) + n * a + q * a);
   if (r.fit.method == kKernelPls) bytes += 8.0 * (n * p + n * a + 2 * n);
   return (size_t)bytes;
+}
+
+// A SIMPLS fit that runs as one persistent launch (one direction per
+// component, within the launch's co-resident CTAs) and can share that launch
+// with other such fits of the same storage type.
+bool batchable_fit(const Request& r) {
+  const FitRequest& f = r.fit;
+  if (r.kind != kFit || f.method != kSimpls || !persistent_enabled()) return false;
+  if (f.n < 2 || f.p < 1 || f.components < 1 || f.components > std::min(f.n - 1, f.p)) return false;
+  if (!persistent_supported(f.q, f.components)) return false;
+  if (simpls_block_size(f.n, f.p, f.q, f.components, !r.labels.empty(), r.precision == 32) != 1)
+    return false;
+  const int elem = r.precision == 16 ? 2 : r.precision == 32 ? 4 : 8;
+  const int cap = persistent_capacity(elem);
+  return cap > 0 && persistent_ctas(f.n, f.p) <= cap;
 }
 
 size_t predict_footprint(int rows, const Model& m) {
@@ -195,6 +211,12 @@ class Server {
     if (models) *models = models_.size();
   }
 
+  void batch_stats(size_t* launches, size_t* fits) {
+    std::lock_guard<std::mutex> lock(mu_);
+    if (launches) *launches = batched_launches_;
+    if (fits) *fits = batched_fits_;
+  }
+
  private:
   // Oldest admissible request; predictions for the same model queued behind
   // it join its batch. Called with mu_ held.
@@ -240,6 +262,26 @@ class Server {
       std::vector<Request*> batch{r};
       size_t fp = r->footprint;
       pending_.erase(it);
+      if (r->kind == kFit && batchable_fit(*r)) {
+        // later compatible fits that fit the budget share its persistent
+        // launch, up to the launch's co-resident CTAs
+        const int elem = r->precision == 16 ? 2 : r->precision == 32 ? 4 : 8;
+        const int cap = persistent_capacity(elem);
+        int ctas = persistent_ctas(r->fit.n, r->fit.p);
+        for (auto jt = pending_.begin(); jt != pending_.end() && (int)batch.size() < kFitBatchMax;) {
+          Request* o = *jt;
+          if (o->kind == kFit && o->precision == r->precision && batchable_fit(*o) &&
+              ctas + persistent_ctas(o->fit.n, o->fit.p) <= cap &&
+              in_use_ + fp + o->footprint <= budget_) {
+            ctas += persistent_ctas(o->fit.n, o->fit.p);
+            batch.push_back(o);
+            fp += o->footprint;
+            jt = pending_.erase(jt);
+          } else {
+            ++jt;
+          }
+        }
+      }
       if (model) {
         for (auto jt = pending_.begin(); jt != pending_.end();) {
           Request* o = *jt;
@@ -266,6 +308,21 @@ class Server {
 
   void worker() {
     cudaSetDevice(device_);
+    // this worker's stream for the persistent launches of fit batches
+    cudaStream_t launch_stream = nullptr;
+    if (cudaStreamCreateWithFlags(&launch_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      launch_stream = nullptr;
+    }
+    struct StreamGuard {
+      cudaStream_t s;
+      ~StreamGuard() {
+        if (s) {
+          cudaStreamSynchronize(s);
+          cudaStreamDestroy(s);
+        }
+      }
+    } guard{launch_stream};
     for (;;) {
       std::vector<Request*> batch;
       {
@@ -281,7 +338,11 @@ class Server {
       for (auto* r : batch) r->started = start;
       size_t charged = 0;
       for (auto* r : batch) charged += r->footprint;
-      if (batch[0]->kind == kFit) run_fit(batch[0], charged);
+      if (batch[0]->kind == kFit && batch.size() > 1 && launch_stream)
+        run_fit_batch(batch, launch_stream);
+      else if (batch[0]->kind == kFit && batch.size() > 1)
+        for (auto* r : batch) run_fit(r, r->footprint);
+      else if (batch[0]->kind == kFit) run_fit(batch[0], charged);
       else run_predict(batch, charged);
     }
   }
@@ -329,6 +390,96 @@ class Server {
     finish({r}, charged, nullptr);
   }
 
+  // Several SIMPLS fits in one persistent launch: each fit's inputs, moments
+  // and cross-product are prepared on its own handle's stream, one
+  // cooperative launch (on this worker's stream, after all of them) runs the
+  // component loops of every fit, and each handle then finishes on its own
+  // stream. A fit keeps the CTA count and chunking it has alone, so its
+  // result is bit-identical alone or in a batch.
+  void run_fit_batch(const std::vector<Request*>& batch, cudaStream_t batch_stream_) {
+    std::vector<std::unique_ptr<ResidentHandle>> handles(batch.size());
+    std::vector<PersistentPlan*> plans;
+    std::vector<size_t> pending_idx;
+    for (size_t i = 0; i < batch.size(); ++i) {
+      Request* r = batch[i];
+      try {
+        r->fit.x = r->x.data();
+        r->fit.y = r->y.empty() ? nullptr : r->y.data();
+        r->fit.labels = r->labels.empty() ? nullptr : r->labels.data();
+        handles[i].reset(make_handle(r->precision, r->fit, true));
+        if (PersistentPlan* pl = handles[i]->pending_plan()) {
+          plans.push_back(pl);
+          pending_idx.push_back(i);
+        }
+      } catch (const std::exception& e) {
+        r->status = 1;
+        r->error = e.what();
+        handles[i].reset();
+      }
+    }
+    if (!plans.empty()) {
+      std::vector<cudaEvent_t> evs;
+      try {
+        for (size_t i : pending_idx) {
+          cudaEvent_t e = nullptr;
+          FPLS_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+          evs.push_back(e);
+          FPLS_CHECK(cudaEventRecord(e, handles[i]->stream()));
+          FPLS_CHECK(cudaStreamWaitEvent(batch_stream_, e, 0));
+        }
+        launch_persistent(plans, batch_stream_);
+        cudaEvent_t done = nullptr;
+        FPLS_CHECK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        evs.push_back(done);
+        FPLS_CHECK(cudaEventRecord(done, batch_stream_));
+        for (size_t i : pending_idx) FPLS_CHECK(cudaStreamWaitEvent(handles[i]->stream(), done, 0));
+      } catch (const std::exception& e) {
+        cudaStreamSynchronize(batch_stream_);
+        for (size_t i : pending_idx) {
+          batch[i]->status = 1;
+          batch[i]->error = e.what();
+          handles[i].reset();
+        }
+      }
+      for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    }
+    for (size_t i = 0; i < batch.size(); ++i) {
+      Request* r = batch[i];
+      size_t keep = 0;
+      if (handles[i]) {
+        try {
+          handles[i]->complete_fit();
+          handles[i]->compact(false);  // training predictors are not needed for serving
+          Model m;
+          m.handle = std::move(handles[i]);
+          m.precision = r->precision;
+          m.q = r->fit.q;
+          m.p = r->fit.p;
+          m.ncomp = r->fit.components;
+          m.footprint = resident_footprint(*r);
+          keep = m.footprint;
+          std::lock_guard<std::mutex> lock(mu_);
+          models_.emplace(r->ticket, std::move(m));
+          in_use_ += keep;
+        } catch (const std::exception& e) {
+          r->status = 1;
+          r->error = e.what();
+          handles[i].reset();
+        }
+      }
+      r->x.clear();
+      r->x.shrink_to_fit();
+      r->y.clear();
+      r->y.shrink_to_fit();
+      finish({r}, r->footprint, nullptr);
+    }
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      ++batched_launches_;
+      batched_fits_ += plans.size();
+    }
+  }
+
   void run_predict(const std::vector<Request*>& batch, size_t charged) {
     Model* model = nullptr;
     {
@@ -374,6 +525,8 @@ class Server {
     finish(batch, charged, model);
   }
 
+  static constexpr int kFitBatchMax = 32;
+  size_t batched_launches_ = 0, batched_fits_ = 0;
   size_t budget_, in_use_ = 0;
   int device_ = 0;
   bool stop_ = false;
@@ -527,6 +680,13 @@ FASTPLS_B200_API int fastpls_b200_server_stats(void* server, size_t* bytes_in_us
                                                size_t* queued, size_t* resident_models) {
   if (!server) return 1;
   static_cast<Server*>(server)->stats(bytes_in_use, queued, resident_models);
+  return 0;
+}
+
+FASTPLS_B200_API int fastpls_b200_server_batch_stats(void* server, size_t* launches,
+                                                     size_t* fits) {
+  if (!server) return 1;
+  static_cast<Server*>(server)->batch_stats(launches, fits);
   return 0;
 }
 

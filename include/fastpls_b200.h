@@ -438,6 +438,15 @@ FASTPLS_B200_API int fastpls_b200_server_release(void* server, unsigned long lon
                                                  char* error, size_t error_capacity);
 FASTPLS_B200_API int fastpls_b200_server_stats(void* server, size_t* bytes_in_use,
                                                size_t* queued, size_t* resident_models);
+/* Fit batching: queued SIMPLS fits of one storage precision that each run as
+ * one persistent launch (one direction per component, 1..32 responses) are
+ * taken together, up to 32 fits or the launch's co-resident CTAs, and run
+ * their component loops in ONE cooperative launch; each fit keeps the CTA
+ * count and chunking it has alone, so its result is bit-identical alone or
+ * batched. launches: persistent launches that ran batches; fits: the fits
+ * they carried. */
+FASTPLS_B200_API int fastpls_b200_server_batch_stats(void* server, size_t* launches,
+                                                     size_t* fits);
 
 /* out (p x nb, FP64) = X^T V for device-resident X (n x p, leading
  * dimension ldx, FP32 or FP64 by `precision`), V (n x nb FP64, ldv) and out

@@ -82,3 +82,31 @@ def test_kernelpls_classification_block():
     for j, k in enumerate([3, 6]):
         assert O.rel_err(pred[j], O.kernelpls_predict(ref, xt, k)) < 1e-9
     model.close()
+
+
+def test_massive_fp32_regression_cross_covariance():
+    """FP32 regression whose p x q cross-covariance exceeds 512 MiB (4.2e6 x
+    33 x 4 bytes = 554 MB): the regime where the reference switches to its
+    implicit cross-covariance route and to blocks of min(8, a, p, q)
+    candidates (src/cuda_resident_simpls.cuh:125-127, :133-153). The device
+    keeps S explicit (1.1 GB in FP64) and takes the same candidate blocks;
+    coefficients and predictions match the FP64 oracle run with that block
+    rule on the same FP32-rounded values."""
+    n, p, q, a = 40, 4_200_000, 33, 10
+    assert p * q * 4 > 512 * 1024 * 1024
+    x, y = W.latent_regression(n, p, q, 6, 0.5, 71, dtype=np.float32)
+    block = O.simpls_block_size(n, p, q, a, False, fp32=True)
+    assert block == 8
+    model = api.fit_resident(x, y, ncomp=a, precision=32)
+    R = model.export(0).astype(np.float64)
+    Qm = model.export(1).astype(np.float64)
+    pre = [1, 8, 10]
+    pred = model.predict_path(x[:20], pre).astype(np.float64)
+    model.close()
+    x64 = x.astype(np.float64)
+    del x
+    ref = O.simpls_fit(x64, y.astype(np.float64), ncomp=a, scaling=1, block=block)
+    for k in pre:
+        assert O.rel_err(R[:, :k] @ Qm[:, :k].T, ref["R"][:, :k] @ ref["Q"][:, :k].T) < 1e-7, k
+    for j, k in enumerate(pre):
+        assert O.rel_err(pred[j], O.simpls_predict(ref, x64[:20], k)) < 1e-7, k

@@ -122,3 +122,35 @@ def test_prediction_behind_a_failing_fit_reports_it():
     with pytest.raises(Exception, match="fit failed|unknown model"):
         srv.wait(pt)
     srv.close()
+
+
+def test_batched_fits_share_one_persistent_launch():
+    """SIMPLS fits queued together (one worker, so later ones wait) run as
+    batches in one persistent cooperative launch; every fit's predictions
+    are bitwise those of the same fit made alone, and the oracle's."""
+    srv = api.Server(workers=1)
+    specs = [(200 + 37 * i, 150 + 61 * i, 1 + i % 4, 3 + i % 6) for i in range(16)]
+    data, tickets = [], []
+    for i, (n, p, q, a) in enumerate(specs):
+        x, y = W.latent_regression(n, p, q, 4, 0.4, 300 + i, dtype=np.float32)
+        data.append((x, y))
+    for i, (n, p, q, a) in enumerate(specs):
+        x, y = data[i]
+        tickets.append(srv.submit_fit(x, y, ncomp=a, precision=32))
+    for t in tickets:
+        srv.wait(t)
+    stats = srv.batch_stats()
+    assert stats["launches"] >= 1 and stats["fits"] >= 2, stats
+    for i, (n, p, q, a) in enumerate(specs):
+        x, y = data[i]
+        xt, _ = W.latent_regression(23, p, q, 4, 0.4, 700 + i, dtype=np.float32)
+        got, _, _ = srv.wait(srv.submit_predict(tickets[i], xt, [1, a]))
+        alone = api.fit_resident(x, y, ncomp=a, precision=32)
+        want = alone.predict_path(xt, [1, a])
+        alone.close()
+        assert np.array_equal(got, want), i
+        ref = O.simpls_fit(x.astype(np.float64), y.astype(np.float64), ncomp=a)
+        assert O.rel_err(got[1].astype(np.float64),
+                         O.simpls_predict(ref, xt.astype(np.float64), a)) < 1e-5, i
+        srv.release(tickets[i])
+    srv.close()
