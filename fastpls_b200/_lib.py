@@ -90,6 +90,8 @@ SIGNATURES = {
     "fastpls_b200_guard_refits": (_i, []),
     "fastpls_b200_last_fit_times": (None, [_dp, _dp]),
     "fastpls_b200_set_persistent": (None, [_i]),
+    "fastpls_b200_int8_wait_test": (None, [_i, C.c_longlong]),
+    "fastpls_b200_persistent_wait_test": (None, [_i, C.c_longlong]),
     "fastpls_b200_persistent": (_i, []),
     "fastpls_b200_set_autotune": (None, [_i]),
     "fastpls_b200_autotune": (_i, []),

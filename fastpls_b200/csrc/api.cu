@@ -641,6 +641,16 @@ void fastpls_b200_set_persistent(int enable) { persistent_enabled() = enable ? 1
 
 int fastpls_b200_persistent(void) { return persistent_enabled(); }
 
+void fastpls_b200_int8_wait_test(int skip_last_stage, long long wait_cycles) {
+  ozaki_wait_test().skip_last = skip_last_stage ? 1 : 0;
+  ozaki_wait_test().cycles = wait_cycles;
+}
+
+void fastpls_b200_persistent_wait_test(int absent_cta, long long wait_cycles) {
+  persistent_wait_test().absent = absent_cta ? 1 : 0;
+  persistent_wait_test().cycles = wait_cycles;
+}
+
 void fastpls_b200_set_autotune(int enable) { batch_autotune() = enable ? 1 : 0; }
 
 int fastpls_b200_autotune(void) { return batch_autotune(); }

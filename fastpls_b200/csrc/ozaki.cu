@@ -41,6 +41,11 @@ int& ozaki_slices() {
 // (consecutive MMAs alternate between the diagonals' accumulators), 0 =
 // diagonal-major. Bit-identical results either way; the environment
 // variable FASTPLS_B200_INT8_ORDER (0 or 1) overrides the default.
+OzakiWaitTest& ozaki_wait_test() {
+  static OzakiWaitTest t;
+  return t;
+}
+
 int ozaki_mma_order() {
   static const int order = [] {
     const char* e = std::getenv("FASTPLS_B200_INT8_ORDER");
@@ -85,6 +90,8 @@ struct OzArgs {
   int rows_pa, rows_pb;  // padded rows of the digit layouts of A and B
   int slices, stages, lower, accumulate;
   int interleave;    // MMA order within a stage (1: digit-major across diagonals)
+  int skip_last;     // test of the bounded waits: withhold each tile's last stage
+  long long wait_cycles;  // bound of the MMA issuer's wait for a stage
   long ldc;
   double* C;
   const double* scale_a;
@@ -125,11 +132,12 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
 // thread of the CTA gave up (abort set, unless ignore_abort) or after
 // OZ_WAIT_CYCLES; a timeout sets the CTA abort flag and the error flag.
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
-                          int* flag, bool ignore_abort = false) {
+                          int* flag, bool ignore_abort = false,
+                          long long limit = OZ_WAIT_CYCLES) {
   const long long start = clock64();
   while (!mbar_test(bar, parity)) {
     if (!ignore_abort && *abort) return false;
-    if (clock64() - start > OZ_WAIT_CYCLES) {
+    if (clock64() - start > limit) {
       *abort = 1;
       flag_error(flag, 4);
       return false;
@@ -303,6 +311,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int kb = 0; kb < args.kblocks; kb += kbs) {
           const int nk = min(kbs, args.kblocks - kb);
           const int st = it % stages;
+          if (args.skip_last && pass + 1 == npass && kb + kbs >= args.kblocks) {
+            ok = false;  // the stage is never issued: the MMA issuer's wait runs out
+            break;
+          }
           if (it >= (uint32_t)stages &&
               !mbar_wait(&empty_bar[st], ((it / stages) - 1) & 1, abort, args.flag)) {
             ok = false;
@@ -347,7 +359,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int kb = 0; kb < args.kblocks; kb += kbs) {
           const int nk = min(kbs, args.kblocks - kb);
           const int st = it % stages;
-          if (!mbar_wait(&full_bar[st], (it / stages) & 1, abort, args.flag)) {
+          if (!mbar_wait(&full_bar[st], (it / stages) & 1, abort, args.flag, false,
+                         args.wait_cycles)) {
             ok = false;
             break;
           }
@@ -1127,6 +1140,8 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   const int S = a.slices;
   require(tile_n == 0 || tile_n == 128 || tile_n == 192 || tile_n == 256,
           "int8 split product: tile width 128, 192 or 256");
+  require(!(pair == 1 && ozaki_wait_test().skip_last),
+          "int8 split product: the bounded-wait test runs on single-CTA tiles");
   require(!(pair == 1 && (lower || tile_n == 128)),
           "int8 split product: CTA pairs need a rectangular product with 192 or 256 columns");
   const TileChoice tc = lower ? TileChoice{128, false} : pick_tile(a.rows, b.rows, tile_n, pair);
@@ -1144,6 +1159,8 @@ void ozaki_gemm(const OzakiOperand& a, const OzakiOperand& b, double* C, long ld
   args.rows_pa = a.rows_p;
   args.rows_pb = b.rows_p;
   args.interleave = ozaki_mma_order();
+  args.skip_last = ozaki_wait_test().skip_last;
+  args.wait_cycles = ozaki_wait_test().cycles > 0 ? ozaki_wait_test().cycles : OZ_WAIT_CYCLES;
   const int tiles_n = ceil_div(b.rows, bn);
   args.tiles_n = tiles_n;
   if (tc.pair) {

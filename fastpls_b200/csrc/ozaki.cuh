@@ -75,6 +75,17 @@ int ozaki_wide_tile(int a_rows, int b_rows);
 int& ozaki_slices();
 int ozaki_mma_order();
 
+// Test of the bounded waits of the int8 product (single-CTA tiles): with
+// skip_last set, every tile's producer withholds its last stage, so the MMA
+// issuer's wait for it runs out after `cycles` clocks; the kernel then sets
+// its error flag (4), waits for the copies and MMAs it issued, frees TMEM and
+// returns. cycles <= 0 keeps the default bound (about 2 s).
+struct OzakiWaitTest {
+  int skip_last = 0;
+  long long cycles = 0;
+};
+OzakiWaitTest& ozaki_wait_test();
+
 // Timing of the last ozaki_gemm launches (CUDA events), for benchmarks.
 void ozaki_profile_enable(bool on);
 bool ozaki_profile_enabled();

@@ -87,7 +87,7 @@ __device__ bool group_sync(const Fit& f, int* flag, F&& reduce) {
     if (!last_s) {
       const long long t0 = clock64();
       while (ld_acquire(f.bar + 1) == gen) {
-        if (clock64() - t0 > kBarrierCycles) {
+        if (clock64() - t0 > f.barrier_cycles) {
           flag_error(flag, 5);
           ok_s = 0;
           break;
@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(PT, 2)
   const Fit f = fits[fi];
   int* const flag = f.flag;
   const int cta = (int)blockIdx.x - f.cta0;
+  if (cta == f.absent_cta) return;  // bounded-wait test only
   const T* X = static_cast<const T*>(f.X);
   const int n = f.n, p = f.p, m = f.m, C = f.C;
   const int tid = threadIdx.x;
@@ -550,6 +551,11 @@ bool persistent_supported(int m, int a) {
   return m >= 1 && m <= kPersistMaxResponses && a >= 1 && a <= kPersistMaxComponents;
 }
 
+PersistentWaitTest& persistent_wait_test() {
+  static PersistentWaitTest t;
+  return t;
+}
+
 std::unique_ptr<PersistentPlan>*& persistent_deferral() {
   thread_local std::unique_ptr<PersistentPlan>* sink = nullptr;
   return sink;
@@ -636,6 +642,9 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   f.vec = aligned16 ? VN : 1;
   f.pair = (reinterpret_cast<uintptr_t>(X) % (2 * sizeof(T)) == 0 && ld % 2 == 0) ? 1 : 0;
   f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2));
+  const PersistentWaitTest& wt = persistent_wait_test();
+  f.barrier_cycles = wt.cycles > 0 ? wt.cycles : kBarrierCycles;
+  f.absent_cta = wt.absent ? 0 : -1;
 
   // scratch of this fit (stream-ordered, freed behind the launch); the
   // workspace's own scalar arrays hold the Gram of S and stay untouched

@@ -35,6 +35,8 @@ struct PersistentFit {
   int vec;                  // rows per 16-byte load in the t pass (1: scalar)
   int pair;                 // row pairs per lane in the loading pass
   int cslots;               // per-CTA partial slots
+  long long barrier_cycles; // bound of each barrier wait
+  int absent_cta;           // test of the bounded waits: this CTA never arrives (-1: none)
 };
 
 // One planned fit: its descriptor and the scratch it owns until the launch
@@ -74,5 +76,15 @@ std::unique_ptr<PersistentPlan>*& persistent_deferral();
 
 // Process-wide switch (1 = use the persistent path where it applies).
 int& persistent_enabled();
+
+// Test of the bounded barrier waits: with absent set, CTA 0 of every fit
+// leaves before its first barrier, so the other CTAs' waits run out after
+// `cycles` clocks; they set the fit's error flag (5) and return, and the fit
+// reports an error. cycles <= 0 keeps the default bound (about 2 s).
+struct PersistentWaitTest {
+  int absent = 0;
+  long long cycles = 0;
+};
+PersistentWaitTest& persistent_wait_test();
 
 }  // namespace fpls

@@ -259,6 +259,18 @@ FASTPLS_B200_API void fastpls_b200_last_fit_times(double* copy_ms, double* fit_m
  * components); 0 runs the per-kernel loop. Results agree to rounding.
  * Process-wide. */
 FASTPLS_B200_API void fastpls_b200_set_persistent(int enable);
+/* Tests of the bounded waits (no reference counterpart). Every wait of the
+ * tensor-core product and of the persistent fit has an iteration bound after
+ * which the kernel records an error, finishes its own copies and MMAs, and
+ * returns, so the call fails with an error and the device stays usable.
+ * fastpls_b200_int8_wait_test(1, cycles): every tile of the int8 product
+ * withholds its last pipeline stage, so the MMA issuer's wait for it runs
+ * out after `cycles` clocks and the product reports a timed-out wait.
+ * fastpls_b200_persistent_wait_test(1, cycles): one CTA of each persistent
+ * fit leaves before its first barrier, so the others' barrier waits run out.
+ * (0, 0) restores normal operation. Process-wide; for tests only. */
+FASTPLS_B200_API void fastpls_b200_int8_wait_test(int skip_last_stage, long long wait_cycles);
+FASTPLS_B200_API void fastpls_b200_persistent_wait_test(int absent_cta, long long wait_cycles);
 FASTPLS_B200_API int fastpls_b200_persistent(void);
 FASTPLS_B200_API void fastpls_b200_set_autotune(int enable);
 FASTPLS_B200_API int fastpls_b200_autotune(void);
