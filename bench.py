@@ -810,7 +810,30 @@ def main():
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t0
         plain_fits = a.plain_perms * FOLDS
+        # one fold-sized fit alone: device time of the fit proper against the
+        # HBM bound of its X passes ((1 + 2a) n_train p 4 bytes)
+        from fastpls_b200 import api as _fapi
+        tr = np.nonzero(fo != 1)[0]
+        xtr, ytr = np.asfortranarray(xf[tr]), np.asfortranarray(yf[tr])
+        for _ in range(2):
+            _fapi.fit_resident(xtr, ytr, ncomp=NCOMP, precision=32).close()
+        fms = []
+        for _ in range(5):
+            _fapi.fit_resident(xtr, ytr, ncomp=NCOMP, precision=32).close()
+            fms.append(_fapi.last_fit_times()["fit_ms"])
+        fold_ms = float(np.median(fms))
+        fold_bytes = (1.0 + 2.0 * NCOMP) * len(tr) * P * 4
+        pk = measured_peaks()
+        fold_gbs = fold_bytes / (fold_ms * 1e-3) / 1e9
         plain = {"value": plain_fits / dt, "unit": "fits/s",
+                 "fold_fit": {"shape": f"{len(tr)}x{P} f32, ncomp {NCOMP}",
+                              "fit_ms": fold_ms,
+                              "path": "persistent" if _fapi.persistent() else "per-kernel loop",
+                              "roofline": {"bound": "hbm", "achieved": fold_gbs,
+                                           "peak": pk["hbm_gbs"], "unit": "GB/s",
+                                           "frac": fold_gbs / pk["hbm_gbs"],
+                                           "algorithmic_bytes": fold_bytes,
+                                           "peak_source": pk["source"]}},
                  "sample": f"{a.plain_perms} permutations x {FOLDS} folds through "
                            "fastpls_resident_simpls_cv_regression (one fold fit at a "
                            "time, FP32 storage, host buffers)",
