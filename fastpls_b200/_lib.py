@@ -71,6 +71,8 @@ SIGNATURES = {
     "fastpls_b200_fastsvd": (_i, [_vp, _i, _i, _i, _i, _i, _i, _ull, _vp, _vp, _vp, _cp, _sz]),
     "fastpls_b200_simpls_cv_permutation_classification": (
         _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _cp, _sz]),
+    "fastpls_b200_simpls_cv_permutation_classification_head": (
+        _i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _i, _i, _i, _vp, _vp, _cp, _sz]),
     "fastpls_b200_resident_vip": (_i, [_vp, _vp, _sz, _cp, _sz]),
     "fastpls_b200_model_import": (_vp, [_i, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp,
                                         _vp, _vp, _cp, _sz]),

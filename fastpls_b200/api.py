@@ -597,16 +597,17 @@ def fastsvd(x, ncomp, oversample=32, power=5, seed=1, precision=64, audit=False)
 
 
 def cv_permutation_classification(X, labels, classes, folds, permutations, prefixes,
-                                  scaling="centering", precision=32, digits=None):
+                                  scaling="centering", precision=32, digits=None, lda=False):
     """Batched classification CV over the observed labels and their row
-    permutations (``fastpls_b200_simpls_cv_permutation_classification``,
-    argmax head). Returns dict(accuracy=(permutations + 1, prefixes), status)."""
+    permutations (``fastpls_b200_simpls_cv_permutation_classification_head``;
+    argmax head, or LDA on the latent scores with lda=True). Returns
+    dict(accuracy=(permutations + 1, prefixes), status)."""
     if digits is not None:
         old = product_digits()
         set_product_digits(digits)
         try:
             return cv_permutation_classification(X, labels, classes, folds, permutations,
-                                                 prefixes, scaling, precision, None)
+                                                 prefixes, scaling, precision, None, lda)
         finally:
             set_product_digits(old)
     dt = _dtype(precision)
@@ -625,9 +626,9 @@ def cv_permutation_classification(X, labels, classes, folds, permutations, prefi
     status = np.zeros(int(folds.max()), dtype=np.int32)
     sc = SCALING[scaling] if isinstance(scaling, str) else int(scaling)
     err, cap = _lib.error_buffer()
-    rc = _lib.load().fastpls_b200_simpls_cv_permutation_classification(
+    rc = _lib.load().fastpls_b200_simpls_cv_permutation_classification_head(
         _p(x), _p(lab), _p(folds), _p(perms), P, precision, n, p, int(classes), _p(pre), k, sc,
-        _p(acc), _p(status), err, cap)
+        1 if lda else 0, _p(acc), _p(status), err, cap)
     _lib.check(rc, err)
     return dict(accuracy=acc.reshape((P + 1, k)), status=status)
 

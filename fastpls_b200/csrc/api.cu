@@ -206,7 +206,7 @@ template <class T>
 void cv_permutation_classification(const T* predictors, const int* labels, const int* folds,
                                    const int* permutations, int permutation_count, int n, int p,
                                    int classes, const int* prefixes, int prefix_count,
-                                   int scaling, double* accuracy, int* status) {
+                                   int scaling, double* accuracy, int* status, bool lda = false) {
   if (!predictors || !labels || !folds || !prefixes || !accuracy || n < 2 || p < 1 ||
       classes < 2 || classes > kBatchMaxResponses || prefix_count < 1 || scaling < 1 ||
       scaling > 3 || permutation_count < 0 || (permutation_count > 0 && !permutations))
@@ -274,6 +274,7 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
     }
     BatchedCv<T> engine;
     engine.class_labels = L.get();
+    engine.lda_head = lda;
     engine.run(X.get(), n, p, Y.get(), classes, folds, P.get(), permutation_count, prefixes,
                prefix_count, scaling, s);
     engine.accuracy(accuracy);
@@ -761,6 +762,27 @@ int fastpls_b200_simpls_cv_permutation_classification(
       cv_permutation_classification<double>(static_cast<const double*>(predictors), labels, folds,
                                             permutations, permutation_count, n, p, classes,
                                             prefixes, prefix_count, scaling, accuracy, status);
+  });
+}
+
+int fastpls_b200_simpls_cv_permutation_classification_head(
+    const void* predictors, const int* labels, const int* folds, const int* permutations,
+    int permutation_count, int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, int lda, double* accuracy, int* status, char* error,
+    size_t error_capacity) {
+  return guarded(error, error_capacity, "unknown batched CUDA CV error", [&] {
+    if (precision != 32 && precision != 64)
+      throw std::invalid_argument("invalid batched CUDA CV precision");
+    if (lda != 0 && lda != 1) throw std::invalid_argument("invalid batched CUDA CV head");
+    if (precision == 32)
+      cv_permutation_classification<float>(static_cast<const float*>(predictors), labels, folds,
+                                           permutations, permutation_count, n, p, classes, prefixes,
+                                           prefix_count, scaling, accuracy, status, lda != 0);
+    else
+      cv_permutation_classification<double>(static_cast<const double*>(predictors), labels, folds,
+                                            permutations, permutation_count, n, p, classes,
+                                            prefixes, prefix_count, scaling, accuracy, status,
+                                            lda != 0);
   });
 }
 

@@ -30,6 +30,7 @@
 #include "small.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -66,6 +67,12 @@ struct InstanceView {
                             // decision fell inside the int8-product margin
                             // (null: FP64 products, no margin)
   double guard;             // relative argmax margin (argmax_guard())
+  // LDA head (classification): the training scores (n x kmax per instance,
+  // zero on held-out rows) and held-out scores (max_test x kmax) are kept and
+  // the head runs after the last component; null for the argmax head
+  double* ttr;
+  double* tte;
+  int max_test;
 };
 
 __device__ __forceinline__ int src_row(const InstanceView& v, int perm, int r) {
@@ -280,8 +287,12 @@ __global__ void scores_batched(InstanceView v, const double* Y1, double* Tm,
   const bool ok = tn > 0.0 && isfinite(tn);
   if (!ok && threadIdx.x == 0) flag_error(flag, 1);
   const double inv = ok ? 1.0 / tn : 0.0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x)
-    t[r] = (v.fold_of_row[r] != f + 1) ? (y[r] - mu) * inv : 0.0;
+  double* ttr = v.ttr ? v.ttr + ((long)i * v.kmax + a) * n : nullptr;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const double tv = (v.fold_of_row[r] != f + 1) ? (y[r] - mu) * inv : 0.0;
+    t[r] = tv;
+    if (ttr) ttr[r] = tv;
+  }
   __syncthreads();
   const double* c0 = C0 + (long)i * n * q;
   for (int c = 0; c < q; ++c) {
@@ -300,14 +311,19 @@ __global__ void scores_batched(InstanceView v, const double* Y1, double* Tm,
   double* yh = yhat + (long)i * yhat_ld * q;
   const int slot = prefix_slot[a];
   double err = 0.0;
+  double* tte = v.tte ? v.tte + ((long)i * v.kmax + a) * v.max_test : nullptr;
   for (int k = threadIdx.x; k < nte; k += blockDim.x) {
     const int r = te[k];
     const double tt = (y[r] - mu) * inv;
+    if (tte) {
+      tte[k] = tt;  // the LDA head reads the held-out scores after the last component
+      continue;
+    }
     for (int c = 0; c < q; ++c)
       yh[k + (long)c * yhat_ld] = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
     if (slot >= 0) err += heldout_term(v, i, b, r, ymean, yh + k, yhat_ld);
   }
-  if (slot >= 0) {
+  if (slot >= 0 && !tte) {
     err = block_sum(err, scratch);
     if (threadIdx.x == 0) sse[(long)i * prefix_count + slot] = err;
   }
@@ -489,11 +505,15 @@ __global__ void __launch_bounds__(BT)
   const bool ok = tn > 0.0 && isfinite(tn);
   if (!ok && threadIdx.x == 0) flag_error(flag, 1);
   const double inv = ok ? 1.0 / tn : 0.0;
+  double* ttr = v.ttr ? v.ttr + ((long)i * v.kmax + a) * n : nullptr;
 #pragma unroll
   for (int j = 0; j < RPT; ++j) {
     const int r = threadIdx.x + j * BT;
     val[j] = (train >> j & 1u) ? (val[j] - mu) * inv : 0.0;
-    if (r < n) t[r] = val[j];
+    if (r < n) {
+      t[r] = val[j];
+      if (ttr) ttr[r] = val[j];
+    }
   }
   const double* c0 = C0 + (long)i * n * q;
   for (int c = 0; c < q; ++c) {
@@ -513,16 +533,172 @@ __global__ void __launch_bounds__(BT)
   double* yh = yhat + (long)i * yhat_ld * q;
   const int slot = prefix_slot[a];
   double err = 0.0;
+  double* tte = v.tte ? v.tte + ((long)i * v.kmax + a) * v.max_test : nullptr;
   for (int k = threadIdx.x; k < nte; k += blockDim.x) {
     const int r = te[k];
     const double tt = (y[r] - mu) * inv;
+    if (tte) {
+      tte[k] = tt;  // the LDA head reads the held-out scores after the last component
+      continue;
+    }
     for (int c = 0; c < q; ++c)
       yh[k + (long)c * yhat_ld] = fma(tt, qs[c], yh[k + (long)c * yhat_ld]);
     if (slot >= 0) err += heldout_term(v, i, b, r, ymean, yh + k, yhat_ld);
   }
-  if (slot >= 0) {
+  if (slot >= 0 && !tte) {
     err = block_sum(err, scratch);
     if (threadIdx.x == 0) sse[(long)i * prefix_count + slot] = err;
+  }
+}
+
+// LDA head of one instance, after its last component (classification with
+// the LDA head): training scores T (n x kmax, zero on held-out rows), the
+// counts of its active classes (those present in its training rows), the
+// score Gram T^T T and the class sums; then per prefix k the pooled
+// within-class covariance (T_k^T T_k - sum_c n_c mu_c mu_c^T) / max(1, n - c),
+// the first ridge rho * trace / k (rho in 1e-8, 1e-6, 1e-5, 1e-4, 1e-3,
+// 1e-2) whose Cholesky factorisation and solves succeed, the linear terms
+// Sigma^-1 mu_c and constants -mu_c^T Sigma^-1 mu_c / 2 + log prior_c
+// (train_lda_prefixes / finalize_lda_prefixes,
+// inst/include/fastpls/core/lda.hpp:86-223), and the held-out argmax over
+// the active classes (first wins on ties) against the row's class. The hit
+// count of prefix slot j goes to sse[j]. Dynamic shared memory:
+// 3 K^2 + 2 q K + q + K doubles (K = kmax <= kLdaMaxComponents).
+constexpr int kLdaMaxComponents = 32;
+constexpr int LDA_BT = 128;
+
+__global__ void __launch_bounds__(LDA_BT)
+    lda_heads(InstanceView v, const int* __restrict__ prefixes, int prefix_count, double* sse,
+              int* flag) {
+  extern __shared__ double sm[];
+  __shared__ int cnt[kBatchMaxResponses];
+  __shared__ int active[kBatchMaxResponses];
+  __shared__ int nact_s;
+  __shared__ double red[32];
+  const int i = blockIdx.x;
+  const int f = v.inst_fold[i], b = v.inst_perm[i];
+  const int n = v.n, q = v.q, K = v.kmax;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  double* gram = sm;               // K x K
+  double* sums = gram + K * K;     // q x K (class-major)
+  double* cov = sums + q * K;      // K x K
+  double* L = cov + K * K;         // K x K
+  double* lin = L + K * K;         // q x K (active classes first)
+  double* cst = lin + q * K;       // q
+  double* rhs = cst + q;           // K
+  const double* T = v.ttr + (long)i * K * n;
+  const double* Tt = v.tte + (long)i * K * v.max_test;
+  for (int c = threadIdx.x; c < q; c += blockDim.x) cnt[c] = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < n; r += blockDim.x)
+    if (v.fold_of_row[r] != f + 1) atomicAdd(&cnt[v.labels[src_row(v, b, r)]], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int na = 0;
+    for (int c = 0; c < q; ++c)
+      if (cnt[c] > 0) active[na++] = c;
+    nact_s = na;
+  }
+  // Gram of the training scores (held-out rows hold zeros), lower triangle
+  const int pairs = K * (K + 1) / 2;
+  for (int k = warp; k < pairs; k += warps) {
+    int c1 = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+    while (c1 * (c1 + 1) / 2 > k) --c1;
+    while ((c1 + 1) * (c1 + 2) / 2 <= k) ++c1;
+    const int c2 = k - c1 * (c1 + 1) / 2;
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32) acc = fma(T[(long)c1 * n + r], T[(long)c2 * n + r], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      gram[c1 + c2 * K] = acc;
+      gram[c2 + c1 * K] = acc;
+    }
+  }
+  __syncthreads();
+  const int nact = nact_s;
+  // class sums of the training scores (active classes, in class order)
+  for (int k = warp; k < nact * K; k += warps) {
+    const int ci = k / K, comp = k % K;
+    const int cls = active[ci];
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32)
+      if (v.fold_of_row[r] != f + 1 && v.labels[src_row(v, b, r)] == cls)
+        acc += T[(long)comp * n + r];
+    acc = warp_sum(acc);
+    if (lane == 0) sums[ci * K + comp] = acc;
+  }
+  __syncthreads();
+  const int ntr = v.ntrain[f];
+  const int* te = v.test_rows + v.test_off[f];
+  const int nte = v.test_off[f + 1] - v.test_off[f];
+  for (int j = 0; j < prefix_count; ++j) {
+    const int k = prefixes[j];
+    if (threadIdx.x == 0) {
+      // means (in sums' slots scaled on the fly), pooled covariance, ridge grid
+      const double denom = (double)max(1, ntr > nact ? ntr - nact : 1);
+      double trace = 0.0;
+      for (int c2 = 0; c2 < k; ++c2)
+        for (int c1 = 0; c1 < k; ++c1) {
+          double val = gram[c1 + c2 * K];
+          for (int ci = 0; ci < nact; ++ci) {
+            const double nc = (double)cnt[active[ci]];
+            val -= nc * (sums[ci * K + c1] / nc) * (sums[ci * K + c2] / nc);
+          }
+          cov[c1 + c2 * k] = val / denom;
+          if (c1 == c2) trace += cov[c1 + c2 * k];
+        }
+      double scale = trace / k;
+      if (!isfinite(scale) || scale <= 0.0) scale = 1.0;
+      const double grid[6] = {1e-8, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2};
+      bool solved = false;
+      for (int g = 0; g < 6 && !solved; ++g) {
+        for (int idx = 0; idx < k * k; ++idx) L[idx] = cov[idx];
+        if (!cholesky_serial(L, k, grid[g] * scale)) continue;
+        bool ok = true;
+        for (int ci = 0; ci < nact && ok; ++ci) {
+          const double nc = (double)cnt[active[ci]];
+          for (int c1 = 0; c1 < k; ++c1) rhs[c1] = sums[ci * K + c1] / nc;
+          ok = cholesky_solve_serial(L, k, rhs);
+          for (int c1 = 0; c1 < k; ++c1) lin[ci * K + c1] = rhs[c1];
+        }
+        solved = ok;
+      }
+      if (!solved) flag_error(flag, 6);
+      for (int ci = 0; ci < nact; ++ci) {
+        const double nc = (double)cnt[active[ci]];
+        double prod = 0.0;
+        for (int c1 = 0; c1 < k; ++c1) prod += (sums[ci * K + c1] / nc) * lin[ci * K + c1];
+        cst[ci] = -0.5 * prod + log(fmax(nc / (double)ntr, DBL_MIN));
+      }
+    }
+    __syncthreads();
+    double hits = 0.0;
+    for (int kk = threadIdx.x; kk < nte; kk += blockDim.x) {
+      const int r = te[kk];
+      int best = -1;
+      double bv = 0.0, sv = 0.0;
+      bool second = false;
+      for (int ci = 0; ci < nact; ++ci) {
+        double d = cst[ci];
+        for (int c1 = 0; c1 < k; ++c1) d = fma(Tt[(long)c1 * v.max_test + kk], lin[ci * K + c1], d);
+        if (best < 0 || d > bv) {
+          if (best >= 0) {
+            sv = bv;
+            second = true;
+          }
+          best = ci;
+          bv = d;
+        } else if (!second || d > sv) {
+          sv = d;
+          second = true;
+        }
+      }
+      if (v.amb && second && !(bv - sv > v.guard * fmax(fabs(bv), fabs(sv)))) v.amb[i] = 1;
+      if (best >= 0 && active[best] == v.labels[src_row(v, b, r)]) hits += 1.0;
+    }
+    hits = block_sum(hits, red);
+    if (threadIdx.x == 0) sse[(long)i * prefix_count + j] = hits;
+    __syncthreads();
   }
 }
 
@@ -680,7 +856,8 @@ struct BatchedWorkspace {
   // per-call inputs and the shared Gram
   OzakiOperand gram_split, x_split;
   DeviceArray<double> gram, Y64, x64;
-  DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, flag, perms, labels;
+  DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, d_pre, flag, perms, labels;
+  DeviceArray<double> Ttr, Tte;  // LDA head: training / held-out scores per instance
   std::vector<GroupGraph> graphs;
 
   BatchedWorkspace() {
@@ -707,10 +884,10 @@ struct BatchedWorkspace {
       L.rhs.scale.release();
     }
     for (auto* a : {&d_if, &d_ip, &amb, &d_fold, &d_ntrain, &d_test_rows, &d_test_off, &d_slot,
-                    &flag, &perms, &labels})
+                    &d_pre, &flag, &perms, &labels})
       a->release();
     for (auto* a : {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram,
-                    &Y64, &x64})
+                    &Y64, &x64, &Ttr, &Tte})
       a->release();
     for (OzakiOperand* o : {&gram_split, &x_split}) {
       o->digits.release();
@@ -734,7 +911,7 @@ struct BatchedWorkspace {
   size_t held_bytes() const {
     size_t b = (d_if.size() + d_ip.size() + amb.size()) * sizeof(int);
     for (const auto* a :
-         {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram})
+         {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram, &Ttr, &Tte})
       b += a->size() * sizeof(double);
     return b + gram_split.digits.size();
   }
@@ -969,6 +1146,18 @@ void BatchedCv<T>::enqueue_group(int I, int nlanes, int tile_n, cudaStream_t s) 
       FPLS_LAUNCH("deflate_batched");
     }
   }
+  if (lda_head) {
+    const size_t smem_lda =
+        (3 * (size_t)kmax * kmax + 2 * (size_t)q * kmax + q + kmax) * sizeof(double);
+    for (int l = 0; l < nlanes; ++l) {
+      LaneState& L = ws->lanes[l];
+      lda_heads<<<L.cnt, LDA_BT, smem_lda, L.st>>>(L.v, ws->d_pre.get(), prefix_count,
+                                                     ws->sse.get() + (size_t)L.off * prefix_count,
+                                                     ws->flag.get());
+      count_launch();
+      FPLS_LAUNCH("lda_heads");
+    }
+  }
   for (int l = 0; l < nlanes; ++l) {
     FPLS_CHECK(cudaEventRecord(ws->lanes[l].done, ws->lanes[l].st));
     FPLS_CHECK(cudaStreamWaitEvent(s, ws->lanes[l].done, 0));
@@ -1003,6 +1192,10 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
   grow(ws->U, (size_t)n * cI, s);
   grow(ws->Y1, (size_t)n * cI, s);
   grow(ws->KC0, nq * cI, s);
+  if (lda_head) {
+    grow(ws->Ttr, (size_t)n * kmax * cI, s);
+    grow(ws->Tte, (size_t)max_test * kmax * cI, s);
+  }
   FPLS_CHECK(cudaMemcpyAsync(ws->d_if.get(), inst_fold.data(), sizeof(int) * I,
                              cudaMemcpyHostToDevice, s));
   FPLS_CHECK(cudaMemcpyAsync(ws->d_ip.get(), inst_perm.data(), sizeof(int) * I,
@@ -1053,6 +1246,9 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
       v.labels = class_labels;
       v.guard = argmax_guard();
       v.amb = guard ? ws->amb.get() + L.off : nullptr;
+      v.max_test = max_test;
+      v.ttr = lda_head ? ws->Ttr.get() + (size_t)L.off * n * kmax : nullptr;
+      v.tte = lda_head ? ws->Tte.get() + (size_t)L.off * max_test * kmax : nullptr;
       if (digits > 0) {
         // size the digits of the largest right-hand side (K C0: q columns
         // per instance) so the products inside the sequence never allocate
@@ -1068,7 +1264,8 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     if (timed) FPLS_CHECK(cudaEventRecord(ws->t0, s));
     if (use_graph) {
       std::vector<long long> gkey = {n, q, I, kmax, prefix_count, max_test, digits, center,
-                                     d.lanes, d.tile_n, class_labels ? 1 : 0, guard ? 1 : 0};
+                                     d.lanes, d.tile_n, class_labels ? 1 : 0, guard ? 1 : 0,
+                                     lda_head ? 1 : 0};
       long long gbits = 0;
       const double gv = argmax_guard();
       std::memcpy(&gbits, &gv, sizeof(gbits));
@@ -1084,7 +1281,8 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
             (const void*)ws->d_fold.get(), (const void*)ws->d_ntrain.get(),
             (const void*)ws->d_test_rows.get(), (const void*)ws->d_test_off.get(),
             (const void*)ws->d_slot.get(), (const void*)ws->flag.get(), (const void*)perms,
-            (const void*)class_labels})
+            (const void*)class_labels, (const void*)ws->d_pre.get(), (const void*)ws->Ttr.get(),
+            (const void*)ws->Tte.get()})
         gkey.push_back((long long)(uintptr_t)ptr);
       for (int l = 0; l < d.lanes; ++l) {
         gkey.push_back((long long)(uintptr_t)ws->lanes[l].rhs.digits.get());
@@ -1199,11 +1397,14 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   center = scaling != 3;
   digits = ozaki_slices();
   require(q >= 1 && q <= kBatchMaxResponses, "batched CV supports 1..32 responses");
+  require(!lda_head || class_labels, "the LDA head needs class labels");
   kmax = 0;
   for (int j = 0; j < count; ++j) {
     if (prefixes_[j] <= kmax) throw std::invalid_argument("CUDA CV component path must be strictly increasing");
     kmax = prefixes_[j];
   }
+  require(!lda_head || kmax <= kLdaMaxComponents,
+          "batched classification with the LDA head takes up to 32 components");
   folds = 0;
   for (int i = 0; i < n; ++i) {
     if (folds_host[i] < 1) throw std::invalid_argument("invalid CUDA CV fold");
@@ -1261,6 +1462,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   grow(ws->d_test_rows, test_rows.size(), s);
   grow(ws->d_test_off, folds + 1, s);
   grow(ws->d_slot, kmax + 1, s);
+  grow(ws->d_pre, count, s);
   grow(ws->flag, 1, s);
   FPLS_CHECK(cudaMemsetAsync(ws->flag.get(), 0, sizeof(int), s));
   FPLS_CHECK(cudaMemcpyAsync(ws->d_fold.get(), folds_host, sizeof(int) * n, cudaMemcpyHostToDevice, s));
@@ -1268,6 +1470,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
   FPLS_CHECK(cudaMemcpyAsync(ws->d_test_rows.get(), test_rows.data(), sizeof(int) * test_rows.size(), cudaMemcpyHostToDevice, s));
   FPLS_CHECK(cudaMemcpyAsync(ws->d_test_off.get(), test_off.data(), sizeof(int) * (folds + 1), cudaMemcpyHostToDevice, s));
   FPLS_CHECK(cudaMemcpyAsync(ws->d_slot.get(), slot.data(), sizeof(int) * (kmax + 1), cudaMemcpyHostToDevice, s));
+  FPLS_CHECK(cudaMemcpyAsync(ws->d_pre.get(), prefixes_, sizeof(int) * count, cudaMemcpyHostToDevice, s));
   // permutations and labels are copied in, so that captured groups always
   // read them at the workspace's addresses
   perms = nullptr;

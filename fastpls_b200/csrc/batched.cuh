@@ -59,6 +59,9 @@ struct BatchedCv {
   // zero-based class of each base row (device, n) for classification, with
   // Y the one-hot indicator of the classes; null for regression
   const int* class_labels = nullptr;
+  // classification head: false = argmax of the predicted indicators, true =
+  // LDA on the latent scores (per instance, after the last component)
+  bool lda_head = false;
 
   std::vector<int> status;          // per fold: 1 fitted, 2 empty
   std::vector<double> inst_sse;     // (P+1) x folds x prefixes

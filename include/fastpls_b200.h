@@ -339,6 +339,19 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_classification(
 
 /* As above with predictors, responses, folds and permutations already in
  * device memory (prefixes and outputs stay on the host). */
+/* The same with the classification head chosen: lda = 0 is the argmax of
+ * the predicted class indicators (as fastpls_b200_simpls_cv_permutation_
+ * classification), lda = 1 is LDA on the latent scores as the reference's
+ * classification CV offers it (inst/include/fastpls/core/cross_validation.hpp:
+ * 1567-1612, lda.hpp:86-223): per instance, after its last component,
+ * class means and pooled covariance of its training scores over the classes
+ * present in its training rows, the ridge retry grid, and the held-out
+ * argmax of the discriminants. Up to 32 components with the LDA head. */
+FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_classification_head(
+    const void* predictors, const int* labels, const int* folds, const int* permutations,
+    int permutation_count, int precision, int n, int p, int classes, const int* prefixes,
+    int prefix_count, int scaling, int lda, double* accuracy, int* status, char* error,
+    size_t error_capacity);
 FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_device(
     const void* predictors, const void* responses, const int* folds,
     const int* permutations, int permutation_count, int precision, int n,

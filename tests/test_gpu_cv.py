@@ -241,3 +241,32 @@ def test_batched_graph_replay_and_schedules_bit_identical():
         yb = y2 if b == 0 else y2[perms[b - 1]]
         ref = O.cv_regression(x2.astype(np.float64), yb.astype(np.float64), folds, pre)
         assert np.allclose(got["q2"][b], ref["q2"], rtol=1e-5, atol=1e-7), b
+
+
+@pytest.mark.parametrize("digits", [0, 6])
+@pytest.mark.parametrize("scaling", [1, 2])
+def test_batched_classification_lda_head(digits, scaling):
+    """LDA on the latent scores per (fold, permutation) instance, as the
+    reference's classification CV with the LDA head (compacted active
+    classes per training fold): accuracies equal the FP64 oracle's for every
+    permutation and prefix, including a class absent from most training
+    folds."""
+    n, p, classes = 300, 160, 4
+    x, lab = W.latent_classification(n, p, classes, 4, 0.5, 44, dtype=np.float32)
+    lab = lab.copy()
+    lab[11] = 5
+    classes = 5
+    folds = W.uneven_folds(n, 5, 44)
+    perms = W.permutations(n, 3, 44)
+    pre = [1, 2, 4, 7]
+    got = api.cv_permutation_classification(x, lab, classes, folds, perms, pre,
+                                            scaling=scaling, digits=digits, lda=True)
+    x64 = x.astype(np.float64)
+    for b in range(4):
+        lb = lab if b == 0 else lab[perms[b - 1]]
+        want = O.cv_classification(x64, lb, classes, folds, pre, scaling=scaling, head=1)["metrics"]
+        assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
+    # the argmax head on the same inputs is a different classifier
+    arg = api.cv_permutation_classification(x, lab, classes, folds, perms, pre,
+                                            scaling=scaling, digits=digits)
+    assert arg["accuracy"].shape == got["accuracy"].shape
