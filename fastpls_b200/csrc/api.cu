@@ -220,6 +220,11 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
   const int kmax = prefixes[prefix_count - 1];
   const int B = permutation_count + 1;
   std::vector<int> count((size_t)classes);
+  // instances whose training rows hold one class predict that class for every
+  // held-out row (the reference's status 4 fold, cross_validation.hpp:
+  // 1360-1788); they are counted here and not fitted
+  std::vector<unsigned char> single((size_t)B * folds_n, 0);
+  std::vector<double> single_hits((size_t)B * folds_n, 0.0);
   for (int b = 0; b < B; ++b)
     for (int f = 1; f <= folds_n; ++f) {
       std::fill(count.begin(), count.end(), 0);
@@ -235,10 +240,24 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
         ++ntrain;
       }
       if (nheld == 0) continue;
-      int active = 0;
-      for (int c = 0; c < classes; ++c) active += count[c] > 0;
-      if (active < 2)
-        throw std::invalid_argument("batched classification CV needs two classes in every training fold");
+      int active = 0, only = 0;
+      for (int c = 0; c < classes; ++c)
+        if (count[c] > 0) {
+          ++active;
+          only = c + 1;
+        }
+      if (active < 2) {
+        const int predicted = active == 1 ? only : 1;
+        double hits = 0.0;
+        for (int r = 0; r < n; ++r) {
+          if (folds[r] != f) continue;
+          const int src = b == 0 ? r : permutations[(size_t)(b - 1) * n + r];
+          hits += labels[src] == predicted ? 1.0 : 0.0;
+        }
+        single[(size_t)b * folds_n + f - 1] = 1;
+        single_hits[(size_t)b * folds_n + f - 1] = hits;
+        continue;
+      }
       if (kmax >= 4 && (double)ntrain * p * active >= 5.0e8)
         throw std::invalid_argument(
             "batched classification CV does not take candidate blocks (n_train p classes >= 5e8); "
@@ -275,8 +294,17 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
     BatchedCv<T> engine;
     engine.class_labels = L.get();
     engine.lda_head = lda;
+    engine.skip = single;
     engine.run(X.get(), n, p, Y.get(), classes, folds, P.get(), permutation_count, prefixes,
                prefix_count, scaling, s);
+    for (int b = 0; b < B; ++b)
+      for (int f = 0; f < folds_n; ++f)
+        if (single[(size_t)b * folds_n + f])
+          for (int j = 0; j < prefix_count; ++j)
+            engine.inst_sse[((size_t)b * folds_n + f) * prefix_count + j] =
+                single_hits[(size_t)b * folds_n + f];
+    for (int f = 0; f < folds_n; ++f)
+      if (single[f] && engine.status[f] == 1) engine.status[f] = 4;
     engine.accuracy(accuracy);
     if (status)
       for (size_t f = 0; f < engine.status.size(); ++f) status[f] = engine.status[f];

@@ -1564,6 +1564,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
       form_gram(ks.get(), s);
       std::vector<int> fl, pl;
       for (int b = 0; b < B; ++b) {
+        if (!skip.empty() && skip[(size_t)b * folds + f]) continue;
         fl.push_back(f);
         pl.push_back(b - 1);
       }
@@ -1576,6 +1577,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
     for (int b = 0; b < B; ++b)
       for (int f = 0; f < folds; ++f) {
         if (test[f].empty()) continue;
+        if (!skip.empty() && skip[(size_t)b * folds + f]) continue;
         fl.push_back(f);
         pl.push_back(b - 1);
       }
@@ -1623,7 +1625,7 @@ void BatchedCv<T>::accuracy(double* out) const {
     for (int j = 0; j < prefix_count; ++j) {
       double hits = 0.0, rows = 0.0;
       for (int f = 0; f < folds; ++f) {
-        if (status[f] != 1) continue;
+        if (status[f] != 1 && status[f] != 4) continue;
         hits += inst_sse[((size_t)b * folds + f) * prefix_count + j];
         rows += heldout[f];
       }

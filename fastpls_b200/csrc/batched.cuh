@@ -62,8 +62,12 @@ struct BatchedCv {
   // classification head: false = argmax of the predicted indicators, true =
   // LDA on the latent scores (per instance, after the last component)
   bool lda_head = false;
+  // (P+1) x folds, optional: instances the caller handles itself (not run;
+  // their inst_sse entries are the caller's to fill after run)
+  std::vector<unsigned char> skip;
 
-  std::vector<int> status;          // per fold: 1 fitted, 2 empty
+  std::vector<int> status;          // per fold: 1 fitted, 2 empty (the caller may
+                                    // set 4: one class in the training rows)
   std::vector<double> inst_sse;     // (P+1) x folds x prefixes
   std::vector<double> inst_sst;     // (P+1) x folds
   std::vector<int> heldout;         // held-out rows per fold

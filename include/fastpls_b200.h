@@ -325,12 +325,14 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation(
  * folds and zero-based permutations as there; responses are the one-hot
  * indicators of the permuted labels, each fold fit predicts the argmax over
  * the classes present in its training rows (the reference's argmax head,
- * src/cuda_resident_api.cuh:620-745; no LDA). accuracy ((B + 1) x
- * prefix_count, row-major, B = permutation_count, row 0 the observed labels):
- * held-out accuracy per prefix. Every training fold must hold two classes,
- * and n_train p classes must stay below 5e8 when the path has 4 or more
- * components (the reference switches to candidate blocks there); other
- * inputs fail with an error. */
+ * src/cuda_resident_api.cuh:620-745; the LDA head is in
+ * fastpls_b200_simpls_cv_permutation_classification_head). accuracy
+ * ((B + 1) x prefix_count, row-major, B = permutation_count, row 0 the
+ * observed labels): held-out accuracy per prefix. A training fold with one
+ * class predicts that class for its held-out rows (status 4, as the
+ * reference's classification CV). n_train p classes must stay below 5e8 when
+ * the path has 4 or more components (the reference switches to candidate
+ * blocks there); other inputs fail with an error. */
 FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_classification(
     const void* predictors, const int* labels, const int* folds, const int* permutations,
     int permutation_count, int precision, int n, int p, int classes, const int* prefixes,

@@ -191,14 +191,26 @@ def test_batched_classification_ten_classes_bit_exact():
         assert np.array_equal(got["accuracy"][b], want), (b, got["accuracy"][b], want)
 
 
-def test_batched_classification_rejects_single_class_folds():
+@pytest.mark.parametrize("lda", [False, True])
+def test_batched_classification_single_class_folds(lda):
+    """A training fold with one class predicts that class for its held-out
+    rows (the reference's status-4 fold); the other folds are fitted."""
     n = 120
     x, _ = W.latent_classification(n, 40, 2, 3, 0.5, 42, dtype=np.float32)
     folds = W.uneven_folds(n, 4, 42)
     lab = np.ones(n, dtype=np.int32)
     lab[folds == 1] = 2          # class 2 only in fold 1: its training rows hold one class
-    with pytest.raises(api._lib.FastplsError, match="two classes"):
-        api.cv_permutation_classification(x, lab, 2, folds, None, [1, 2])
+    lab[:5] = 2
+    perms = W.permutations(n, 2, 42)
+    pre = [1, 2]
+    got = api.cv_permutation_classification(x, lab, 2, folds, perms, pre, digits=0, lda=lda)
+    x64 = x.astype(np.float64)
+    for b in range(3):
+        lb = lab if b == 0 else lab[perms[b - 1]]
+        want = O.cv_classification(x64, lb, 2, folds, pre, head=1 if lda else 0)
+        assert np.array_equal(got["accuracy"][b], want["metrics"]), b
+        if b == 0:
+            assert list(got["status"]) == list(want["status"])
 
 
 def test_batched_graph_replay_and_schedules_bit_identical():
