@@ -224,6 +224,7 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
   // held-out row (the reference's status 4 fold, cross_validation.hpp:
   // 1360-1788); they are counted here and not fitted
   std::vector<unsigned char> single((size_t)B * folds_n, 0);
+  std::vector<int> blocks((size_t)B * folds_n, 1);
   std::vector<double> single_hits((size_t)B * folds_n, 0.0);
   for (int b = 0; b < B; ++b)
     for (int f = 1; f <= folds_n; ++f) {
@@ -258,10 +259,10 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
         single_hits[(size_t)b * folds_n + f - 1] = hits;
         continue;
       }
-      if (kmax >= 4 && (double)ntrain * p * active >= 5.0e8)
-        throw std::invalid_argument(
-            "batched classification CV does not take candidate blocks (n_train p classes >= 5e8); "
-            "use fastpls_resident_simpls_cv_classification");
+      // the reference's candidate blocks (classification: n_train p classes
+      // >= 5e8 and 4+ components) on this instance's training rows and its
+      // active classes (src/cuda_resident_simpls.cuh:144-153)
+      blocks[(size_t)b * folds_n + f - 1] = simpls_block_size(ntrain, p, active, kmax, true, false);
     }
   std::vector<T> onehot((size_t)n * classes, T(0));
   std::vector<int> zero_based(n);
@@ -295,6 +296,7 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
     engine.class_labels = L.get();
     engine.lda_head = lda;
     engine.skip = single;
+    engine.blocks = blocks;
     engine.run(X.get(), n, p, Y.get(), classes, folds, P.get(), permutation_count, prefixes,
                prefix_count, scaling, s);
     for (int b = 0; b < B; ++b)

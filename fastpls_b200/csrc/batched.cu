@@ -73,6 +73,14 @@ struct InstanceView {
   double* ttr;
   double* tte;
   int max_test;
+  // candidate blocks (classification fits with n_train p classes >= 5e8 and
+  // 4+ components): per instance the block width (1: a direction per
+  // component), the scaled eigenvectors z_j / sqrt(lambda_j) of the block's
+  // start Gram (q x q) and its coefficients C at the block start (n x q);
+  // null when no instance takes blocks
+  const int* blk;
+  double* zblk;
+  double* cblk;
 };
 
 __device__ __forceinline__ int src_row(const InstanceView& v, int perm, int r) {
@@ -212,6 +220,44 @@ __device__ void dominant_z(const InstanceView& v, int i, const double* G, int* f
   __syncthreads();
 }
 
+// The `count` leading eigenpairs of the instance's q x q Gram, by decreasing
+// eigenvalue (ties: lower index first), scaled z_j / sqrt(lambda_j) with the
+// largest |z_j| entry positive, into zblk (q x count) of instance i; zs gets
+// the first (the candidate block of simpls_fit / direction_kernel).
+__device__ void block_z(const InstanceView& v, int i, const double* G, int* flag, int count,
+                        double* A, double* E, double* zs) {
+  const int q = v.q;
+  const double* g = G + (long)i * q * (q + 1) / 2;
+  for (int c = threadIdx.x; c < q; c += blockDim.x)
+    for (int d = 0; d <= c; ++d) {
+      A[c + d * q] = g[c * (c + 1) / 2 + d];
+      A[d + c * q] = g[c * (c + 1) / 2 + d];
+    }
+  __syncthreads();
+  jacobi_eigen(A, E, q);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double* zb = v.zblk + (long)i * q * q;
+    for (int j = 0; j < count; ++j) {
+      int best = -1;
+      for (int k = 0; k < q; ++k)
+        if (best < 0 || A[k + k * q] > A[best + best * q]) best = k;
+      const double lam = A[best + best * q];
+      A[best + best * q] = -INFINITY;  // taken
+      const bool ok = lam > 0.0 && isfinite(lam);
+      if (!ok) flag_error(flag, 1);
+      int arg = 0;
+      for (int k = 1; k < q; ++k)
+        if (fabs(E[k + best * q]) > fabs(E[arg + best * q])) arg = k;
+      const double sgn = E[arg + best * q] < 0.0 ? -1.0 : 1.0;
+      const double inv = ok ? 1.0 / sqrt(lam) : 0.0;
+      for (int k = 0; k < q; ++k) zb[k + (long)j * q] = sgn * E[k + best * q] * inv;
+    }
+    for (int k = 0; k < q; ++k) zs[k] = zb[k];
+  }
+  __syncthreads();
+}
+
 // Dominant direction of instance i: u = C z / sqrt(lambda) (zero on held-out
 // rows, re-centred over the training rows), written to column i of U. When
 // KC0 is given (first component, C = C0) the product K u is formed directly
@@ -222,13 +268,19 @@ __device__ void direction_body(const InstanceView& v, int i, const double* G,
                                double* zs, double* scratch) {
   const int f = v.inst_fold[i];
   const int n = v.n, q = v.q;
-  dominant_z(v, i, G, flag, A, E, zs);
+  const int blk = v.blk ? v.blk[i] : 1;
+  if (blk > 1) block_z(v, i, G, flag, blk, A, E, zs);
+  else dominant_z(v, i, G, flag, A, E, zs);
   const double* c = C + (long)i * n * q;
+  double* cb = blk > 1 ? v.cblk + (long)i * n * q : nullptr;
   double* u = U + (long)i * n;
   double s = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     double val = 0.0;
-    for (int k = 0; k < q; ++k) val = fma(c[r + (long)k * n], zs[k], val);
+    for (int k = 0; k < q; ++k) {
+      if (cb) cb[r + (long)k * n] = c[r + (long)k * n];
+      val = fma(c[r + (long)k * n], zs[k], val);
+    }
     u[r] = val;
     s += val;
   }
@@ -427,7 +479,22 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
       for (int d = 0; d <= cc; ++d) g[cc * (cc + 1) / 2 + d] -= row[cc] * row[d];
   }
   __syncthreads();
-  dominant_z(v, i, G, flag, A, E, zs);
+  // next direction: the dominant pair of the deflated Gram, or within a
+  // candidate block the block start's next eigenpair applied to the block
+  // start's coefficients
+  const int blk = v.blk ? v.blk[i] : 1;
+  const int nxt = a + 1;
+  const bool start = blk > 1 && nxt % blk == 0;
+  const bool inside = blk > 1 && !start;
+  if (start) {
+    block_z(v, i, G, flag, blk, A, E, zs);
+  } else if (inside) {
+    if (threadIdx.x < q) zs[threadIdx.x] = v.zblk[(long)i * q * q + (long)(nxt % blk) * q + threadIdx.x];
+    __syncthreads();
+  } else {
+    dominant_z(v, i, G, flag, A, E, zs);
+  }
+  double* cb = blk > 1 ? v.cblk + (long)i * n * q : nullptr;
   // C -= (w / v) row^T and the next direction u = C z (over t~)
   double su = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
@@ -436,7 +503,8 @@ __global__ void deflate_batched(InstanceView v, const double* Y2,
     for (int cc = 0; cc < q; ++cc) {
       const double cv = fma(-wr, row[cc], c[r + (long)cc * n]);
       c[r + (long)cc * n] = cv;
-      u = fma(cv, zs[cc], u);
+      if (start) cb[r + (long)cc * n] = cv;
+      u = fma(inside ? cb[r + (long)cc * n] : cv, zs[cc], u);
     }
     t[r] = u;
     su += u;
@@ -858,6 +926,8 @@ struct BatchedWorkspace {
   DeviceArray<double> gram, Y64, x64;
   DeviceArray<int> d_fold, d_ntrain, d_test_rows, d_test_off, d_slot, d_pre, flag, perms, labels;
   DeviceArray<double> Ttr, Tte;  // LDA head: training / held-out scores per instance
+  DeviceArray<int> d_blk;          // candidate-block width per instance
+  DeviceArray<double> zblk, cblk;  // candidate blocks: start eigenvectors, start coefficients
   std::vector<GroupGraph> graphs;
 
   BatchedWorkspace() {
@@ -884,10 +954,10 @@ struct BatchedWorkspace {
       L.rhs.scale.release();
     }
     for (auto* a : {&d_if, &d_ip, &amb, &d_fold, &d_ntrain, &d_test_rows, &d_test_off, &d_slot,
-                    &d_pre, &flag, &perms, &labels})
+                    &d_pre, &flag, &perms, &labels, &d_blk})
       a->release();
     for (auto* a : {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram,
-                    &Y64, &x64, &Ttr, &Tte})
+                    &Y64, &x64, &Ttr, &Tte, &zblk, &cblk})
       a->release();
     for (OzakiOperand* o : {&gram_split, &x_split}) {
       o->digits.release();
@@ -910,8 +980,8 @@ struct BatchedWorkspace {
   // next call, so they count as available when a group is sized).
   size_t held_bytes() const {
     size_t b = (d_if.size() + d_ip.size() + amb.size()) * sizeof(int);
-    for (const auto* a :
-         {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0, &gram, &Ttr, &Tte})
+    for (const auto* a : {&C0, &C, &G, &ym, &sst, &sse, &yhat, &Wb, &KWb, &Ws, &U, &Y1, &KC0,
+                          &gram, &Ttr, &Tte, &zblk, &cblk})
       b += a->size() * sizeof(double);
     return b + gram_split.digits.size();
   }
@@ -1196,6 +1266,21 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     grow(ws->Ttr, (size_t)n * kmax * cI, s);
     grow(ws->Tte, (size_t)max_test * kmax * cI, s);
   }
+  // candidate-block widths of this group's instances
+  std::vector<int> hblk(I, 1);
+  bool any_block = false;
+  if (!blocks.empty())
+    for (int k = 0; k < I; ++k) {
+      hblk[k] = std::max(1, blocks[(size_t)(inst_perm[k] + 1) * folds + inst_fold[k]]);
+      any_block = any_block || hblk[k] > 1;
+    }
+  if (any_block) {
+    grow(ws->d_blk, cI, s);
+    grow(ws->zblk, (size_t)q * q * cI, s);
+    grow(ws->cblk, nq * cI, s);
+    FPLS_CHECK(cudaMemcpyAsync(ws->d_blk.get(), hblk.data(), sizeof(int) * I,
+                               cudaMemcpyHostToDevice, s));
+  }
   FPLS_CHECK(cudaMemcpyAsync(ws->d_if.get(), inst_fold.data(), sizeof(int) * I,
                              cudaMemcpyHostToDevice, s));
   FPLS_CHECK(cudaMemcpyAsync(ws->d_ip.get(), inst_perm.data(), sizeof(int) * I,
@@ -1249,6 +1334,9 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
       v.max_test = max_test;
       v.ttr = lda_head ? ws->Ttr.get() + (size_t)L.off * n * kmax : nullptr;
       v.tte = lda_head ? ws->Tte.get() + (size_t)L.off * max_test * kmax : nullptr;
+      v.blk = any_block ? ws->d_blk.get() + L.off : nullptr;
+      v.zblk = any_block ? ws->zblk.get() + (size_t)L.off * q * q : nullptr;
+      v.cblk = any_block ? ws->cblk.get() + (size_t)L.off * nq : nullptr;
       if (digits > 0) {
         // size the digits of the largest right-hand side (K C0: q columns
         // per instance) so the products inside the sequence never allocate
@@ -1265,7 +1353,7 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
     if (use_graph) {
       std::vector<long long> gkey = {n, q, I, kmax, prefix_count, max_test, digits, center,
                                      d.lanes, d.tile_n, class_labels ? 1 : 0, guard ? 1 : 0,
-                                     lda_head ? 1 : 0};
+                                     lda_head ? 1 : 0, any_block ? 1 : 0};
       long long gbits = 0;
       const double gv = argmax_guard();
       std::memcpy(&gbits, &gv, sizeof(gbits));
@@ -1282,7 +1370,8 @@ void BatchedCv<T>::run_group(const std::vector<int>& inst_fold,
             (const void*)ws->d_test_rows.get(), (const void*)ws->d_test_off.get(),
             (const void*)ws->d_slot.get(), (const void*)ws->flag.get(), (const void*)perms,
             (const void*)class_labels, (const void*)ws->d_pre.get(), (const void*)ws->Ttr.get(),
-            (const void*)ws->Tte.get()})
+            (const void*)ws->Tte.get(), (const void*)ws->d_blk.get(), (const void*)ws->zblk.get(),
+            (const void*)ws->cblk.get()})
         gkey.push_back((long long)(uintptr_t)ptr);
       for (int l = 0; l < d.lanes; ++l) {
         gkey.push_back((long long)(uintptr_t)ws->lanes[l].rhs.digits.get());

@@ -65,6 +65,10 @@ struct BatchedCv {
   // (P+1) x folds, optional: instances the caller handles itself (not run;
   // their inst_sse entries are the caller's to fill after run)
   std::vector<unsigned char> skip;
+  // (P+1) x folds, optional: candidate-block width of each instance (the
+  // reference's block rule on its training rows and active classes); empty =
+  // one direction per component everywhere
+  std::vector<int> blocks;
 
   std::vector<int> status;          // per fold: 1 fitted, 2 empty (the caller may
                                     // set 4: one class in the training rows)

@@ -330,9 +330,10 @@ FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation(
  * ((B + 1) x prefix_count, row-major, B = permutation_count, row 0 the
  * observed labels): held-out accuracy per prefix. A training fold with one
  * class predicts that class for its held-out rows (status 4, as the
- * reference's classification CV). n_train p classes must stay below 5e8 when
- * the path has 4 or more components (the reference switches to candidate
- * blocks there); other inputs fail with an error. */
+ * reference's classification CV). Where n_train p classes reaches 5e8 and the
+ * path has 4 or more components, an instance takes min(64, components, p,
+ * classes) directions from one decomposition per block, as the reference's
+ * candidate blocks (src/cuda_resident_simpls.cuh:144-153). */
 FASTPLS_B200_API int fastpls_b200_simpls_cv_permutation_classification(
     const void* predictors, const int* labels, const int* folds, const int* permutations,
     int permutation_count, int precision, int n, int p, int classes, const int* prefixes,
