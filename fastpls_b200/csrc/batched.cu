@@ -1533,6 +1533,7 @@ void BatchedCv<T>::run(const T* X_, int n_, int p_, const T* Y_, int q_,
     ws = own.get();
   }
   last_batched_stats() = BatchedStats{};
+  if (digits > 0) ozaki_configure_kernels();  // attributes are not set inside a capture
   const cudaStream_t s = ws->main;
   // the caller's earlier work (input copies) before ours; ours before its later work
   FPLS_CHECK(cudaEventRecord(ws->fork, caller));

@@ -986,6 +986,16 @@ TileChoice pick_tile(int M, int N, int tile_n, int pair) {
 }
 
 template <int BN>
+bool configure_gemm() {
+  static const bool configured = [] {
+    FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel<BN>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
+    return true;
+  }();
+  return configured;
+}
+
+template <int BN>
 void launch_gemm(const OzakiOperand& a, const OzakiOperand& b, OzArgs args, long tiles,
                  cudaStream_t stream) {
   const int S = a.slices;
@@ -993,12 +1003,7 @@ void launch_gemm(const OzakiOperand& a, const OzakiOperand& b, OzArgs args, long
   args.stages = std::min(OZ_MAX_STAGES, OZ_DATA / stage_bytes);
   require(args.stages >= 2, "int8 split product: stages do not fit shared memory");
   const size_t smem = (size_t)args.stages * stage_bytes + 1024;
-  static const bool configured = [] {
-    FPLS_CHECK(cudaFuncSetAttribute(ozaki_gemm_kernel<BN>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_DATA + 1024));
-    return true;
-  }();
-  (void)configured;
+  configure_gemm<BN>();
   // int32 accumulators stay exact while (digit pairs on a diagonal) x k x 127^2 < 2^31
   const int kb_total = a.k_p / OZ_BK;
   const int seg_bytes = std::max(OZ_KPAD, (int)((2147483647LL / (16129LL * S)) / OZ_KPAD * OZ_KPAD));
@@ -1054,6 +1059,12 @@ void launch_gemm_pair(const OzakiOperand& a, const OzakiOperand& b, OzArgs args,
 }
 
 }  // namespace
+
+void ozaki_configure_kernels() {
+  configure_gemm<128>();
+  configure_gemm<192>();
+  configure_gemm<256>();
+}
 
 void ozaki_profile_enable(bool on) { oz_timing().enabled = on; }
 

@@ -87,6 +87,9 @@ struct OzakiWaitTest {
 OzakiWaitTest& ozaki_wait_test();
 
 // Timing of the last ozaki_gemm launches (CUDA events), for benchmarks.
+// Sets the kernels' launch attributes once (before any stream capture).
+void ozaki_configure_kernels();
+
 void ozaki_profile_enable(bool on);
 bool ozaki_profile_enabled();
 void ozaki_profile_read(double* ms, double* int8_ops, unsigned long long* launches);
