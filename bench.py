@@ -314,29 +314,46 @@ def _kw(r):
     return dict(kernel="rbf", gamma=1.0 / r["p"]) if r["method"] == "kernelpls" else {}
 
 
+def _describe(r):
+    if r["kind"] != "fit":
+        return f"predict rows={r['x'].shape[0]} p={r['src']['p']}"
+    return (f"{r['method']} n={r['x'].shape[0]} p={r['p']} q={r['q']} a={r['ncomp']} "
+            f"{'classification' if r['labels'] is not None else 'regression'}")
+
+
 def run_plain(lib_api, reqs):
-    """Each request through the drop-in entry points, one at a time."""
+    """Each request through the drop-in entry points, one at a time. A
+    request that fails is recorded (count, first message) and its
+    predictions are skipped."""
     kw = _kw
     models = {}
     plain_lat = []
+    failed = []
     t0 = time.perf_counter()
     for i, r in enumerate(reqs):
         s = time.perf_counter()
-        if r["kind"] == "fit":
-            models[id(r)] = lib_api.fit_resident(
-                r["x"], r["y"], labels=r["labels"], classes=r["classes"],
-                ncomp=r["ncomp"], method=r["method"], precision=32, **kw(r))
-        else:
-            src = r["src"]
-            models[id(src)].predict_path(r["x"], [src["ncomp"]])
+        try:
+            if r["kind"] == "fit":
+                models[id(r)] = lib_api.fit_resident(
+                    r["x"], r["y"], labels=r["labels"], classes=r["classes"],
+                    ncomp=r["ncomp"], method=r["method"], precision=32, **kw(r))
+            else:
+                src = r["src"]
+                if id(src) in models:
+                    models[id(src)].predict_path(r["x"], [src["ncomp"]])
+        except Exception as exc:  # recorded in the bench line
+            failed.append(f"{_describe(r)}: {exc}")
         plain_lat.append(1000 * (time.perf_counter() - s))
     plain_time = time.perf_counter() - t0
     for mdl in models.values():
         mdl.close()
     fits = sum(1 for r in reqs if r["kind"] == "fit")
-    return {"plain_fits_per_s": fits / plain_time,
-            "plain_p50_ms": float(np.percentile(plain_lat, 50)),
-            "plain_p99_ms": float(np.percentile(plain_lat, 99))}
+    out = {"plain_fits_per_s": fits / plain_time,
+           "plain_p50_ms": float(np.percentile(plain_lat, 50)),
+           "plain_p99_ms": float(np.percentile(plain_lat, 99))}
+    if failed:
+        out["plain_failed"] = {"count": len(failed), "first": failed[0]}
+    return out
 
 
 def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
@@ -366,17 +383,29 @@ def run_served(lib_api, reqs, mean_gap_ms=2.0, workers=4):
         tickets.append(t)
         submit_t.append(time.perf_counter())
     lat = []
+    failed = []
     for t in tickets:
-        _, qms, sms = srv.wait(t)
-        lat.append(qms + sms)
+        try:
+            _, qms, sms = srv.wait(t)
+            lat.append(qms + sms)
+        except Exception as exc:  # recorded in the bench line
+            failed.append(str(exc))
     served_time = time.perf_counter() - t0
     for t in fit_tickets.values():
-        srv.release(t)
+        try:
+            srv.release(t)
+        except Exception:
+            pass
+    batches = srv.batch_stats()
     srv.close()
     fits = sum(1 for r in reqs if r["kind"] == "fit")
-    return {"mean_gap_ms": mean_gap_ms, "fits_per_s": fits / served_time,
-            "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99))}
+    out = {"mean_gap_ms": mean_gap_ms, "fits_per_s": fits / served_time,
+           "p50_ms": float(np.percentile(lat, 50)) if lat else None,
+           "p99_ms": float(np.percentile(lat, 99)) if lat else None,
+           "batched_launches": batches["launches"], "batched_fits": batches["fits"]}
+    if failed:
+        out["failed"] = {"count": len(failed), "first": failed[0]}
+    return out
 
 
 def int8_peak_tops(torch, dev):

@@ -36,7 +36,10 @@ def test_simpls_regression_vs_reference(scaling):
     assert O.rel_err(R * sg, g["R"]) < 1e-9
     assert O.rel_err(Q * sg, g["Q"]) < 1e-9
     assert O.rel_err(T * sg, g["T"]) < 1e-9
-    assert O.rel_err(m.export(3), g["centre"]) < 1e-12
+    # the fixture's X is column-centred already: its means are rounding
+    # noise, compared in absolute terms against the scale of X
+    xs = np.abs(g["x"]).max()
+    assert np.abs(m.export(3) - g["centre"]).max() < 1e-13 * xs
     assert O.rel_err(m.export(4), g["scale"]) < 1e-12
     assert O.rel_err(m.export(5), g["ymean"]) < 1e-12
     m.close()
