@@ -238,6 +238,7 @@ __device__ void block_z(const InstanceView& v, int i, const double* G, int* flag
   __syncthreads();
   if (threadIdx.x == 0) {
     double* zb = v.zblk + (long)i * q * q;
+    double inv0 = 0.0;
     for (int j = 0; j < count; ++j) {
       int best = -1;
       for (int k = 0; k < q; ++k)
@@ -245,12 +246,15 @@ __device__ void block_z(const InstanceView& v, int i, const double* G, int* flag
       const double lam = A[best + best * q];
       A[best + best * q] = -INFINITY;  // taken
       const bool ok = lam > 0.0 && isfinite(lam);
-      if (!ok) flag_error(flag, 1);
+      // a later candidate beyond the rank of the Gram takes the leading
+      // pair's scale (the direction's scale cancels in the scores)
+      if (!ok && j == 0) flag_error(flag, 1);
       int arg = 0;
       for (int k = 1; k < q; ++k)
         if (fabs(E[k + best * q]) > fabs(E[arg + best * q])) arg = k;
       const double sgn = E[arg + best * q] < 0.0 ? -1.0 : 1.0;
-      const double inv = ok ? 1.0 / sqrt(lam) : 0.0;
+      const double inv = ok ? 1.0 / sqrt(lam) : inv0;
+      if (j == 0) inv0 = inv;
       for (int k = 0; k < q; ++k) zb[k + (long)j * q] = sgn * E[k + best * q] * inv;
     }
     for (int k = 0; k < q; ++k) zs[k] = zb[k];

@@ -134,14 +134,22 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
   jacobi_eigen(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
+    double inv0 = 0.0;
     for (int j = 0; j < count; ++j) {
       int best = -1;
       for (int k = 0; k < m; ++k)
         if (best < 0 || A[k + k * m] > A[best + best * m]) best = k;
       const double lam = A[best + best * m];
       A[best + best * m] = -INFINITY;  // taken (A is scratch after the solve)
-      if (!(lam > 0.0) || !isfinite(lam)) flag_error(flag, 1);
-      const double inv = (lam > 0.0 && isfinite(lam)) ? 1.0 / sqrt(lam) : 0.0;
+      const bool ok = lam > 0.0 && isfinite(lam);
+      // The leading pair must exist (S not zero). A later candidate of a
+      // block wider than the rank of S (a block of q classes, rank q - 1)
+      // has a numerically zero eigenvalue: it takes the leading pair's scale
+      // (R and T do not depend on the scale of r), as the reference's sketch
+      // yields some unit direction there instead of failing.
+      if (!ok && j == 0) flag_error(flag, 1);
+      const double inv = ok ? 1.0 / sqrt(lam) : inv0;
+      if (j == 0) inv0 = inv;
       // deterministic sign: largest-magnitude entry of z positive
       int arg = 0;
       for (int k = 1; k < m; ++k)

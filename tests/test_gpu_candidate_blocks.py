@@ -110,3 +110,26 @@ def test_massive_fp32_regression_cross_covariance():
         assert O.rel_err(R[:, :k] @ Qm[:, :k].T, ref["R"][:, :k] @ ref["Q"][:, :k].T) < 1e-7, k
     for j, k in enumerate(pre):
         assert O.rel_err(pred[j], O.simpls_predict(ref, x64[:20], k)) < 1e-7, k
+
+
+def test_block_wider_than_the_rank_completes():
+    """A classification block of q classes is one wider than the rank q - 1
+    of the centred label cross-product: the last candidate of the block has a
+    numerically zero eigenvalue. The fit completes (as the reference's does,
+    with whatever unit direction its sketch gives there), and every prefix
+    within the rank matches the oracle."""
+    n, p, q, a = 4000, 25000, 6, 8
+    x, lab = W.latent_classification(n, p, q, 5, 0.5, 73, dtype=np.float64)
+    present = np.unique(lab)
+    assert present.size == q
+    assert O.simpls_block_size(n, p, q, a, True) == q
+    model = api.fit_resident(x, labels=lab, classes=q, ncomp=a, precision=64)
+    assert model.controls()["block"] == q
+    xt, _ = W.latent_classification(300, p, q, 5, 0.5, 74, dtype=np.float64)
+    pre = [1, 3, q - 1]
+    pred = model.predict_path(xt, pre).astype(np.float64)
+    ref = O.simpls_fit(x, labels=lab, classes=q, ncomp=a, scaling=1)
+    for j, k in enumerate(pre):
+        assert O.rel_err(pred[j], O.simpls_predict(ref, xt, k)) < 1e-8, k
+    assert np.all(np.isfinite(model.export(0)))
+    model.close()

@@ -289,8 +289,9 @@ def test_batched_classification_candidate_blocks(digits):
     """Training folds with n_train p classes >= 5e8 and 4+ components take
     candidate blocks (min(64, components, p, classes) directions from one
     decomposition, src/cuda_resident_simpls.cuh:144-153): 2400 x 8000 training
-    rows with 30 classes give blocks of 8. Accuracies equal the FP64 oracle
-    run with the same block rule, for the observed and permuted labels."""
+    rows with 28 active classes and 10 components take all ten directions
+    from the first decomposition. Accuracies equal the FP64 oracle run with
+    the same block rule, for the observed and permuted labels."""
     n, p, classes = 3000, 8000, 30
     x, lab = W.latent_classification(n, p, classes, 12, 0.5, 45, dtype=np.float32)
     folds = W.uneven_folds(n, 5, 45)
@@ -299,7 +300,7 @@ def test_batched_classification_candidate_blocks(digits):
     ntr = n - int(np.sum(folds == 1))
     active = np.unique(lab[folds != 1]).size
     assert ntr * p * active >= 5e8
-    assert O.simpls_block_size(ntr, p, active, 10, True) == 8
+    assert O.simpls_block_size(ntr, p, active, 10, True) == 10
     got = api.cv_permutation_classification(x, lab, classes, folds, perms, pre, digits=digits)
     x64 = x.astype(np.float64)
     for b in range(3):
