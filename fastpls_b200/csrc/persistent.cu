@@ -123,11 +123,20 @@ __device__ __forceinline__ void col_range(int p, int C, int c, int& j0, int& j1)
   j1 = min(p, j0 + per);
 }
 
-// Sum over the C per-CTA partials of slot `k` (stride cslots), CTA order.
-__device__ __forceinline__ double sum_slots(const Fit& f, int k) {
-  double s = 0.0;
-  for (int c = 0; c < f.C; ++c) s += __ldcg(f.cpart + (long)c * f.cslots + k);
-  return s;
+// Sums over the C per-CTA partials of slots 0 .. count-1 (stride cslots),
+// by the whole CTA: warp w takes slots w, w + 8, ...; lane l adds the
+// partials of CTAs l, l + 32, ... in order, then the warp's shuffle tree
+// (a fixed order). store(k, sum) runs on lane 0.
+template <class F>
+__device__ __forceinline__ void reduce_slots(const Fit& f, int count, F&& store) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = warp; k < count; k += PT / 32) {
+    double s = 0.0;
+#pragma unroll 4
+    for (int c = lane; c < f.C; c += 32) s += __ldcg(f.cpart + (long)c * f.cslots + k);
+    s = warp_sum(s);
+    if (lane == 0) store(k, s);
+  }
 }
 
 template <class T> struct Vec16;
@@ -158,23 +167,6 @@ template <> struct Vec16<bf16> {
   }
 };
 
-template <class T> struct Pair2;
-template <> struct Pair2<float> {
-  using type = float2;
-  static __device__ __forceinline__ double lo(type v) { return v.x; }
-  static __device__ __forceinline__ double hi(type v) { return v.y; }
-};
-template <> struct Pair2<double> {
-  using type = double2;
-  static __device__ __forceinline__ double lo(type v) { return v.x; }
-  static __device__ __forceinline__ double hi(type v) { return v.y; }
-};
-template <> struct Pair2<bf16> {
-  using type = __nv_bfloat162;
-  static __device__ __forceinline__ double lo(type v) { return __low2float(v); }
-  static __device__ __forceinline__ double hi(type v) { return __high2float(v); }
-};
-
 // P2: partial scores of one item (row tile x column chunk k): thread rows
 // i .. i + VEC - 1, columns of the chunk in order.
 template <class T>
@@ -197,13 +189,13 @@ __device__ void xr_item(const Fit& f, const T* X, int tile, int k, double* rts) 
 #pragma unroll
     for (int u = 0; u < VN; ++u) acc[u] = 0.0;
     int j = 0;
-    for (; j + 3 < cols; j += 4) {
-      V x[4];
+    for (; j + 7 < cols; j += 8) {
+      V x[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 8; ++u)
         x[u] = __ldg(reinterpret_cast<const V*>(base + (long)(j + u) * f.ld));
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         double e[VN];
         Vec16<T>::get(x[u], e);
         const double w = rts[j + u];
@@ -231,9 +223,45 @@ __device__ void xr_item(const Fit& f, const T* X, int tile, int k, double* rts) 
   }
 }
 
-// P4: loading partials of one item (row chunk kc x 32 columns from jt*32):
-// warp per column, lanes over row pairs (or rows), t rows staged in shared
-// memory.
+// Eight consecutive rows of a column as FP64 (16-byte aligned source): one
+// 16-byte load for BF16, two for FP32, four for FP64.
+template <class T> struct Oct;
+template <> struct Oct<bf16> {
+  static __device__ __forceinline__ void load(const bf16* p, double (&x)[8]) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      x[2 * k] = (double)__uint_as_float(w[k] << 16);
+      x[2 * k + 1] = (double)__uint_as_float(w[k] & 0xffff0000u);
+    }
+  }
+};
+template <> struct Oct<float> {
+  static __device__ __forceinline__ void load(const float* p, double (&x)[8]) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+  }
+};
+template <> struct Oct<double> {
+  static __device__ __forceinline__ void load(const double* p, double (&x)[8]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = __ldg(reinterpret_cast<const double2*>(p) + k);
+      x[2 * k] = v.x;
+      x[2 * k + 1] = v.y;
+    }
+  }
+};
+
+// P4: loading partials of one item (row chunk kc x 32 columns from jt*32).
+// Warp w owns columns w, w + 8, w + 16, w + 24 of the tile and walks them
+// together; lane l takes the row octets l, l + 32, ... (8 consecutive rows
+// per load, in row order), then the leftover rows one per lane; the t rows
+// are staged in shared memory. The summation order depends only on the
+// row count, so it is the same for every storage type.
 template <class T>
 __device__ void xtv_item(const Fit& f, const T* X, int kc, int jt, const double* tcol,
                          double* ts) {
@@ -243,38 +271,38 @@ __device__ void xtv_item(const Fit& f, const T* X, int kc, int jt, const double*
   for (int r = threadIdx.x; r < rows; r += PT) ts[r] = __ldcg(tcol + r0 + r);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int jj = warp; jj < 32; jj += PT / 32) {
-    const int j = jt * 32 + jj;
-    if (j >= f.p) break;
-    const T* col = X + (long)j * f.ld + r0;
-    double acc = 0.0;
-    if (f.pair) {
-      using P = Pair2<T>;
-      const typename P::type* col2 = reinterpret_cast<const typename P::type*>(col);
-      const int pairs = rows >> 1;
-      int q = lane;
-      for (; q + 96 < pairs; q += 128) {
-        typename P::type x[4];
+  const T* col[4];
+  bool ok[4];
+  double acc[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = __ldg(col2 + q + 32 * u);
+  for (int c = 0; c < 4; ++c) {
+    const int j = jt * 32 + warp + 8 * c;
+    ok[c] = j < f.p;
+    col[c] = X + (long)(ok[c] ? j : 0) * f.ld + r0;
+    acc[c] = 0.0;
+  }
+  const int octs = f.oct ? rows >> 3 : 0;
+  for (int o = lane; o < octs; o += 32) {
+    const double* tv = ts + 8 * o;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int r = 2 * (q + 32 * u);
-          acc = fma(P::lo(x[u]), ts[r], acc);
-          acc = fma(P::hi(x[u]), ts[r + 1], acc);
-        }
-      }
-      for (; q < pairs; q += 32) {
-        const typename P::type x = __ldg(col2 + q);
-        acc = fma(P::lo(x), ts[2 * q], acc);
-        acc = fma(P::hi(x), ts[2 * q + 1], acc);
-      }
-      if ((rows & 1) && lane == 0) acc = fma(as_f64(col[rows - 1]), ts[rows - 1], acc);
-    } else {
-      for (int r = lane; r < rows; r += 32) acc = fma(as_f64(col[r]), ts[r], acc);
+    for (int c = 0; c < 4; ++c) {
+      if (!ok[c]) continue;
+      double x[8];
+      Oct<T>::load(col[c] + 8 * o, x);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) acc[c] = fma(x[e], tv[e], acc[c]);
     }
-    acc = warp_sum(acc);
-    if (lane == 0) f.ppart[(long)kc * f.p + j] = acc;
+  }
+  for (int r = 8 * octs + lane; r < rows; r += 32) {
+    const double tv = ts[r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (ok[c]) acc[c] = fma(as_f64(col[c][r]), tv, acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double v = warp_sum(acc[c]);
+    if (lane == 0 && ok[c]) f.ppart[(long)kc * f.p + jt * 32 + warp + 8 * c] = v;
   }
 }
 
@@ -335,8 +363,7 @@ __global__ void __launch_bounds__(PT, 2)
     // B0: Gram of the deflated S (after the first component) and direction
     if (!group_sync(f, flag, [&] {
           if (a > 0) {
-            const int G = m * (m + 1) / 2;
-            for (int k = tid; k < G; k += PT) f.gpk[k] = sum_slots(f, k);
+            reduce_slots(f, m * (m + 1) / 2, [&](int k, double v) { f.gpk[k] = v; });
             __syncthreads();
             __threadfence();
           }
@@ -358,7 +385,7 @@ __global__ void __launch_bounds__(PT, 2)
     acc = cta_sum(acc, red);
     if (tid == 0) f.cpart[(long)cta * f.cslots] = acc;
     if (!group_sync(f, flag, [&] {
-          if (tid == 0) f.scal[SC_C] = sum_slots(f, 0);
+          reduce_slots(f, 1, [&](int, double v) { f.scal[SC_C] = v; });
         }))
       return;
     // P2: score partials, items (row tile, column chunk)
@@ -374,9 +401,17 @@ __global__ void __launch_bounds__(PT, 2)
       double* tcol = f.T + (long)a * n;
       double s2 = 0.0, s1 = 0.0;
       for (int i = cta * PT + tid; i < n; i += C * PT) {
-        double s = 0.0;
-        for (int k = 0; k < f.kt; ++k) s += __ldcg(f.tpart + (long)k * n + i);
-        const double t = s - cc;
+        // four interleaved partial sums (more loads in flight), fixed order
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        int k = 0;
+        for (; k + 3 < f.kt; k += 4) {
+          q0 += __ldcg(f.tpart + (long)k * n + i);
+          q1 += __ldcg(f.tpart + (long)(k + 1) * n + i);
+          q2 += __ldcg(f.tpart + (long)(k + 2) * n + i);
+          q3 += __ldcg(f.tpart + (long)(k + 3) * n + i);
+        }
+        for (; k < f.kt; ++k) q0 += __ldcg(f.tpart + (long)k * n + i);
+        const double t = ((q0 + q1) + (q2 + q3)) - cc;
         tcol[i] = t;
         s2 = fma(t, t, s2);
         s1 += t;
@@ -389,10 +424,7 @@ __global__ void __launch_bounds__(PT, 2)
       }
     }
     if (!group_sync(f, flag, [&] {
-          if (tid == 0) {
-            f.scal[SC_T2] = sum_slots(f, 0);
-            f.scal[SC_ST] = sum_slots(f, 1);
-          }
+          reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
         }))
       return;
     // P4: loading partials, items (row chunk, 32-column tile)
@@ -418,8 +450,16 @@ __global__ void __launch_bounds__(PT, 2)
     double* rs = psm + 2048;   // R values
     for (int jl = tid; jl < j1 - j0; jl += PT) {
       const int j = j0 + jl;
-      double pr = 0.0;
-      for (int k = 0; k < f.kp; ++k) pr += __ldcg(f.ppart + (long)k * p + j);
+      double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+      int k = 0;
+      for (; k + 3 < f.kp; k += 4) {
+        q0 += __ldcg(f.ppart + (long)k * p + j);
+        q1 += __ldcg(f.ppart + (long)(k + 1) * p + j);
+        q2 += __ldcg(f.ppart + (long)(k + 2) * p + j);
+        q3 += __ldcg(f.ppart + (long)(k + 3) * p + j);
+      }
+      for (; k < f.kp; ++k) q0 += __ldcg(f.ppart + (long)k * p + j);
+      const double pr = (q0 + q1) + (q2 + q3);
       const double pj = (pr - f.mean[j] * sum_t) / f.scale[j] * inv_t;
       const double rj = __ldcg(f.r + j) * inv_t;
       f.pv[j] = pj;
@@ -445,14 +485,14 @@ __global__ void __launch_bounds__(PT, 2)
       }
     }
     if (!group_sync(f, flag, [&] {
-          for (int k = tid; k < a + m; k += PT) {
-            const double s = sum_slots(f, k);
-            if (k < a) f.scal[SC_H + k] = s;
-            else {
-              f.scal[SC_Q + k - a] = s;
-              f.Q[(k - a) + (long)a * m] = s;
+          reduce_slots(f, a + m, [&](int k, double v) {
+            if (k < a) {
+              f.scal[SC_H + k] = v;
+            } else {
+              f.scal[SC_Q + k - a] = v;
+              f.Q[(k - a) + (long)a * m] = v;
             }
-          }
+          });
         }))
       return;
     // P6: v = p - V h; partial v.v and S^T v
@@ -482,11 +522,10 @@ __global__ void __launch_bounds__(PT, 2)
       if (tid == 0) f.cpart[(long)cta * f.cslots] = vvp;
     }
     if (!group_sync(f, flag, [&] {
-          for (int k = tid; k < 1 + m; k += PT) {
-            const double s = sum_slots(f, k);
-            if (k == 0) f.scal[SC_VV] = s;
-            else f.scal[SC_SV + k - 1] = s;
-          }
+          reduce_slots(f, 1 + m, [&](int k, double v) {
+            if (k == 0) f.scal[SC_VV] = v;
+            else f.scal[SC_SV + k - 1] = v;
+          });
         }))
       return;
     // P7: V[:, a], deflate S, partial Gram of the deflated S; T[:, a] /= |t|
@@ -640,7 +679,9 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   constexpr int VN = sizeof(T) == 2 ? 8 : (sizeof(T) == 4 ? 4 : 2);
   const bool aligned16 = reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % VN == 0;
   f.vec = aligned16 ? VN : 1;
-  f.pair = (reinterpret_cast<uintptr_t>(X) % (2 * sizeof(T)) == 0 && ld % 2 == 0) ? 1 : 0;
+  // octet loads in the loading pass: the same condition for every storage
+  // type (so BF16 and FP32 storage of the same values sum in one order)
+  f.oct = (reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % 8 == 0) ? 1 : 0;
   f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2));
   const PersistentWaitTest& wt = persistent_wait_test();
   f.barrier_cycles = wt.cycles > 0 ? wt.cycles : kBarrierCycles;

@@ -33,7 +33,7 @@ struct PersistentFit {
   int cc, kt;               // t pass: columns per chunk, chunks
   int rc, kp;               // loading pass: rows per chunk, chunks
   int vec;                  // rows per 16-byte load in the t pass (1: scalar)
-  int pair;                 // row pairs per lane in the loading pass
+  int oct;                  // 8-row loads per lane in the loading pass
   int cslots;               // per-CTA partial slots
   long long barrier_cycles; // bound of each barrier wait
   int absent_cta;           // test of the bounded waits: this CTA never arrives (-1: none)
