@@ -329,6 +329,7 @@ void cv_classification(int method, const T* predictors, const int* labels,
       FPLS_CHECK(cudaMemsetAsync(ws.flag.get(), 0, sizeof(int), s));
       DeviceModel model;
       model.classification = true;
+      model.label_view = lab_tr.get();
       model.ymean.allocate(c, s);
       prepare_responses<T>(nullptr, lab_tr.get(), ntr, c, Yc.get(), model.ymean.get(), ycsum.get(), ws.flag.get(), s);
       fit_method<T>(method, Xtr.get(), ntr, p, Yc.get(), ycsum.get(), c, maximum_prefix, scaling, model, ws, s);

@@ -487,7 +487,11 @@ void compute_crossprod(const T* X, int n, int p, long ld, const double* Yc,
   double* sum = moments.get();
   double* sumsq = sum + p;
   double* cross = sumsq + p;
-  column_moments<T>(X, n, p, ld, Yc, m, sum, sumsq, cross, ws.stream_partial, stream);
+  if (model.label_view && m <= kClassMomentsMaxClasses)
+    class_moments<T>(X, n, p, ld, model.label_view, m, model.ymean.get(), sum, sumsq, cross,
+                     ws.stream_partial, stream);
+  else
+    column_moments<T>(X, n, p, ld, Yc, m, sum, sumsq, cross, ws.stream_partial, stream);
   const unsigned gp = std::min<unsigned>(ceil_div(p, TB), 8 * num_sms());
   finish_moments<<<gp, TB, 0, stream>>>(sum, sumsq, cross, ycsum, n, p, m,
                                         scaling, model.mean.get(),

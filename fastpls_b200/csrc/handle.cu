@@ -481,6 +481,7 @@ class TypedHandle final : public ResidentHandle {
       model_.class_counts.assign(q, 0);
       for (int i = 0; i < n; ++i)
         if (rq_.labels[i] >= 1 && rq_.labels[i] <= q) ++model_.class_counts[rq_.labels[i] - 1];
+      model_.label_view = model_.labels.get();
     } else {
       y.allocate((size_t)n * q, stream_);
       FPLS_CHECK(cudaMemcpyAsync(y.get(), rq_.y, sizeof(TO) * n * q, cudaMemcpyHostToDevice, stream_));

@@ -48,6 +48,15 @@ void column_moments(const T* X, int n, int p, long ld, const double* Yc, int m,
                     double* sum, double* sumsq, double* cross,
                     DeviceArray<double>& scratch, cudaStream_t stream);
 
+// Classification: sum[j], sumsq[j] and cross[j + c*p] = X^T (onehot - prior)
+// from one-based labels (n), classes m <= kClassMomentsMaxClasses, in one
+// pass over X (per-class column sums minus prior * column sum).
+constexpr int kClassMomentsMaxClasses = 32;
+template <class T>
+void class_moments(const T* X, int n, int p, long ld, const int* labels, int m,
+                   const double* prior, double* sum, double* sumsq, double* cross,
+                   DeviceArray<double>& scratch, cudaStream_t stream);
+
 // out[i + c*n] = sum_j X[i,j] * R[j + c*ldr] - offset[c]   (c < nb)
 // (scores of a scaled/centred X folded into R and offset). FP64 result.
 template <class T>

@@ -41,6 +41,9 @@ struct DeviceModel {
   DeviceArray<double> sigma;               // PLS-SVD singular values (a)
   DeviceArray<double> W;                   // PLS-SVD per-prefix weights (a x m x a)
   DeviceArray<int> labels;                 // training labels (classification)
+  const int* label_view = nullptr;         // labels of the rows being fitted
+                                           // (one-based, not owned): the
+                                           // class-sum cross-product pass
   std::vector<int> class_counts;           // host copy (classification)
   // kernel PLS: input standardisation (in_p columns), standardised training
   // rows, their squared norms, training kernel column means (+ grand mean)

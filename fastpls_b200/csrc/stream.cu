@@ -557,6 +557,135 @@ void column_moments(const T* X, int n, int p, long ld, const double* Yc, int m,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Column moments with one-based class labels (classification): per column
+// the sum, the sum of squares and the per-class sums, in one pass over X.
+// Block = 8 warps over a 32-column tile and a chunk of rows whose labels are
+// staged in shared memory; each lane keeps its own class accumulators in
+// shared memory (acc[warp][class][lane]), so an element costs one add into
+// its class's slot instead of m products with staged responses. partial
+// layout: [chunk][j][slot], slots = classes, sum, sumsq.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    class_moments_kernel(const T* __restrict__ X, int n, int p, long ld,
+                         const int* __restrict__ labels, int m, int rc,
+                         double* __restrict__ partial) {
+  extern __shared__ double csm[];
+  int* lab = reinterpret_cast<int*>(csm);                  // rc labels
+  double* acc = csm + (rc + 1) / 2;                        // 8 x m x 32
+  const int chunk = blockIdx.y;
+  const int r0 = chunk * rc;
+  const int rows = min(rc, n - r0);
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) lab[r] = labels[r0 + r] - 1;
+  __syncthreads();
+  const int slots = m + 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* my = acc + (long)warp * m * 32;
+  for (int jj = warp; jj < 32; jj += kThreads / 32) {
+    const int j = blockIdx.x * 32 + jj;
+    if (j >= p) break;
+    for (int c = 0; c < m; ++c) my[c * 32 + lane] = 0.0;
+    __syncwarp();
+    const T* col = X + (long)j * ld + r0;
+    double s = 0.0, ss = 0.0;
+    int r = lane;
+    for (; r + 96 < rows; r += 128) {
+      double x[4];
+      int l[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        x[u] = as_f64(col[r + 32 * u]);
+        l[u] = lab[r + 32 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        s += x[u];
+        ss = fma(x[u], x[u], ss);
+        if (l[u] >= 0 && l[u] < m) my[l[u] * 32 + lane] += x[u];
+      }
+    }
+    for (; r < rows; r += 32) {
+      const double x = as_f64(col[r]);
+      const int l = lab[r];
+      s += x;
+      ss = fma(x, x, ss);
+      if (l >= 0 && l < m) my[l * 32 + lane] += x;
+    }
+    __syncwarp();
+    double* out = partial + ((long)chunk * p + j) * slots;
+    for (int c = 0; c < m; ++c) {
+      const double v = warp_sum(my[c * 32 + lane]);
+      if (lane == 0) out[c] = v;
+    }
+    s = warp_sum(s);
+    ss = warp_sum(ss);
+    if (lane == 0) {
+      out[m] = s;
+      out[m + 1] = ss;
+    }
+    __syncwarp();
+  }
+}
+
+// cross[j + c p] = classsum[j, c] - prior[c] * colsum[j] (= X^T (onehot -
+// prior)), sum and sumsq, from the per-chunk partials.
+__global__ void class_moments_finish(const double* __restrict__ partial, int chunks, int p,
+                                     int m, const double* __restrict__ prior, double* sum,
+                                     double* sumsq, double* cross) {
+  const int slots = m + 2;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p; j += gridDim.x * blockDim.x) {
+    double s = 0.0, ss = 0.0;
+    for (int k = 0; k < chunks; ++k) {
+      s += partial[((long)k * p + j) * slots + m];
+      ss += partial[((long)k * p + j) * slots + m + 1];
+    }
+    sum[j] = s;
+    sumsq[j] = ss;
+    for (int c = 0; c < m; ++c) {
+      double v = 0.0;
+      for (int k = 0; k < chunks; ++k) v += partial[((long)k * p + j) * slots + c];
+      cross[j + (long)c * p] = v - prior[c] * s;
+    }
+  }
+}
+
+template <class T>
+void class_moments(const T* X, int n, int p, long ld, const int* labels, int m,
+                   const double* prior, double* sum, double* sumsq, double* cross,
+                   DeviceArray<double>& scratch, cudaStream_t stream) {
+  // rows per chunk: enough blocks to cover every SM several times
+  const int col_tiles = (int)ceil_div(p, 32);
+  int rc = 2048;
+  int chunks = (int)ceil_div(n, rc);
+  const int want = 6 * num_sms();
+  if (col_tiles * chunks < want && n > 256) {
+    const int target = std::min((int)ceil_div(n, 256), (int)ceil_div(want, col_tiles));
+    if (target > chunks) {
+      rc = std::max(256, (int)ceil_div(n, target));
+      rc = (rc + 127) / 128 * 128;
+      chunks = (int)ceil_div(n, rc);
+    }
+  }
+  const int slots = m + 2;
+  scratch.reserve((size_t)chunks * p * slots, stream);
+  const size_t smem = (size_t)(rc + 1) / 2 * sizeof(double) + (size_t)8 * m * 32 * sizeof(double);
+  static const bool configured = [] {
+    FPLS_CHECK(cudaFuncSetAttribute(class_moments_kernel<T>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (2048 / 2 + 8 * kClassMomentsMaxClasses * 32) * 8));
+    return true;
+  }();
+  (void)configured;
+  class_moments_kernel<T><<<dim3(col_tiles, chunks), kThreads, smem, stream>>>(
+      X, n, p, ld, labels, m, rc, scratch.get());
+  count_launch();
+  FPLS_LAUNCH("class_moments_kernel");
+  class_moments_finish<<<std::min<unsigned>(ceil_div(p, 256), 8 * num_sms()), 256, 0, stream>>>(
+      scratch.get(), chunks, p, m, prior, sum, sumsq, cross);
+  count_launch();
+  FPLS_LAUNCH("class_moments_finish");
+}
+
 template <class T>
 void xtv_product(const T* X, int n, int p, long ld, const double* V, long ldv,
                  int nb, double* out, long ldo, DeviceArray<double>& scratch,
@@ -607,6 +736,9 @@ void topk_rows(const double* values, int rows, int classes, int top, int* out,
 }
 
 #define FPLS_INSTANTIATE(T)                                                   \
+  template void class_moments<T>(const T*, int, int, long, const int*, int,  \
+                                 const double*, double*, double*, double*,   \
+                                 DeviceArray<double>&, cudaStream_t);        \
   template void column_moments<T>(const T*, int, int, long, const double*,    \
                                   int, double*, double*, double*,             \
                                   DeviceArray<double>&, cudaStream_t);        \
