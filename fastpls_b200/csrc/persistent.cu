@@ -637,6 +637,11 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
                             DeviceArray<double>& S, double* gpk, Workspace& ws, cudaStream_t stream,
                             PersistentPlan& plan) {
   if (!persistent_enabled() || !persistent_supported(m, a) || n < 2 || p < 1) return false;
+  // Large fits take the per-kernel loop: its streaming kernels keep more
+  // loads in flight (many CTAs per SM) and a component's two passes over X
+  // dwarf its launch latency; the persistent launch pays off where the
+  // passes are short and the per-component launches dominate.
+  if ((long)n * p > kPersistMaxElements) return false;
   const int C = persistent_ctas(n, p);
   const int cap = capacity_of<T>();
   if (cap == 0 || C > cap) return false;

@@ -11,6 +11,8 @@ namespace fpls {
 
 constexpr int kPersistMaxResponses = 32;
 constexpr int kPersistMaxComponents = 256;
+// Largest fit (n p elements of X) that runs as one persistent launch.
+constexpr long kPersistMaxElements = 1L << 26;
 
 // Device-side description of one fit of a persistent launch.
 struct PersistentFit {

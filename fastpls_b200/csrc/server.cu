@@ -95,6 +95,7 @@ bool batchable_fit(const Request& r) {
   if (r.kind != kFit || f.method != kSimpls || !persistent_enabled()) return false;
   if (f.n < 2 || f.p < 1 || f.components < 1 || f.components > std::min(f.n - 1, f.p)) return false;
   if (!persistent_supported(f.q, f.components)) return false;
+  if ((long)f.n * f.p > kPersistMaxElements) return false;
   if (simpls_block_size(f.n, f.p, f.q, f.components, !r.labels.empty(), r.precision == 32) != 1)
     return false;
   const int elem = r.precision == 16 ? 2 : r.precision == 32 ? 4 : 8;
