@@ -560,7 +560,6 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
     FPLS_CHECK(cudaFuncSetAttribute(tail3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
-  gram_of_columns(S.get(), p, m, gpk, ws, stream);
 
   // cached-Gram route (FP32 / FP64 storage): Gs = X_s^T X_s once
   gram_route = gram_route && !std::is_same<T, bf16>::value;
@@ -602,6 +601,7 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
       return;
     }
   }
+  gram_of_columns(S.get(), p, m, gpk, ws, stream);
 
   // Candidate blocks (the reference's block refresh): the directions of
   // `use` consecutive components are the leading left singular vectors of S

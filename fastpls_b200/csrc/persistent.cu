@@ -59,7 +59,8 @@ constexpr int SC_ST = 34;          // sum t
 constexpr int SC_VV = 35;          // |v|^2
 constexpr int SC_Q = 40;           // q (m)
 constexpr int SC_SV = 72;          // S^T v (m)
-constexpr int SC_H = 104;          // V^T p (a)
+constexpr int SC_U = 104;          // S^T (mean / scale) (m)
+constexpr int SC_H = 136;          // V^T p (a)
 
 using Fit = PersistentFit;
 
@@ -170,12 +171,18 @@ template <> struct Vec16<bf16> {
 // P2: partial scores of one item (row tile x column chunk k): thread rows
 // i .. i + VEC - 1, columns of the chunk in order.
 template <class T>
-__device__ void xr_item(const Fit& f, const T* X, int tile, int k, double* rts) {
+__device__ void xr_item(const Fit& f, const T* X, int tile, int k, const double* zs,
+                        double* rts) {
   constexpr int VN = Vec16<T>::N;
   const int c0 = k * f.cc;
   const int cols = min(f.cc, f.p - c0);
   __syncthreads();
-  for (int j = threadIdx.x; j < cols; j += PT) rts[j] = __ldcg(f.rt + c0 + j);
+  // rt = (S z) / scale for the chunk's columns (S is not deflated until P7)
+  for (int j = threadIdx.x; j < cols; j += PT) {
+    double rv = 0.0;
+    for (int c = 0; c < f.m; ++c) rv = fma(__ldcg(f.S + c0 + j + (long)c * f.p), zs[c], rv);
+    rts[j] = rv / f.scale[c0 + j];
+  }
   __syncthreads();
   const int vec = f.vec;  // VN or 1
   const int rows_tile = PT * vec;
@@ -338,8 +345,60 @@ __device__ void direction_step(const Fit& f, double* sm, int* flag) {
   __syncthreads();
 }
 
+// Over this CTA's columns [j0, j1): when a >= 0, V[:, a] = v / |v| and the
+// deflation S -= V[:, a] (S^T v / |v|)^T; then the partials of the Gram of S
+// (slots 0 .. G-1, packed lower triangle) and of u = S^T (mean / scale)
+// (slots G .. G+m-1) into the CTA's partial row. Whole CTA.
+__device__ void gram_u_partials(const Fit& f, int cta, int j0, int j1, int a, double inv_v,
+                                const double* sv, double* sm) {
+  const int m = f.m, p = f.p;
+  const int G = m * (m + 1) / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* ss = sm;                                        // kGramRows x m
+  double* gacc = sm + kGramRows * kPersistMaxResponses;   // G + m running sums (warp-owned)
+  double* wsc = gacc + 640;                               // kGramRows mean / scale
+  __syncthreads();
+  for (int k = threadIdx.x; k < G + m; k += PT) gacc[k] = 0.0;
+  for (int g0 = j0; g0 < j1; g0 += kGramRows) {
+    const int rows = min(kGramRows, j1 - g0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < rows * m; idx += PT) {
+      const int jl = idx % rows, c = idx / rows;
+      const int j = g0 + jl;
+      double sval = __ldcg(f.S + j + (long)c * p);
+      if (a >= 0) {
+        const double vj = __ldcg(f.v + j) * inv_v;
+        if (c == 0) f.V[j + (long)a * p] = vj;
+        sval = fma(-vj, sv[c] * inv_v, sval);
+        f.S[j + (long)c * p] = sval;
+      }
+      ss[jl + c * kGramRows] = sval;
+      if (c == 0) wsc[jl] = f.mean[j] / f.scale[j];
+    }
+    __syncthreads();
+    for (int k = warp; k < G + m; k += PT / 32) {
+      double s = 0.0;
+      if (k < G) {
+        int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+        while (c * (c + 1) / 2 > k) --c;
+        while ((c + 1) * (c + 2) / 2 <= k) ++c;
+        const int d = k - c * (c + 1) / 2;
+        for (int jl = lane; jl < rows; jl += 32)
+          s = fma(ss[jl + c * kGramRows], ss[jl + d * kGramRows], s);
+      } else {
+        const int c = k - G;
+        for (int jl = lane; jl < rows; jl += 32) s = fma(ss[jl + c * kGramRows], wsc[jl], s);
+      }
+      s = warp_sum(s);
+      if (lane == 0) gacc[k] += s;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < G + m; k += PT) f.cpart[(long)cta * f.cslots + k] = gacc[k];
+}
+
 template <class T>
-__global__ void __launch_bounds__(PT, 2)
+__global__ void __launch_bounds__(PT, 3)
     persistent_simpls(const Fit* __restrict__ fits, int nfits) {
   extern __shared__ double psm[];
   __shared__ double red[32];
@@ -359,40 +418,43 @@ __global__ void __launch_bounds__(PT, 2)
   int j0, j1;
   col_range(p, C, cta, j0, j1);
 
+  __shared__ int item_s;
+  const int G = m * (m + 1) / 2;
+  // partials of the Gram of S and of u = S^T (mean / scale) over this CTA's
+  // columns, before the first component (S = S0)
+  gram_u_partials(f, cta, j0, j1, -1, 0.0, sv, psm);
   for (int a = 0; a < f.a; ++a) {
-    // B0: Gram of the deflated S (after the first component) and direction
+    // B0: Gram and u of the (deflated) S, the direction z / sqrt(lambda), and
+    // the score offset c = mean . (S z / scale) = z . u
     if (!group_sync(f, flag, [&] {
-          if (a > 0) {
-            reduce_slots(f, m * (m + 1) / 2, [&](int k, double v) { f.gpk[k] = v; });
-            __syncthreads();
-            __threadfence();
-          }
+          reduce_slots(f, G + m, [&](int k, double v) {
+            if (k < G) f.gpk[k] = v;
+            else f.scal[SC_U + k - G] = v;
+          });
+          __syncthreads();
+          __threadfence();
           direction_step(f, psm, flag);
+          if (tid == 0) {
+            double cz = 0.0;
+            for (int c = 0; c < m; ++c) cz = fma(f.scal[SC_Z + c], __ldcg(f.scal + SC_U + c), cz);
+            f.scal[SC_C] = cz;
+            atomicExch(f.bar + 2, 0u);  // item counter of the score pass
+          }
         }))
       return;
     for (int c = tid; c < m; c += PT) zs[c] = __ldcg(f.scal + SC_Z + c);
     __syncthreads();
-    // P1: r = S z, rt = r / scale, partial mean . rt
-    double acc = 0.0;
-    for (int j = cta * PT + tid; j < p; j += C * PT) {
-      double rv = 0.0;
-      for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + j + (long)c * p), zs[c], rv);
-      const double w = rv / f.scale[j];
-      f.r[j] = rv;
-      f.rt[j] = w;
-      acc = fma(f.mean[j], w, acc);
-    }
-    acc = cta_sum(acc, red);
-    if (tid == 0) f.cpart[(long)cta * f.cslots] = acc;
-    if (!group_sync(f, flag, [&] {
-          reduce_slots(f, 1, [&](int, double v) { f.scal[SC_C] = v; });
-        }))
-      return;
-    // P2: score partials, items (row tile, column chunk)
+    // P2: score partials, items (row tile, column chunk) claimed in order
     {
       const int tiles = (n + PT * f.vec - 1) / (PT * f.vec);
       const int items = tiles * f.kt;
-      for (int it = cta; it < items; it += C) xr_item<T>(f, X, it % tiles, it / tiles, psm);
+      for (;;) {
+        if (tid == 0) item_s = (int)atomicAdd(f.bar + 2, 1u);
+        __syncthreads();
+        const int it = item_s;
+        if (it >= items) break;
+        xr_item<T>(f, X, it % tiles, it / tiles, zs, psm);
+      }
     }
     if (!group_sync(f, flag, [] {})) return;
     // P3: t = sum of the chunk partials - c; |t|^2 and sum t
@@ -401,17 +463,17 @@ __global__ void __launch_bounds__(PT, 2)
       double* tcol = f.T + (long)a * n;
       double s2 = 0.0, s1 = 0.0;
       for (int i = cta * PT + tid; i < n; i += C * PT) {
-        // four interleaved partial sums (more loads in flight), fixed order
-        double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        // eight interleaved partial sums (more loads in flight), fixed order
+        double q[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) q[u] = 0.0;
         int k = 0;
-        for (; k + 3 < f.kt; k += 4) {
-          q0 += __ldcg(f.tpart + (long)k * n + i);
-          q1 += __ldcg(f.tpart + (long)(k + 1) * n + i);
-          q2 += __ldcg(f.tpart + (long)(k + 2) * n + i);
-          q3 += __ldcg(f.tpart + (long)(k + 3) * n + i);
+        for (; k + 7 < f.kt; k += 8) {
+#pragma unroll
+          for (int u = 0; u < 8; ++u) q[u] += __ldcg(f.tpart + (long)(k + u) * n + i);
         }
-        for (; k < f.kt; ++k) q0 += __ldcg(f.tpart + (long)k * n + i);
-        const double t = ((q0 + q1) + (q2 + q3)) - cc;
+        for (; k < f.kt; ++k) q[0] += __ldcg(f.tpart + (long)k * n + i);
+        const double t = (((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]))) - cc;
         tcol[i] = t;
         s2 = fma(t, t, s2);
         s1 += t;
@@ -425,17 +487,24 @@ __global__ void __launch_bounds__(PT, 2)
     }
     if (!group_sync(f, flag, [&] {
           reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
+          if (tid == 0) atomicExch(f.bar + 3, 0u);  // item counter of the loading pass
         }))
       return;
-    // P4: loading partials, items (row chunk, 32-column tile)
+    // P4: loading partials, items (row chunk, 32-column tile) claimed in order
     {
       const int jtiles = (p + 31) / 32;
       const int items = jtiles * f.kp;
       const double* tcol = f.T + (long)a * n;
-      for (int it = cta; it < items; it += C) xtv_item<T>(f, X, it % f.kp, it / f.kp, tcol, psm);
+      for (;;) {
+        if (tid == 0) item_s = (int)atomicAdd(f.bar + 3, 1u);
+        __syncthreads();
+        const int it = item_s;
+        if (it >= items) break;
+        xtv_item<T>(f, X, it % f.kp, it / f.kp, tcol, psm);
+      }
     }
     if (!group_sync(f, flag, [] {})) return;
-    // P5: p, R[:, a]; partial V^T p (a) and S0^T R[:, a] (m)
+    // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
     if (tid == 0) {
       const double t2 = __ldcg(f.scal + SC_T2);
       const double tn = sqrt(t2);
@@ -446,7 +515,7 @@ __global__ void __launch_bounds__(PT, 2)
     }
     __syncthreads();
     const double inv_t = scal_s[0], sum_t = scal_s[1];
-    double* ps = psm;          // p values of this CTA's columns (<= 4096)
+    double* ps = psm;          // p values of this CTA's columns (<= 2048)
     double* rs = psm + 2048;   // R values
     for (int jl = tid; jl < j1 - j0; jl += PT) {
       const int j = j0 + jl;
@@ -460,8 +529,10 @@ __global__ void __launch_bounds__(PT, 2)
       }
       for (; k < f.kp; ++k) q0 += __ldcg(f.ppart + (long)k * p + j);
       const double pr = (q0 + q1) + (q2 + q3);
+      double rv = 0.0;
+      for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + j + (long)c * p), zs[c], rv);
       const double pj = (pr - f.mean[j] * sum_t) / f.scale[j] * inv_t;
-      const double rj = __ldcg(f.r + j) * inv_t;
+      const double rj = rv * inv_t;
       f.pv[j] = pj;
       f.R[j + (long)a * p] = rj;
       ps[jl] = pj;
@@ -503,6 +574,7 @@ __global__ void __launch_bounds__(PT, 2)
     for (int jl = tid; jl < j1 - j0; jl += PT) {
       const int j = j0 + jl;
       double vj = __ldcg(f.pv + j);
+#pragma unroll 4
       for (int k = 0; k < a; ++k) vj = fma(-__ldcg(f.V + j + (long)k * p), hs[k], vj);
       f.v[j] = vj;
       vs[jl] = vj;
@@ -528,7 +600,8 @@ __global__ void __launch_bounds__(PT, 2)
           });
         }))
       return;
-    // P7: V[:, a], deflate S, partial Gram of the deflated S; T[:, a] /= |t|
+    // P7: V[:, a], deflate S, partials of the Gram and u of the deflated S;
+    // T[:, a] /= |t|
     if (tid == 0) {
       const double vn = sqrt(__ldcg(f.scal + SC_VV));
       const bool ok = vn > 0.0 && isfinite(vn);
@@ -537,43 +610,9 @@ __global__ void __launch_bounds__(PT, 2)
     }
     for (int c = tid; c < m; c += PT) sv[c] = __ldcg(f.scal + SC_SV + c);
     __syncthreads();
-    const double inv_v = scal_s[2];
-    {
-      const int G = m * (m + 1) / 2;
-      const int lane = tid & 31, warp = tid >> 5;
-      double* ss = psm;  // kGramRows x m
-      double* gacc = psm + kGramRows * kPersistMaxResponses;  // G running sums (warp-owned)
-      for (int k = tid; k < G; k += PT) gacc[k] = 0.0;
-      for (int g0 = j0; g0 < j1; g0 += kGramRows) {
-        const int rows = min(kGramRows, j1 - g0);
-        __syncthreads();
-        for (int idx = tid; idx < rows * m; idx += PT) {
-          const int jl = idx % rows, c = idx / rows;
-          const int j = g0 + jl;
-          const double vj = __ldcg(f.v + j) * inv_v;
-          if (c == 0) f.V[j + (long)a * p] = vj;
-          const double s = fma(-vj, sv[c] * inv_v, __ldcg(f.S + j + (long)c * p));
-          f.S[j + (long)c * p] = s;
-          ss[jl + c * kGramRows] = s;
-        }
-        __syncthreads();
-        for (int k = warp; k < G; k += PT / 32) {
-          int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
-          while (c * (c + 1) / 2 > k) --c;
-          while ((c + 1) * (c + 2) / 2 <= k) ++c;
-          const int d = k - c * (c + 1) / 2;
-          double s = 0.0;
-          for (int jl = lane; jl < rows; jl += 32)
-            s = fma(ss[jl + c * kGramRows], ss[jl + d * kGramRows], s);
-          s = warp_sum(s);
-          if (lane == 0) gacc[k] += s;
-        }
-      }
-      __syncthreads();
-      for (int k = tid; k < G; k += PT) f.cpart[(long)cta * f.cslots + k] = gacc[k];
-      double* tcol = f.T + (long)a * n;
-      for (int i = cta * PT + tid; i < n; i += C * PT) tcol[i] = __ldcg(tcol + i) * inv_t;
-    }
+    gram_u_partials(f, cta, j0, j1, a, scal_s[2], sv, psm);
+    double* tcol = f.T + (long)a * n;
+    for (int i = cta * PT + tid; i < n; i += C * PT) tcol[i] = __ldcg(tcol + i) * inv_t;
   }
 }
 
@@ -601,9 +640,9 @@ std::unique_ptr<PersistentPlan>*& persistent_deferral() {
 }
 
 int persistent_ctas(int n, int p) {
-  // from (n, p) only, never from the storage type: at most two per SM
+  // from (n, p) only, never from the storage type: at most three per SM
   const long elems = (long)n * p;
-  return (int)std::max(1L, std::min<long>(2L * num_sms(), (elems + (1L << 17) - 1) >> 17));
+  return (int)std::max(1L, std::min<long>(3L * num_sms(), (elems + (1L << 17) - 1) >> 17));
 }
 
 namespace {
@@ -621,7 +660,7 @@ int capacity_of() {
       cudaGetLastError();
       return 0;
     }
-    return v >= 2 ? v * num_sms() : 0;
+    return v >= 3 ? v * num_sms() : 0;
   }();
   return cap;
 }
@@ -664,8 +703,6 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   f.Q = model.Q.get();
   f.T = model.T.get();
   f.gpk = gpk;
-  f.r = ws.vec_p[0].get();
-  f.rt = ws.vec_p[1].get();
   f.pv = ws.vec_p[2].get();
   f.v = ws.vec_p[3].get();
   f.flag = ws.flag.get();
@@ -687,13 +724,13 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   // octet loads in the loading pass: the same condition for every storage
   // type (so BF16 and FP32 storage of the same values sum in one order)
   f.oct = (reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % 8 == 0) ? 1 : 0;
-  f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2));
+  f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2 + m));
   const PersistentWaitTest& wt = persistent_wait_test();
   f.barrier_cycles = wt.cycles > 0 ? wt.cycles : kBarrierCycles;
   f.absent_cta = wt.absent ? 0 : -1;
 
   // scratch of this fit (stream-ordered, freed behind the launch); the
-  // workspace's own scalar arrays hold the Gram of S and stay untouched
+  // kernel forms the Gram of S itself (into gpk) before the first component
   plan.elem = (int)sizeof(T);
   plan.S = std::move(S);
   f.S = plan.S.get();
@@ -702,7 +739,7 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   f.ppart = f.tpart + (size_t)f.kt * n;
   plan.cpart.allocate((size_t)C * f.cslots, stream);
   plan.scal.allocate((size_t)SC_H + kPersistMaxComponents + 8, stream);
-  plan.bar.allocate(2, stream);
+  plan.bar.allocate(4, stream);
   plan.bar.zero(stream);
   f.cpart = plan.cpart.get();
   f.scal = plan.scal.get();

@@ -24,12 +24,12 @@ struct PersistentFit {
   const double* S0;
   double *S, *R, *V, *Q, *T;
   double* gpk;              // packed Gram of S (m (m + 1) / 2)
-  double *r, *rt, *pv, *v;  // p
+  double *pv, *v;           // p
   double* tpart;            // kt x n
   double* ppart;            // kp x p
   double* cpart;            // C x cslots
   double* scal;             // scalar slots
-  unsigned* bar;            // [count, generation]
+  unsigned* bar;            // [count, generation, score items, loading items]
   int* flag;                // the fit's error flag
   int cta0, C;              // CTA range of this fit in the launch
   int cc, kt;               // t pass: columns per chunk, chunks
@@ -58,8 +58,9 @@ int persistent_ctas(int n, int p);
 int persistent_capacity(int elem);
 
 // Plans the whole component loop of a SIMPLS fit (one direction per
-// component) from S (p x m, deflated in place; the plan takes it over), its
-// packed Gram gpk and model.{mean, scale, S0}, to fill model.{R, Q, V, T}.
+// component) from S (p x m, deflated in place; the plan takes it over) and
+// model.{mean, scale, S0}, to fill model.{R, Q, V, T}; gpk receives the
+// packed Gram of the deflated S.
 // Returns false (nothing planned, S untouched) when the shape or the device
 // does not allow it.
 template <class T>
