@@ -131,6 +131,26 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
       A[d + c * m] = v;
     }
   __syncthreads();
+  if (count == 1 && m <= kDominantMaxOrder) {
+    // one direction: the dominant pair alone (repeated squaring)
+    double* C = E + m * m;
+    double* v = C + m * m;
+    double lam = 0.0;
+    const bool found = dominant_pair(A, E, C, v, m, lam);
+    if (threadIdx.x == 0) {
+      const bool ok = found && lam > 0.0 && isfinite(lam);
+      if (!ok) flag_error(flag, 1);
+      const double inv = ok ? 1.0 / sqrt(lam) : 0.0;
+      int arg = 0;
+      if (found)
+        for (int k = 1; k < m; ++k)
+          if (fabs(v[k]) > fabs(v[arg])) arg = k;
+      const double sgn = found && v[arg] < 0.0 ? -1.0 : 1.0;
+      for (int k = 0; k < m; ++k) zs[k] = found ? sgn * v[k] * inv : 0.0;
+      if (lambda_out) *lambda_out = found ? lam : 0.0;
+    }
+    return;
+  }
   jacobi_eigen(A, E, m);
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -466,7 +486,8 @@ __global__ void s_times_z(const double* __restrict__ S, int p, int m,
 
 void dominant_direction(const double* S, int p, int m, const double* gpk,
                         double* zs, double* w, Workspace& ws, cudaStream_t s) {
-  const size_t smem_dir = 2 * (size_t)m * m * sizeof(double);
+  // A, B, C, v of the dominant pair (one direction), or A, E of the Jacobi sweeps
+  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m : 2 * (size_t)m * m) * sizeof(double);
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
   direction_kernel<<<1, jacobi_threads(m), smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get(), 1);
@@ -555,7 +576,8 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
   const unsigned g3 = ceil_div(p, jb3);
   const size_t smem3 = ((size_t)jb3 * m + (size_t)m * (m + 1) / 2) * sizeof(double);
   const unsigned g1 = ceil_div(p, TB);
-  const size_t smem_dir = 2 * (size_t)m * m * sizeof(double);
+  // A, B, C, v of the dominant pair (one direction), or A, E of the Jacobi sweeps
+  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m : 2 * (size_t)m * m) * sizeof(double);
   if (smem3 > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(tail3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
   if (smem_dir > 48 * 1024)

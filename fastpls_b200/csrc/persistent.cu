@@ -45,8 +45,6 @@ namespace fpls {
 namespace {
 
 constexpr int PT = 256;                       // threads per CTA
-constexpr int kMaxXrCols = 2048;              // columns of rt staged per item
-constexpr int kMaxXtvRows = 4096;             // rows of t staged per item
 constexpr int kGramRows = 64;                 // S rows staged per Gram step
 constexpr int kSmemDoubles = 4096;            // 32 KB of dynamic shared memory
 constexpr long long kBarrierCycles = 4000000000LL;  // about 2 s
@@ -59,8 +57,7 @@ constexpr int SC_ST = 34;          // sum t
 constexpr int SC_VV = 35;          // |v|^2
 constexpr int SC_Q = 40;           // q (m)
 constexpr int SC_SV = 72;          // S^T v (m)
-constexpr int SC_U = 104;          // S^T (mean / scale) (m)
-constexpr int SC_H = 136;          // V^T p (a)
+constexpr int SC_H = 104;          // V^T p (a)
 
 using Fit = PersistentFit;
 
@@ -126,221 +123,299 @@ __device__ __forceinline__ void col_range(int p, int C, int c, int& j0, int& j1)
 
 // Sums over the C per-CTA partials of slots 0 .. count-1 (stride cslots),
 // by the whole CTA: warp w takes slots w, w + 8, ...; lane l adds the
-// partials of CTAs l, l + 32, ... in order, then the warp's shuffle tree
-// (a fixed order). store(k, sum) runs on lane 0.
+// partials of CTAs l, l + 32, ... in order (the first kReduceLoads of them
+// loaded together), then the warp's shuffle tree (a fixed order).
+// store(k, sum) runs on lane 0.
+constexpr int kReduceLoads = 12;
 template <class F>
 __device__ __forceinline__ void reduce_slots(const Fit& f, int count, F&& store) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = warp; k < count; k += PT / 32) {
+    double v[kReduceLoads];
+#pragma unroll
+    for (int i = 0; i < kReduceLoads; ++i) {
+      const int c = lane + 32 * i;
+      v[i] = c < f.C ? __ldcg(f.cpart + (long)c * f.cslots + k) : 0.0;
+    }
     double s = 0.0;
-#pragma unroll 4
-    for (int c = lane; c < f.C; c += 32) s += __ldcg(f.cpart + (long)c * f.cslots + k);
+#pragma unroll
+    for (int i = 0; i < kReduceLoads; ++i) s += v[i];
+    for (int c = lane + 32 * kReduceLoads; c < f.C; c += 32) s += __ldcg(f.cpart + (long)c * f.cslots + k);
     s = warp_sum(s);
     if (lane == 0) store(k, s);
   }
 }
 
-template <class T> struct Vec16;
-template <> struct Vec16<float> {
-  static constexpr int N = 4;
-  using type = float4;
-  static __device__ __forceinline__ void get(const type& v, double (&o)[4]) {
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-  }
+// ---------------------------------------------------------------------------
+// Streaming passes over X. Each CTA owns a region of X: a row block of
+// f.rb rows (block rbk = cta % Cr) times a column range of f.pc columns
+// (range crg = cta / Cr). A pass streams the region through a ring of
+// shared-memory stages of Ring<T>::kCols column segments, one cp.async.bulk
+// copy per segment (its 16-byte aligned cover, or for the segments at the
+// two ends of X its aligned interior, the rows outside it read from global
+// memory by the consumers) completing on the stage's mbarrier. Warps consume
+// the stages independently; the last warp done with a stage refills its
+// slot. The scores pass walks the region's columns forward, the loading
+// pass backward, so the stages read last by one pass are read first by the
+// next while they are still in L2. The partition and the order of every sum
+// depend on (n, p) only: every storage type sums in the same order.
+
+constexpr int kBlockRows = 512;   // largest row block (rows of a segment)
+constexpr int kAuxDoubles = 1024; // rt of the region's columns / t of its rows
+
+// Stage geometry per storage type: kCols column segments of kBlockRows
+// rows, kStages stages, about 100 KB of ring per CTA so that two CTAs fit
+// an SM. Each stage carries 8192 elements (16 per thread, 4096 for FP64)
+// so that the per-stage handshake is small beside the consume work.
+template <class T>
+struct Ring {
+  static constexpr int kColStride = kBlockRows * (int)sizeof(T) + 16;
+  static constexpr int kCols = sizeof(T) == 8 ? 8 : 16;
+  static constexpr int kStageBytes = kCols * kColStride;
+  static constexpr int kStages = sizeof(T) == 2 ? 5 : 3;
+  static constexpr int kBytes = kStages * kStageBytes;
+  static constexpr int kDynBytes = kBytes + kAuxDoubles * (int)sizeof(double);
 };
-template <> struct Vec16<double> {
-  static constexpr int N = 2;
-  using type = double2;
-  static __device__ __forceinline__ void get(const type& v, double (&o)[2]) {
-    o[0] = v.x; o[1] = v.y;
-  }
-};
-template <> struct Vec16<bf16> {
-  static constexpr int N = 8;
-  using type = uint4;
-  static __device__ __forceinline__ void get(const type& v, double (&o)[8]) {
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      o[2 * k] = (double)__uint_as_float(w[k] << 16);
-      o[2 * k + 1] = (double)__uint_as_float(w[k] & 0xffff0000u);
-    }
-  }
+constexpr int kMaxRingStages = 8;
+static_assert(kBlockRows == 2 * PT, "the scores pass gives each thread two rows of a block");
+static_assert(Ring<bf16>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8 &&
+                  Ring<float>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8 &&
+                  Ring<double>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8,
+              "the vector phases use the first kSmemDoubles + kPersistMaxComponents doubles of the ring");
+static_assert(Ring<bf16>::kCols <= 32 && Ring<float>::kCols <= 32 && Ring<double>::kCols <= 32 &&
+                  Ring<float>::kCols % (PT / 32) == 0 && Ring<double>::kCols % (PT / 32) == 0 &&
+                  Ring<bf16>::kCols % (PT / 32) == 0,
+              "one lane per column segment when issuing; whole columns per warp when loading");
+
+inline int round_up(long v, long m) { return (int)((v + m - 1) / m * m); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void ring_bar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void ring_expect(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool ring_try(uint64_t* bar, unsigned parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for the phase of `parity` to complete (false on expiry).
+__device__ __forceinline__ bool ring_wait(uint64_t* bar, unsigned parity) {
+  if (ring_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!ring_try(bar, parity))
+    if (clock64() - t0 > kBarrierCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// The region of this CTA.
+struct Region {
+  long r0;   // first row
+  int rows;  // rows of the row block
+  int rbk;   // row block
+  int c0;    // first column
+  int cols;  // columns of the range (0 for an empty trailing range)
+  int crg;   // column range
+  int nst;   // stages per pass
+  int off0;  // byte offset mod 16 of (row r0, column 0) of X
+  int offc;  // byte offset mod 16 added per column
+  bool ends; // holds the first or the last segment of X (plain-loaded rows)
+  // byte offset mod 16 of the region's segment of column col
+  __device__ __forceinline__ int off(int col) const { return (off0 + col * offc) & 15; }
 };
 
-// P2: partial scores of one item (row tile x column chunk k): thread rows
-// i .. i + VEC - 1, columns of the chunk in order.
 template <class T>
-__device__ void xr_item(const Fit& f, const T* X, int tile, int k, const double* zs,
-                        double* rts) {
-  constexpr int VN = Vec16<T>::N;
-  const int c0 = k * f.cc;
-  const int cols = min(f.cc, f.p - c0);
-  __syncthreads();
-  // rt = (S z) / scale for the chunk's columns (S is not deflated until P7)
-  for (int j = threadIdx.x; j < cols; j += PT) {
-    double rv = 0.0;
-    for (int c = 0; c < f.m; ++c) rv = fma(__ldcg(f.S + c0 + j + (long)c * f.p), zs[c], rv);
-    rts[j] = rv / f.scale[c0 + j];
+__device__ __forceinline__ Region region_of(const Fit& f, int cta) {
+  Region g;
+  g.rbk = cta % f.Cr;
+  g.crg = cta / f.Cr;
+  g.r0 = (long)g.rbk * f.rb;
+  g.rows = (int)min((long)f.rb, (long)f.n - g.r0);
+  g.c0 = min(f.p, g.crg * f.pc);
+  g.cols = min(f.pc, f.p - g.c0);
+  g.nst = (g.cols + Ring<T>::kCols - 1) / Ring<T>::kCols;
+  const int es = f.elem;
+  g.off0 = (int)((reinterpret_cast<uintptr_t>(f.X) + (uintptr_t)g.r0 * es) & 15);
+  g.offc = (int)(((uintptr_t)f.ld * es) & 15);
+  // whether an aligned cover leaves X: the region's segments ascend with
+  // the column, so its first and last segments decide
+  g.ends = false;
+  if (g.cols > 0) {
+    const uintptr_t x0 = reinterpret_cast<uintptr_t>(f.X);
+    const uintptr_t x1 = x0 + ((uintptr_t)(f.p - 1) * f.ld + f.n) * es;
+    const uintptr_t first = x0 + ((uintptr_t)g.c0 * f.ld + g.r0) * es;
+    const uintptr_t last = x0 + ((uintptr_t)(g.c0 + g.cols - 1) * f.ld + g.r0 + g.rows) * es;
+    g.ends = (first & ~(uintptr_t)15) < x0 || ((last + 15) & ~(uintptr_t)15) > x1;
   }
+  return g;
+}
+
+// Byte geometry of one column segment (rows r0 .. r0 + rows - 1 of column
+// col, element r at byte off + r * sizeof(T) of its slot). The copy is the
+// segment's 16-byte aligned cover [lo, hi) when that lies inside X (the
+// neighbouring bytes belong to other columns or row blocks and are not
+// used); otherwise (the first and last segments of X, at most) the aligned
+// interior [lo, hi) plus plain loads of the rows [0, head) and [tail0, rows).
+struct Segment {
+  uintptr_t g, lo, hi;
+  int off;
+  int head, tail0;
+};
+
+template <class T>
+__device__ __forceinline__ Segment segment(const Fit& f, const T* X, const Region& g, int col) {
+  Segment sg;
+  sg.g = reinterpret_cast<uintptr_t>(X + (long)col * f.ld + g.r0);
+  const uintptr_t end = sg.g + (uintptr_t)g.rows * sizeof(T);
+  sg.off = (int)(sg.g & 15);
+  const uintptr_t x0 = reinterpret_cast<uintptr_t>(X);
+  const uintptr_t x1 = reinterpret_cast<uintptr_t>(X + (long)(f.p - 1) * f.ld + f.n);
+  sg.lo = sg.g & ~(uintptr_t)15;
+  sg.hi = (end + 15) & ~(uintptr_t)15;
+  if (sg.lo >= x0 && sg.hi <= x1) {
+    sg.head = 0;
+    sg.tail0 = g.rows;
+  } else {
+    sg.lo = (sg.g + 15) & ~(uintptr_t)15;
+    sg.hi = end & ~(uintptr_t)15;
+    sg.head = (int)min((uintptr_t)g.rows, (sg.lo - sg.g) / sizeof(T));
+    sg.tail0 = sg.hi > sg.lo ? (int)((sg.hi - sg.g) / sizeof(T)) : sg.head;
+  }
+  return sg;
+}
+
+// Warp 0: the bulk copies of stage `st` into `slot`, one lane per column,
+// completing on `bar`.
+template <class T>
+__device__ void issue_stage(const Fit& f, const T* X, const Region& g, int st, unsigned char* slot,
+                            uint64_t* bar) {
+  const int lane = threadIdx.x & 31;
+  const int nc = min(Ring<T>::kCols, g.cols - st * Ring<T>::kCols);
+  Segment sg;
+  unsigned bytes = 0;
+  if (lane < nc) {
+    sg = segment(f, X, g, g.c0 + st * Ring<T>::kCols + lane);
+    if (sg.hi > sg.lo) bytes = (unsigned)(sg.hi - sg.lo);
+  }
+  unsigned total = bytes;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+  if (lane == 0) ring_expect(bar, total);
+  __syncwarp();
+  if (bytes > 0)
+    bulk_to_smem(slot + lane * Ring<T>::kColStride + sg.off + ((long)sg.lo - (long)sg.g),
+                 reinterpret_cast<const void*>(sg.lo), bytes, bar);
+}
+
+// Streams the region's stages through the ring: issues the first stages,
+// runs prepare() (whole CTA) while they are in flight, then calls
+// consume(stage, slot) in every warp for each stage in order (forward or
+// backward). Warps run
+// through the stages independently: the last warp done with a stage
+// refills its slot with the stage kStages ahead (done[slot] counts the
+// warps, reset by that warp). `seq` numbers the CTA's stages across passes
+// (slot seq % stages, mbarrier parity (seq / stages) & 1). Returns false
+// when a stage never arrived (flag 5 set, the copies in flight waited for).
+template <class T, class P, class F>
+__device__ bool stream_region(const Fit& f, const T* X, const Region& g, bool backward,
+                              unsigned& seq, unsigned char* ring, uint64_t* bars, unsigned* done,
+                              unsigned* issued, int* flag, P&& prepare, F&& consume) {
+  constexpr int NS = Ring<T>::kStages;
+  constexpr unsigned kWarps = PT / 32;
+  const int nst = g.nst;
+  const int lane = threadIdx.x & 31;
+  auto stage_of = [&](int k) { return backward ? nst - 1 - k : k; };
+  auto slot_of = [&](int k) { return ring + (size_t)((seq + k) % NS) * Ring<T>::kStageBytes; };
+  __syncthreads();  // the ring is free (earlier passes and phases are done with it)
+  if (threadIdx.x < 32) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (int k = 0; k < min(NS, nst); ++k)
+      issue_stage(f, X, g, stage_of(k), slot_of(k), bars + (seq + k) % NS);
+    if (lane == 0) *issued = (unsigned)min(NS, nst);
+  }
+  prepare();  // (whole CTA) while the first stages are in flight
   __syncthreads();
-  const int vec = f.vec;  // VN or 1
-  const int rows_tile = PT * vec;
-  const int i = tile * rows_tile + threadIdx.x * vec;
-  if (i >= f.n) return;
-  double* out = f.tpart + (long)k * f.n;
-  const T* base = X + (long)c0 * f.ld + i;
-  if (vec == VN && i + VN <= f.n) {
-    using V = typename Vec16<T>::type;
-    double acc[VN];
-#pragma unroll
-    for (int u = 0; u < VN; ++u) acc[u] = 0.0;
-    int j = 0;
-    for (; j + 7 < cols; j += 8) {
-      V x[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u)
-        x[u] = __ldg(reinterpret_cast<const V*>(base + (long)(j + u) * f.ld));
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        double e[VN];
-        Vec16<T>::get(x[u], e);
-        const double w = rts[j + u];
-#pragma unroll
-        for (int q = 0; q < VN; ++q) acc[q] = fma(e[q], w, acc[q]);
+  bool ok = true;
+  for (int k = 0; k < nst; ++k) {
+    const unsigned sl = (seq + k) % NS;
+    ok = __all_sync(0xffffffffu, ring_wait(bars + sl, ((seq + k) / NS) & 1u));
+    if (!ok) break;
+    consume(stage_of(k), (const unsigned char*)slot_of(k));
+    __syncwarp();
+    unsigned prev = 0;
+    if (lane == 0) {
+      __threadfence_block();
+      prev = atomicAdd(done + sl, 1u);
+    }
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    if (prev == kWarps - 1) {
+      // every warp is done with the slot: refill it
+      __threadfence_block();
+      if (lane == 0) done[sl] = 0u;
+      if (k + NS < nst) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_stage(f, X, g, stage_of(k + NS), slot_of(k), bars + sl);
+        if (lane == 0) atomicAdd(issued, 1u);
       }
     }
-    for (; j < cols; ++j) {
-      double e[VN];
-      Vec16<T>::get(__ldg(reinterpret_cast<const V*>(base + (long)j * f.ld)), e);
-      const double w = rts[j];
-#pragma unroll
-      for (int q = 0; q < VN; ++q) acc[q] = fma(e[q], w, acc[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < VN; ++q) out[i + q] = acc[q];
-  } else {
-    // scalar rows (unaligned storage, or the last rows of X)
-    const int cnt = min(vec, f.n - i);
-    for (int q = 0; q < cnt; ++q) {
-      double acc = 0.0;
-      for (int j = 0; j < cols; ++j) acc = fma(as_f64(base[q + (long)j * f.ld]), rts[j], acc);
-      out[i + q] = acc;
-    }
   }
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) {
+      flag_error(flag, 5);
+      // the last stages issued may still be in flight
+      const int last = (int)*issued;
+      for (int j = max(0, last - NS); j < last; ++j) ring_wait(bars + (seq + j) % NS, ((seq + j) / NS) & 1u);
+      for (int j = 0; j < NS; ++j) done[j] = 0u;
+    }
+    return false;
+  }
+  seq += (unsigned)nst;
+  return true;
 }
 
-// Eight consecutive rows of a column as FP64 (16-byte aligned source): one
-// 16-byte load for BF16, two for FP32, four for FP64.
-template <class T> struct Oct;
-template <> struct Oct<bf16> {
-  static __device__ __forceinline__ void load(const bf16* p, double (&x)[8]) {
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      x[2 * k] = (double)__uint_as_float(w[k] << 16);
-      x[2 * k + 1] = (double)__uint_as_float(w[k] & 0xffff0000u);
-    }
-  }
-};
-template <> struct Oct<float> {
-  static __device__ __forceinline__ void load(const float* p, double (&x)[8]) {
-    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-    x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
-  }
-};
-template <> struct Oct<double> {
-  static __device__ __forceinline__ void load(const double* p, double (&x)[8]) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const double2 v = __ldg(reinterpret_cast<const double2*>(p) + k);
-      x[2 * k] = v.x;
-      x[2 * k + 1] = v.y;
-    }
-  }
-};
-
-// P4: loading partials of one item (row chunk kc x 32 columns from jt*32).
-// Warp w owns columns w, w + 8, w + 16, w + 24 of the tile and walks them
-// together; lane l takes the row octets l, l + 32, ... (8 consecutive rows
-// per load, in row order), then the leftover rows one per lane; the t rows
-// are staged in shared memory. The summation order depends only on the
-// row count, so it is the same for every storage type.
-template <class T>
-__device__ void xtv_item(const Fit& f, const T* X, int kc, int jt, const double* tcol,
-                         double* ts) {
-  const int r0 = kc * f.rc;
-  const int rows = min(f.rc, f.n - r0);
-  __syncthreads();
-  for (int r = threadIdx.x; r < rows; r += PT) ts[r] = __ldcg(tcol + r0 + r);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* col[4];
-  bool ok[4];
-  double acc[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int j = jt * 32 + warp + 8 * c;
-    ok[c] = j < f.p;
-    col[c] = X + (long)(ok[c] ? j : 0) * f.ld + r0;
-    acc[c] = 0.0;
-  }
-  const int octs = f.oct ? rows >> 3 : 0;
-  for (int o = lane; o < octs; o += 32) {
-    const double* tv = ts + 8 * o;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (!ok[c]) continue;
-      double x[8];
-      Oct<T>::load(col[c] + 8 * o, x);
-#pragma unroll
-      for (int e = 0; e < 8; ++e) acc[c] = fma(x[e], tv[e], acc[c]);
-    }
-  }
-  for (int r = 8 * octs + lane; r < rows; r += 32) {
-    const double tv = ts[r];
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-      if (ok[c]) acc[c] = fma(as_f64(col[c][r]), tv, acc[c]);
-  }
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const double v = warp_sum(acc[c]);
-    if (lane == 0 && ok[c]) f.ppart[(long)kc * f.p + jt * 32 + warp + 8 * c] = v;
-  }
-}
-
-// Dominant eigenpair of the packed m x m Gram (whole CTA): zs = s z / sqrt(lambda),
-// sign fixed so the largest |z| entry is positive (as direction_kernel).
-__device__ void direction_step(const Fit& f, double* sm, int* flag) {
+// Dominant eigenpair of the m x m Gram in A (shared, symmetric; whole CTA;
+// B, C, v shared scratch): scal[SC_Z..] = s z / sqrt(lambda), sign fixed so
+// the largest |z| entry is positive (as direction_kernel), and
+// scal[SC_C] = z . u with u (shared, m) = S^T (mean / scale).
+__device__ void direction_step(const Fit& f, const double* A, double* B, double* C, double* v,
+                               const double* u, int* flag) {
   const int m = f.m;
-  double* A = sm;
-  double* E = sm + m * m;
-  for (int c = threadIdx.x; c < m; c += blockDim.x)
-    for (int d = 0; d <= c; ++d) {
-      const double v = __ldcg(f.gpk + c * (c + 1) / 2 + d);
-      A[c + d * m] = v;
-      A[d + c * m] = v;
-    }
-  __syncthreads();
-  jacobi_eigen(A, E, m);
-  __syncthreads();
+  double lam = 0.0;
+  const bool found = dominant_pair(A, B, C, v, m, lam);
   if (threadIdx.x == 0) {
-    int best = 0;
-    for (int k = 1; k < m; ++k)
-      if (A[k + k * m] > A[best + best * m]) best = k;
-    const double lam = A[best + best * m];
-    const bool ok = lam > 0.0 && isfinite(lam);
+    const bool ok = found && lam > 0.0 && isfinite(lam);
     if (!ok) flag_error(flag, 1);
     const double inv = ok ? 1.0 / sqrt(lam) : 0.0;
     int arg = 0;
-    for (int k = 1; k < m; ++k)
-      if (fabs(E[k + best * m]) > fabs(E[arg + best * m])) arg = k;
-    const double sgn = E[arg + best * m] < 0.0 ? -1.0 : 1.0;
-    for (int k = 0; k < m; ++k) f.scal[SC_Z + k] = sgn * E[k + best * m] * inv;
+    if (found)
+      for (int k = 1; k < m; ++k)
+        if (fabs(v[k]) > fabs(v[arg])) arg = k;
+    const double sgn = found && v[arg] < 0.0 ? -1.0 : 1.0;
+    double cz = 0.0;
+    for (int k = 0; k < m; ++k) {
+      const double zk = found ? sgn * v[k] * inv : 0.0;
+      f.scal[SC_Z + k] = zk;
+      cz = fma(zk, u[k], cz);
+    }
+    f.scal[SC_C] = cz;
   }
   __syncthreads();
 }
@@ -398,12 +473,15 @@ __device__ void gram_u_partials(const Fit& f, int cta, int j0, int j1, int a, do
 }
 
 template <class T>
-__global__ void __launch_bounds__(PT, 3)
+__global__ void __launch_bounds__(PT, 2)
     persistent_simpls(const Fit* __restrict__ fits, int nfits) {
-  extern __shared__ double psm[];
+  // dynamic: the ring of the streaming passes, then kAuxDoubles (rt / t);
+  // the vector phases use its first kSmemDoubles doubles as psm
+  extern __shared__ __align__(16) double psm[];
+  __shared__ __align__(8) uint64_t ring_bars[kMaxRingStages];
+  __shared__ unsigned ring_done[kMaxRingStages], ring_issued;
   __shared__ double red[32];
   __shared__ double zs[kPersistMaxResponses];
-  __shared__ double hs[kPersistMaxComponents];
   __shared__ double sv[kPersistMaxResponses];
   __shared__ double scal_s[4];
   int fi = 0;
@@ -418,7 +496,18 @@ __global__ void __launch_bounds__(PT, 3)
   int j0, j1;
   col_range(p, C, cta, j0, j1);
 
-  __shared__ int item_s;
+  unsigned char* const ring = reinterpret_cast<unsigned char*>(psm);
+  double* const aux = reinterpret_cast<double*>(ring + Ring<T>::kBytes);
+  const Region rg = region_of<T>(f, cta);
+  unsigned seq = 0;  // stages streamed by this CTA so far
+  if (tid == 0) {
+    for (int k = 0; k < Ring<T>::kStages; ++k) {
+      ring_bar_init(ring_bars + k);
+      ring_done[k] = 0u;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
   const int G = m * (m + 1) / 2;
   // partials of the Gram of S and of u = S^T (mean / scale) over this CTA's
   // columns, before the first component (S = S0)
@@ -427,37 +516,89 @@ __global__ void __launch_bounds__(PT, 3)
     // B0: Gram and u of the (deflated) S, the direction z / sqrt(lambda), and
     // the score offset c = mean . (S z / scale) = z . u
     if (!group_sync(f, flag, [&] {
+          double* A = psm;               // m x m Gram
+          double* B = A + m * m;         // squaring scratch
+          double* Cs = B + m * m;
+          double* vd = Cs + m * m;       // dominant eigenvector
+          double* us = vd + m;           // u
           reduce_slots(f, G + m, [&](int k, double v) {
-            if (k < G) f.gpk[k] = v;
-            else f.scal[SC_U + k - G] = v;
+            if (k < G) {
+              int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+              while (c * (c + 1) / 2 > k) --c;
+              while ((c + 1) * (c + 2) / 2 <= k) ++c;
+              const int d = k - c * (c + 1) / 2;
+              A[c + d * m] = v;
+              A[d + c * m] = v;
+              f.gpk[k] = v;
+            } else {
+              us[k - G] = v;
+            }
           });
           __syncthreads();
-          __threadfence();
-          direction_step(f, psm, flag);
-          if (tid == 0) {
-            double cz = 0.0;
-            for (int c = 0; c < m; ++c) cz = fma(f.scal[SC_Z + c], __ldcg(f.scal + SC_U + c), cz);
-            f.scal[SC_C] = cz;
-            atomicExch(f.bar + 2, 0u);  // item counter of the score pass
-          }
+          direction_step(f, A, B, Cs, vd, us, flag);
         }))
       return;
     for (int c = tid; c < m; c += PT) zs[c] = __ldcg(f.scal + SC_Z + c);
     __syncthreads();
-    // P2: score partials, items (row tile, column chunk) claimed in order
+    // P2: score partials of the region, t_part[crg][rows] = X[rows, cols] rt[cols]
+    // with rt = (S z) / scale (S is not deflated until P7)
     {
-      const int tiles = (n + PT * f.vec - 1) / (PT * f.vec);
-      const int items = tiles * f.kt;
-      for (;;) {
-        if (tid == 0) item_s = (int)atomicAdd(f.bar + 2, 1u);
-        __syncthreads();
-        const int it = item_s;
-        if (it >= items) break;
-        xr_item<T>(f, X, it % tiles, it / tiles, zs, psm);
-      }
+      // thread rows tid and tid + 256 of the row block (kBlockRows = 2 PT),
+      // the region's columns in order
+      constexpr int SC = Ring<T>::kCols;
+      double acc0 = 0.0, acc1 = 0.0;
+      const int r1 = tid + PT;
+      const bool in0 = tid < rg.rows, in1 = r1 < rg.rows;
+      auto rt = [&] {
+        for (int j = tid; j < rg.cols; j += PT) {
+          double rv = 0.0;
+          for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + rg.c0 + j + (long)c * p), zs[c], rv);
+          aux[j] = rv / f.scale[rg.c0 + j];
+        }
+      };
+      const bool ok = stream_region(f, X, rg, false, seq, ring, ring_bars, ring_done, &ring_issued, flag, rt,
+                                    [&](int st, const unsigned char* slot) {
+        const int nc = min(SC, rg.cols - st * SC);
+        const double* w = aux + st * SC;
+        const int cb = rg.c0 + st * SC;
+        if (nc == SC && !rg.ends) {
+          double x[SC];
+#pragma unroll
+          for (int c = 0; c < SC; ++c) {
+            const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
+            x[c] = in0 ? as_f64(col[tid]) : 0.0;
+          }
+          double a0 = acc0;
+#pragma unroll
+          for (int c = 0; c < SC; ++c) a0 = fma(x[c], w[c], a0);
+          acc0 = a0;
+#pragma unroll
+          for (int c = 0; c < SC; ++c) {
+            const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
+            x[c] = in1 ? as_f64(col[r1]) : 0.0;
+          }
+          double a1 = acc1;
+#pragma unroll
+          for (int c = 0; c < SC; ++c) a1 = fma(x[c], w[c], a1);
+          acc1 = a1;
+        } else {
+          for (int c = 0; c < nc; ++c) {
+            const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
+            const Segment sg = segment(f, X, rg, cb + c);
+            const T* gcol = X + (long)(cb + c) * f.ld + rg.r0;  // rows outside the copy
+            const double wc = w[c];
+            if (in0) acc0 = fma(as_f64(tid < sg.head || tid >= sg.tail0 ? gcol[tid] : col[tid]), wc, acc0);
+            if (in1) acc1 = fma(as_f64(r1 < sg.head || r1 >= sg.tail0 ? gcol[r1] : col[r1]), wc, acc1);
+          }
+        }
+      });
+      if (!ok) return;
+      double* out = f.tpart + (long)rg.crg * n + rg.r0;
+      if (tid < rg.rows) out[tid] = acc0;
+      if (r1 < rg.rows) out[r1] = acc1;
     }
     if (!group_sync(f, flag, [] {})) return;
-    // P3: t = sum of the chunk partials - c; |t|^2 and sum t
+    // P3: t = sum of the column ranges' partials - c; |t|^2 and sum t
     {
       const double cc = __ldcg(f.scal + SC_C);
       double* tcol = f.T + (long)a * n;
@@ -468,11 +609,11 @@ __global__ void __launch_bounds__(PT, 3)
 #pragma unroll
         for (int u = 0; u < 8; ++u) q[u] = 0.0;
         int k = 0;
-        for (; k + 7 < f.kt; k += 8) {
+        for (; k + 7 < f.Cc; k += 8) {
 #pragma unroll
           for (int u = 0; u < 8; ++u) q[u] += __ldcg(f.tpart + (long)(k + u) * n + i);
         }
-        for (; k < f.kt; ++k) q[0] += __ldcg(f.tpart + (long)k * n + i);
+        for (; k < f.Cc; ++k) q[0] += __ldcg(f.tpart + (long)k * n + i);
         const double t = (((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]))) - cc;
         tcol[i] = t;
         s2 = fma(t, t, s2);
@@ -487,21 +628,73 @@ __global__ void __launch_bounds__(PT, 3)
     }
     if (!group_sync(f, flag, [&] {
           reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
-          if (tid == 0) atomicExch(f.bar + 3, 0u);  // item counter of the loading pass
         }))
       return;
-    // P4: loading partials, items (row chunk, 32-column tile) claimed in order
+    // P4: loading partials of the region, p_part[rbk][cols] = X[rows, cols]^T t[rows],
+    // one warp per column, the stages backward
     {
-      const int jtiles = (p + 31) / 32;
-      const int items = jtiles * f.kp;
-      const double* tcol = f.T + (long)a * n;
-      for (;;) {
-        if (tid == 0) item_s = (int)atomicAdd(f.bar + 3, 1u);
-        __syncthreads();
-        const int it = item_s;
-        if (it >= items) break;
-        xtv_item<T>(f, X, it % f.kp, it / f.kp, tcol, psm);
-      }
+      const double* tcol = f.T + (long)a * n + rg.r0;
+      auto tv = [&] {
+        for (int r = tid; r < rg.rows; r += PT) aux[r] = __ldcg(tcol + r);
+      };
+      const int lane = tid & 31, warp = tid >> 5;
+      // each warp takes CPW columns of the stage; per column four
+      // interleaved sums over the rows in a fixed order, then the warp tree
+      constexpr int SC = Ring<T>::kCols;
+      constexpr int CPW = SC / (PT / 32);
+      const bool ok = stream_region(f, X, rg, true, seq, ring, ring_bars, ring_done, &ring_issued, flag, tv,
+                                    [&](int st, const unsigned char* slot) {
+        const int nc = min(SC, rg.cols - st * SC);
+        const int cb = rg.c0 + st * SC;
+        double q[CPW][4];
+        const T* col[CPW];
+#pragma unroll
+        for (int j = 0; j < CPW; ++j) {
+          const int cl = warp * CPW + j;
+          col[j] = reinterpret_cast<const T*>(slot + cl * Ring<T>::kColStride + rg.off(cb + cl));
+#pragma unroll
+          for (int u = 0; u < 4; ++u) q[j][u] = 0.0;
+        }
+        if (!rg.ends) {
+          int r = lane;
+          for (; r + 96 < rg.rows; r += 128) {
+            double tv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) tv[u] = aux[r + 32 * u];
+#pragma unroll
+            for (int j = 0; j < CPW; ++j)
+#pragma unroll
+              for (int u = 0; u < 4; ++u) q[j][u] = fma(as_f64(col[j][r + 32 * u]), tv[u], q[j][u]);
+          }
+          for (; r < rg.rows; r += 32) {
+            const double tv = aux[r];
+#pragma unroll
+            for (int j = 0; j < CPW; ++j) q[j][0] = fma(as_f64(col[j][r]), tv, q[j][0]);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < CPW; ++j) {
+            const int cl = warp * CPW + j;
+            if (cl >= nc) continue;
+            const Segment sg = segment(f, X, rg, cb + cl);
+            const T* gcol = X + (long)(cb + cl) * f.ld + rg.r0;  // rows outside the copy
+            auto xv = [&](int r) { return as_f64(r < sg.head || r >= sg.tail0 ? gcol[r] : col[j][r]); };
+            int r = lane;
+            for (; r + 96 < rg.rows; r += 128) {
+#pragma unroll
+              for (int u = 0; u < 4; ++u) q[j][u] = fma(xv(r + 32 * u), aux[r + 32 * u], q[j][u]);
+            }
+            for (; r < rg.rows; r += 32) q[j][0] = fma(xv(r), aux[r], q[j][0]);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < CPW; ++j) {
+          const int cl = warp * CPW + j;
+          const double v = warp_sum((q[j][0] + q[j][1]) + (q[j][2] + q[j][3]));
+          if (lane == 0 && cl < nc) f.ppart[(long)rg.rbk * p + cb + cl] = v;
+        }
+      });
+      if (!ok) return;
     }
     if (!group_sync(f, flag, [] {})) return;
     // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
@@ -521,13 +714,13 @@ __global__ void __launch_bounds__(PT, 3)
       const int j = j0 + jl;
       double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
       int k = 0;
-      for (; k + 3 < f.kp; k += 4) {
+      for (; k + 3 < f.Cr; k += 4) {
         q0 += __ldcg(f.ppart + (long)k * p + j);
         q1 += __ldcg(f.ppart + (long)(k + 1) * p + j);
         q2 += __ldcg(f.ppart + (long)(k + 2) * p + j);
         q3 += __ldcg(f.ppart + (long)(k + 3) * p + j);
       }
-      for (; k < f.kp; ++k) q0 += __ldcg(f.ppart + (long)k * p + j);
+      for (; k < f.Cr; ++k) q0 += __ldcg(f.ppart + (long)k * p + j);
       const double pr = (q0 + q1) + (q2 + q3);
       double rv = 0.0;
       for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + j + (long)c * p), zs[c], rv);
@@ -567,6 +760,7 @@ __global__ void __launch_bounds__(PT, 3)
         }))
       return;
     // P6: v = p - V h; partial v.v and S^T v
+    double* const hs = psm + kSmemDoubles;  // V^T p (a), beside psm in the idle ring
     for (int k = tid; k < a; k += PT) hs[k] = __ldcg(f.scal + SC_H + k);
     __syncthreads();
     double* vs = psm;  // v of this CTA's columns
@@ -616,7 +810,6 @@ __global__ void __launch_bounds__(PT, 3)
   }
 }
 
-int round_up(long v, long m) { return (int)((v + m - 1) / m * m); }
 
 }  // namespace
 
@@ -639,10 +832,29 @@ std::unique_ptr<PersistentPlan>*& persistent_deferral() {
   return sink;
 }
 
-int persistent_ctas(int n, int p) {
-  // from (n, p) only, never from the storage type: at most three per SM
+namespace {
+
+// Regions of a fit of n x p: Cr row blocks of rb rows times Cc column ranges
+// of pc columns (a function of the shape only); false when the shape does
+// not fit the persistent launch.
+bool persistent_grid(int n, int p, int& Cr, int& Cc, int& rb, int& pc) {
   const long elems = (long)n * p;
-  return (int)std::max(1L, std::min<long>(3L * num_sms(), (elems + (1L << 17) - 1) >> 17));
+  // about 2^15 elements per CTA: one CTA streams a few tens of GB/s, so
+  // even small fits spread over many SMs (the barriers cost little more)
+  const int c0 = (int)std::max(1L, std::min<long>(2L * num_sms(), (elems + (1L << 15) - 1) >> 15));
+  Cr = (n + kBlockRows - 1) / kBlockRows;
+  rb = round_up((n + Cr - 1) / Cr, 8);
+  Cr = (n + rb - 1) / rb;
+  Cc = std::max(c0 / Cr, (p + kAuxDoubles - 1) / kAuxDoubles);
+  pc = (p + Cc - 1) / Cc;
+  return (long)Cr * Cc <= 2L * num_sms();
+}
+
+}  // namespace
+
+int persistent_ctas(int n, int p) {
+  int Cr, Cc, rb, pc;
+  return persistent_grid(n, p, Cr, Cc, rb, pc) ? Cr * Cc : 0;
 }
 
 namespace {
@@ -654,13 +866,13 @@ int capacity_of() {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
         cudaFuncSetAttribute(persistent_simpls<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kSmemDoubles * (int)sizeof(double)) != cudaSuccess ||
+                             Ring<T>::kDynBytes) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, persistent_simpls<T>, PT,
-                                                      kSmemDoubles * sizeof(double)) != cudaSuccess) {
+                                                      Ring<T>::kDynBytes) != cudaSuccess) {
       cudaGetLastError();
       return 0;
     }
-    return v >= 3 ? v * num_sms() : 0;
+    return v >= 2 ? v * num_sms() : 0;
   }();
   return cap;
 }
@@ -681,7 +893,9 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   // dwarf its launch latency; the persistent launch pays off where the
   // passes are short and the per-component launches dominate.
   if ((long)n * p > kPersistMaxElements) return false;
-  const int C = persistent_ctas(n, p);
+  int Cr, Cc, rb, pc;
+  if (!persistent_grid(n, p, Cr, Cc, rb, pc)) return false;
+  const int C = Cr * Cc;
   const int cap = capacity_of<T>();
   if (cap == 0 || C > cap) return false;
   // per-CTA column ranges must fit the shared staging of P5/P6 (2048 each)
@@ -707,23 +921,10 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   f.v = ws.vec_p[3].get();
   f.flag = ws.flag.get();
   f.C = C;
-  // t pass: chunks of columns so that (row tiles of 1024) x chunks gives
-  // about four items per CTA; loading pass: 32-column tiles x row chunks
-  const int target = 4 * C;
-  const long row_tiles = (n + 1023) / 1024;
-  f.cc = std::max(32, std::min(kMaxXrCols, round_up((p * row_tiles + target - 1) / target, 32)));
-  f.kt = (p + f.cc - 1) / f.cc;
-  const int jtiles = (p + 31) / 32;
-  int kp = std::max((target + jtiles - 1) / jtiles, (n + kMaxXtvRows - 1) / kMaxXtvRows);
-  kp = std::max(1, std::min(kp, (n + 63) / 64));
-  f.rc = std::min(kMaxXtvRows, round_up((n + kp - 1) / kp, 64));
-  f.kp = (n + f.rc - 1) / f.rc;
-  constexpr int VN = sizeof(T) == 2 ? 8 : (sizeof(T) == 4 ? 4 : 2);
-  const bool aligned16 = reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % VN == 0;
-  f.vec = aligned16 ? VN : 1;
-  // octet loads in the loading pass: the same condition for every storage
-  // type (so BF16 and FP32 storage of the same values sum in one order)
-  f.oct = (reinterpret_cast<uintptr_t>(X) % 16 == 0 && ld % 8 == 0) ? 1 : 0;
+  f.Cr = Cr;
+  f.Cc = Cc;
+  f.rb = rb;
+  f.pc = pc;
   f.cslots = std::max(a + m, std::max(1 + m, m * (m + 1) / 2 + m));
   const PersistentWaitTest& wt = persistent_wait_test();
   f.barrier_cycles = wt.cycles > 0 ? wt.cycles : kBarrierCycles;
@@ -732,14 +933,15 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   // scratch of this fit (stream-ordered, freed behind the launch); the
   // kernel forms the Gram of S itself (into gpk) before the first component
   plan.elem = (int)sizeof(T);
+  f.elem = (int)sizeof(T);
   plan.S = std::move(S);
   f.S = plan.S.get();
-  plan.part.allocate((size_t)f.kt * n + (size_t)f.kp * p, stream);
+  plan.part.allocate((size_t)Cc * n + (size_t)Cr * p, stream);
   f.tpart = plan.part.get();
-  f.ppart = f.tpart + (size_t)f.kt * n;
+  f.ppart = f.tpart + (size_t)Cc * n;
   plan.cpart.allocate((size_t)C * f.cslots, stream);
   plan.scal.allocate((size_t)SC_H + kPersistMaxComponents + 8, stream);
-  plan.bar.allocate(4, stream);
+  plan.bar.allocate(2, stream);
   plan.bar.zero(stream);
   f.cpart = plan.cpart.get();
   f.scal = plan.scal.get();
@@ -770,8 +972,10 @@ void launch_persistent(const std::vector<PersistentPlan*>& plans, cudaStream_t s
   const void* fn = elem == 2 ? (const void*)persistent_simpls<bf16>
                  : elem == 4 ? (const void*)persistent_simpls<float>
                              : (const void*)persistent_simpls<double>;
-  FPLS_CHECK(cudaLaunchCooperativeKernel(fn, dim3(total), dim3(PT), args,
-                                         kSmemDoubles * sizeof(double), stream));
+  const int dyn = elem == 2 ? Ring<bf16>::kDynBytes
+                : elem == 4 ? Ring<float>::kDynBytes
+                            : Ring<double>::kDynBytes;
+  FPLS_CHECK(cudaLaunchCooperativeKernel(fn, dim3(total), dim3(PT), args, (size_t)dyn, stream));
   count_launch();
   FPLS_LAUNCH("persistent_simpls");
   // the descriptors are freed stream-ordered, behind the launch

@@ -25,17 +25,16 @@ struct PersistentFit {
   double *S, *R, *V, *Q, *T;
   double* gpk;              // packed Gram of S (m (m + 1) / 2)
   double *pv, *v;           // p
-  double* tpart;            // kt x n
-  double* ppart;            // kp x p
+  double* tpart;            // Cc x n (scores pass, one row per column range)
+  double* ppart;            // Cr x p (loading pass, one row per row block)
   double* cpart;            // C x cslots
   double* scal;             // scalar slots
-  unsigned* bar;            // [count, generation, score items, loading items]
+  unsigned* bar;            // [count, generation]
   int* flag;                // the fit's error flag
   int cta0, C;              // CTA range of this fit in the launch
-  int cc, kt;               // t pass: columns per chunk, chunks
-  int rc, kp;               // loading pass: rows per chunk, chunks
-  int vec;                  // rows per 16-byte load in the t pass (1: scalar)
-  int oct;                  // 8-row loads per lane in the loading pass
+  int Cr, rb;               // row blocks of X and their rows (C = Cr Cc)
+  int Cc, pc;               // column ranges of X and their columns
+  int elem;                 // bytes per element of X
   int cslots;               // per-CTA partial slots
   long long barrier_cycles; // bound of each barrier wait
   int absent_cta;           // test of the bounded waits: this CTA never arrives (-1: none)
@@ -52,7 +51,8 @@ struct PersistentPlan {
 
 // Whether the persistent path takes a fit with m responses and a components.
 bool persistent_supported(int m, int a);
-// CTAs a fit of n x p gets (a function of the shape only).
+// CTAs a fit of n x p gets (a function of the shape only; 0: the shape does
+// not fit a persistent launch).
 int persistent_ctas(int n, int p);
 // CTAs one launch can hold co-resident for a storage type (0: unavailable).
 int persistent_capacity(int elem);

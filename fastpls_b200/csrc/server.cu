@@ -100,7 +100,8 @@ bool batchable_fit(const Request& r) {
     return false;
   const int elem = r.precision == 16 ? 2 : r.precision == 32 ? 4 : 8;
   const int cap = persistent_capacity(elem);
-  return cap > 0 && persistent_ctas(f.n, f.p) <= cap;
+  const int ctas = persistent_ctas(f.n, f.p);
+  return cap > 0 && ctas > 0 && ctas <= cap;
 }
 
 size_t predict_footprint(int rows, const Model& m) {

@@ -17,21 +17,22 @@ namespace fpls {
 // rotation annihilates A[p, q] as in the classical cyclic method (tangent of
 // the smaller root of t^2 + 2 theta t = 1, theta = (a_qq - a_pp) / (2 a_pq)).
 // Stops at off <= 1e-30 diag (sums of squares) or at the rounding floor.
-// Returns the number of sweeps used (<= max_sweeps).
+// Returns the number of sweeps used (<= max_sweeps). Matrices of order
+// m <= warp_limit run in the first warp alone.
 constexpr int kJacobiMaxRotations = 64;
 
 // threads for a block that runs jacobi_eigen on an m x m matrix
 inline unsigned jacobi_threads(int m) { return m > 16 ? 256u : 64u; }
 
-__device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps = 40) {
+__device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps = 40, int warp_limit = 8) {
   __shared__ int rot_p[kJacobiMaxRotations], rot_q[kJacobiMaxRotations];
   __shared__ double rot_c[kJacobiMaxRotations], rot_s[kJacobiMaxRotations];
   __shared__ double red[32];
   if (m > 2 * kJacobiMaxRotations) return 0;  // callers keep m <= 128
-  // small matrices: the first warp alone (warp barriers are cheaper than
-  // block barriers on the latency-bound path); the other threads wait at the
-  // final barrier
-  const bool warp_only = m <= 8;
+  // small matrices (m <= warp_limit): the first warp alone (warp barriers
+  // are cheaper than block barriers on the latency-bound path); the other
+  // threads wait at the final barrier
+  const bool warp_only = m <= warp_limit;
   if (warp_only && threadIdx.x >= 32) {
     __syncthreads();
     return 0;
@@ -158,6 +159,68 @@ __device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps =
   }
   __syncthreads();
   return sweep;
+}
+
+// Dominant eigenpair of a symmetric positive semidefinite m x m matrix A
+// (shared, column-major), whole block. Repeated squaring: B = A / tr(A),
+// then B <- B^2 / tr(B^2). For B of trace one, tr(B^2) is the sum of its
+// squared eigenvalues, 1 exactly when B has rank one; each squaring raises
+// the eigenvalue ratios to the power two, so once tr(B^2) >= 1 - 1e-12 two
+// more squarings leave the non-dominant part below rounding. Then v = the
+// column of B with the largest diagonal entry, normalised (B = v v^T up to
+// rounding), and lam = v^T A v. On random SPD matrices up to 32 x 32
+// (clustered, rank one, condition 1e12) the residual |A v - lam v| / |A|
+// stays below 1e-15 in about 13 squarings (at most 64; an exactly repeated
+// leading eigenvalue yields a vector of its eigenspace). B and C are m x m
+// shared scratch, v (m) the shared output; lam is returned in every thread.
+// Returns false (nothing written) when tr(A) is not positive and finite.
+constexpr int kDominantMaxOrder = 64;  // callers size 3 m^2 + m shared doubles up to this order
+__device__ inline bool dominant_pair(const double* A, double* B, double* C, double* v, int m,
+                                     double& lam, int max_squarings = 64) {
+  const int tid = threadIdx.x, nt = blockDim.x, mm = m * m;
+  double tr = 0.0;
+  for (int i = 0; i < m; ++i) tr += A[i * (m + 1)];
+  if (!(tr > 0.0) || !isfinite(tr)) return false;
+  const double inv_tr = 1.0 / tr;
+  for (int k = tid; k < mm; k += nt) B[k] = A[k] * inv_tr;
+  __syncthreads();
+  int left = -1;  // squarings still to run once converged
+  for (int it = 0; it < max_squarings; ++it) {
+    for (int k = tid; k < mm; k += nt) {
+      const int i = k % m, j = k / m;
+      double acc = 0.0;
+      for (int l = 0; l < m; ++l) acc = fma(B[i + l * m], B[l + j * m], acc);
+      C[k] = acc;
+    }
+    __syncthreads();
+    double s = 0.0;  // tr(B^2), the same in every thread
+    for (int i = 0; i < m; ++i) s += C[i * (m + 1)];
+    if (left < 0 && 1.0 - s <= 1e-12) left = 2;
+    if (left == 0) break;
+    const double inv_s = 1.0 / s;
+    for (int k = tid; k < mm; k += nt) B[k] = C[k] * inv_s;
+    __syncthreads();
+    if (left > 0) --left;
+  }
+  int j = 0;
+  for (int i = 1; i < m; ++i)
+    if (B[i * (m + 1)] > B[j * (m + 1)]) j = i;
+  double n2 = 0.0;
+  for (int i = 0; i < m; ++i) n2 = fma(B[i + j * m], B[i + j * m], n2);
+  const double inv_n = 1.0 / sqrt(n2);
+  __syncthreads();  // every thread has read B
+  for (int i = tid; i < m; i += nt) v[i] = B[i + j * m] * inv_n;
+  __syncthreads();
+  for (int i = tid; i < m; i += nt) {
+    double acc = 0.0;
+    for (int l = 0; l < m; ++l) acc = fma(A[i + l * m], v[l], acc);
+    C[i] = acc;
+  }
+  __syncthreads();
+  lam = 0.0;
+  for (int i = 0; i < m; ++i) lam = fma(v[i], C[i], lam);
+  __syncthreads();
+  return true;
 }
 
 // In-place Cholesky (lower) of an SPD k x k matrix A (+ ridge on the
