@@ -598,44 +598,44 @@ __global__ void __launch_bounds__(PT, 2)
       if (r1 < rg.rows) out[r1] = acc1;
     }
     if (!group_sync(f, flag, [] {})) return;
-    // P3: t = sum of the column ranges' partials - c; |t|^2 and sum t
+    // P4: loading partials of the region, p_part[rbk][cols] = X[rows, cols]^T t[rows],
+    // the stages backward. While the first stages are in flight each CTA
+    // forms t for its row block: t = sum of the column ranges' partials - c
+    // (the CTAs of column range 0 also store T[:, a] and the |t|^2, sum t
+    // partials of their block).
     {
       const double cc = __ldcg(f.scal + SC_C);
-      double* tcol = f.T + (long)a * n;
-      double s2 = 0.0, s1 = 0.0;
-      for (int i = cta * PT + tid; i < n; i += C * PT) {
-        // eight interleaved partial sums (more loads in flight), fixed order
-        double q[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) q[u] = 0.0;
-        int k = 0;
-        for (; k + 7 < f.Cc; k += 8) {
-#pragma unroll
-          for (int u = 0; u < 8; ++u) q[u] += __ldcg(f.tpart + (long)(k + u) * n + i);
-        }
-        for (; k < f.Cc; ++k) q[0] += __ldcg(f.tpart + (long)k * n + i);
-        const double t = (((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]))) - cc;
-        tcol[i] = t;
-        s2 = fma(t, t, s2);
-        s1 += t;
-      }
-      s2 = cta_sum(s2, red);
-      s1 = cta_sum(s1, red);
-      if (tid == 0) {
-        f.cpart[(long)cta * f.cslots] = s2;
-        f.cpart[(long)cta * f.cslots + 1] = s1;
-      }
-    }
-    if (!group_sync(f, flag, [&] {
-          reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
-        }))
-      return;
-    // P4: loading partials of the region, p_part[rbk][cols] = X[rows, cols]^T t[rows],
-    // one warp per column, the stages backward
-    {
-      const double* tcol = f.T + (long)a * n + rg.r0;
+      double* tcol = f.T + (long)a * n + rg.r0;
       auto tv = [&] {
-        for (int r = tid; r < rg.rows; r += PT) aux[r] = __ldcg(tcol + r);
+        double s2 = 0.0, s1 = 0.0;
+        for (int r = tid; r < rg.rows; r += PT) {
+          const long i = rg.r0 + r;
+          // eight interleaved partial sums (more loads in flight), fixed order
+          double q[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) q[u] = 0.0;
+          int k = 0;
+          for (; k + 7 < f.Cc; k += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) q[u] += __ldcg(f.tpart + (long)(k + u) * n + i);
+          }
+          for (; k < f.Cc; ++k) q[0] += __ldcg(f.tpart + (long)k * n + i);
+          const double t = (((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]))) - cc;
+          aux[r] = t;
+          if (rg.crg == 0) {
+            tcol[r] = t;
+            s2 = fma(t, t, s2);
+            s1 += t;
+          }
+        }
+        if (rg.crg == 0) {
+          s2 = cta_sum(s2, red);
+          s1 = cta_sum(s1, red);
+        }
+        if (tid == 0) {
+          f.cpart[(long)cta * f.cslots] = rg.crg == 0 ? s2 : 0.0;
+          f.cpart[(long)cta * f.cslots + 1] = rg.crg == 0 ? s1 : 0.0;
+        }
       };
       const int lane = tid & 31, warp = tid >> 5;
       // each warp takes CPW columns of the stage; per column four
@@ -696,7 +696,10 @@ __global__ void __launch_bounds__(PT, 2)
       });
       if (!ok) return;
     }
-    if (!group_sync(f, flag, [] {})) return;
+    if (!group_sync(f, flag, [&] {
+          reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
+        }))
+      return;
     // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
     if (tid == 0) {
       const double t2 = __ldcg(f.scal + SC_T2);
