@@ -67,37 +67,92 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
-// Barrier of the fit's CTAs. Every thread of the CTA calls it after writing
-// its partials. The last CTA to arrive runs reduce() (whole CTA, reading the
-// other CTAs' partials with L1-bypassing loads) before releasing the rest.
-// Returns false when a wait ran out (flag set to 5); the caller returns.
-template <class F>
-__device__ bool group_sync(const Fit& f, int* flag, F&& reduce) {
-  __shared__ int last_s, ok_s;
+// Barrier of the fit's CTAs with a deterministic reduction of their
+// partials (slots 0 .. count-1 of each CTA's row of cpart). Every thread of
+// the CTA calls it after writing its partials; the reducing CTA calls
+// store(k, sum) in the thread of slot k, then (after a CTA barrier) after(),
+// and releases everyone. Returns false when a wait ran out (flag set to 5);
+// the caller returns.
+//
+// Up to kFlatSlots slots: every CTA arrives at one counter and the last one
+// reduces, Q = PT / count threads per slot, thread q of slot k summing CTAs
+// q, q + Q, ... in order, then the Q sums in order. Wider reductions arrive
+// in groups of kBarGroup CTAs: the last CTA of a group sums the group's
+// partials (thread k: slot k, the group's CTAs in order) into its row of
+// gpart and arrives at the top counter; the last group's reducer sums the
+// group rows in order.
+constexpr int kBarGroup = 32;
+constexpr int kFlatSlots = 64;
+template <class S, class A>
+__device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& after) {
+  __shared__ int role_s, ok_s;  // role: 0 waits, 1 reduced its group, 2 reduces all
+  __shared__ unsigned gen_s;
+  // per-thread sums of the flat reduction: dynamic shared memory past psm and
+  // hs (the ring is idle at barriers; a static array would be duplicated per
+  // instantiation)
+  extern __shared__ __align__(16) double dyn_smem[];
+  double* const part_s = dyn_smem + kSmemDoubles + kPersistMaxComponents;
+  const bool flat = count <= kFlatSlots;
+  const int cta = (int)blockIdx.x - f.cta0;
+  const int g = cta / kBarGroup;
+  const int ngroups = (f.C + kBarGroup - 1) / kBarGroup;
+  const int gsize = min(kBarGroup, f.C - g * kBarGroup);
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    const unsigned gen = ld_acquire(f.bar + 1);
+    gen_s = ld_acquire(f.bar + 1);
     __threadfence();
-    const unsigned ticket = atomicAdd(f.bar, 1u);
-    last_s = ticket == (unsigned)f.C - 1u;
     ok_s = 1;
-    if (!last_s) {
-      const long long t0 = clock64();
-      while (ld_acquire(f.bar + 1) == gen) {
-        if (clock64() - t0 > f.barrier_cycles) {
-          flag_error(flag, 5);
-          ok_s = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
+    if (flat) role_s = atomicAdd(f.bar, 1u) == (unsigned)f.C - 1u ? 2 : 0;
+    else role_s = atomicAdd(f.bar + 2 + g, 1u) == (unsigned)gsize - 1u ? 1 : 0;
   }
   __syncthreads();
-  if (last_s) {
+  if (role_s == 1) {
     __threadfence();
-    reduce();
+    for (int k = threadIdx.x; k < count; k += PT) {
+      const double* src = f.cpart + (long)g * kBarGroup * f.cslots + k;
+      double sum = 0.0;
+#pragma unroll 8
+      for (int c = 0; c < gsize; ++c) sum += __ldcg(src + (long)c * f.cslots);
+      f.gpart[(long)g * f.cslots + k] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      atomicExch(f.bar + 2 + g, 0u);
+      __threadfence();
+      if (atomicAdd(f.bar, 1u) == (unsigned)ngroups - 1u) role_s = 2;
+    }
+    __syncthreads();
+  }
+  if (role_s == 2) {
+    __threadfence();
+    if (flat) {
+      if (count > 0) {
+        const int Q = PT / count;
+        const int t = threadIdx.x;
+        if (t < Q * count) {
+          const int k = t % count, q = t / count;
+          double sum = 0.0;
+#pragma unroll 8
+          for (int c = q; c < f.C; c += Q) sum += __ldcg(f.cpart + (long)c * f.cslots + k);
+          part_s[t] = sum;
+        }
+        __syncthreads();
+        for (int k = t; k < count; k += PT) {
+          double sum = 0.0;
+          for (int q = 0; q < Q; ++q) sum += part_s[q * count + k];
+          store(k, sum);
+        }
+      }
+    } else {
+      for (int k = threadIdx.x; k < count; k += PT) {
+        double sum = 0.0;
+        for (int q = 0; q < ngroups; ++q) sum += __ldcg(f.gpart + (long)q * f.cslots + k);
+        store(k, sum);
+      }
+    }
+    __syncthreads();
+    after();
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -105,10 +160,25 @@ __device__ bool group_sync(const Fit& f, int* flag, F&& reduce) {
       __threadfence();
       atomicAdd(f.bar + 1, 1u);
     }
+  } else if (threadIdx.x == 0) {
+    const long long t0 = clock64();
+    while (ld_acquire(f.bar + 1) == gen_s) {
+      if (clock64() - t0 > f.barrier_cycles) {
+        flag_error(flag, 5);
+        ok_s = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
   }
   __syncthreads();
   __threadfence();
   return ok_s != 0;
+}
+
+// Barrier without partials.
+__device__ __forceinline__ bool group_sync(const Fit& f, int* flag) {
+  return group_sync(f, flag, 0, [](int, double) {}, [] {});
 }
 
 // CTA-level sum; every thread receives it.
@@ -119,31 +189,6 @@ __device__ __forceinline__ void col_range(int p, int C, int c, int& j0, int& j1)
   const int per = (p + C - 1) / C;
   j0 = min(p, c * per);
   j1 = min(p, j0 + per);
-}
-
-// Sums over the C per-CTA partials of slots 0 .. count-1 (stride cslots),
-// by the whole CTA: warp w takes slots w, w + 8, ...; lane l adds the
-// partials of CTAs l, l + 32, ... in order (the first kReduceLoads of them
-// loaded together), then the warp's shuffle tree (a fixed order).
-// store(k, sum) runs on lane 0.
-constexpr int kReduceLoads = 12;
-template <class F>
-__device__ __forceinline__ void reduce_slots(const Fit& f, int count, F&& store) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = warp; k < count; k += PT / 32) {
-    double v[kReduceLoads];
-#pragma unroll
-    for (int i = 0; i < kReduceLoads; ++i) {
-      const int c = lane + 32 * i;
-      v[i] = c < f.C ? __ldcg(f.cpart + (long)c * f.cslots + k) : 0.0;
-    }
-    double s = 0.0;
-#pragma unroll
-    for (int i = 0; i < kReduceLoads; ++i) s += v[i];
-    for (int c = lane + 32 * kReduceLoads; c < f.C; c += 32) s += __ldcg(f.cpart + (long)c * f.cslots + k);
-    s = warp_sum(s);
-    if (lane == 0) store(k, s);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -178,10 +223,11 @@ struct Ring {
 };
 constexpr int kMaxRingStages = 8;
 static_assert(kBlockRows == 2 * PT, "the scores pass gives each thread two rows of a block");
-static_assert(Ring<bf16>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8 &&
-                  Ring<float>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8 &&
-                  Ring<double>::kBytes >= (kSmemDoubles + kPersistMaxComponents) * 8,
-              "the vector phases use the first kSmemDoubles + kPersistMaxComponents doubles of the ring");
+static_assert(Ring<bf16>::kBytes >= (kSmemDoubles + kPersistMaxComponents + PT) * 8 &&
+                  Ring<float>::kBytes >= (kSmemDoubles + kPersistMaxComponents + PT) * 8 &&
+                  Ring<double>::kBytes >= (kSmemDoubles + kPersistMaxComponents + PT) * 8,
+              "the vector phases and barriers use the first kSmemDoubles + kPersistMaxComponents + PT "
+              "doubles of the ring");
 static_assert(Ring<bf16>::kCols <= 32 && Ring<float>::kCols <= 32 && Ring<double>::kCols <= 32 &&
                   Ring<float>::kCols % (PT / 32) == 0 && Ring<double>::kCols % (PT / 32) == 0 &&
                   Ring<bf16>::kCols % (PT / 32) == 0,
@@ -199,14 +245,16 @@ __device__ __forceinline__ void ring_expect(uint64_t* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
+// One try of the wait; the thread may sleep up to 20 us in it (the
+// suspend-time hint) until the phase completes, instead of spinning.
 __device__ __forceinline__ bool ring_try(uint64_t* bar, unsigned parity) {
   uint32_t done;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
       : "memory");
   return done != 0;
 }
@@ -486,7 +534,7 @@ __global__ void __launch_bounds__(PT, 2)
   __shared__ double scal_s[4];
   int fi = 0;
   while (fi + 1 < nfits && (int)blockIdx.x >= fits[fi + 1].cta0) ++fi;
-  const Fit f = fits[fi];
+  const Fit& f = fits[fi];  // read through the read-only path as needed (fewer live registers)
   int* const flag = f.flag;
   const int cta = (int)blockIdx.x - f.cta0;
   if (cta == f.absent_cta) return;  // bounded-wait test only
@@ -515,38 +563,37 @@ __global__ void __launch_bounds__(PT, 2)
   for (int a = 0; a < f.a; ++a) {
     // B0: Gram and u of the (deflated) S, the direction z / sqrt(lambda), and
     // the score offset c = mean . (S z / scale) = z . u
-    if (!group_sync(f, flag, [&] {
-          double* A = psm;               // m x m Gram
-          double* B = A + m * m;         // squaring scratch
-          double* Cs = B + m * m;
-          double* vd = Cs + m * m;       // dominant eigenvector
-          double* us = vd + m;           // u
-          reduce_slots(f, G + m, [&](int k, double v) {
-            if (k < G) {
-              int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
-              while (c * (c + 1) / 2 > k) --c;
-              while ((c + 1) * (c + 2) / 2 <= k) ++c;
-              const int d = k - c * (c + 1) / 2;
-              A[c + d * m] = v;
-              A[d + c * m] = v;
-              f.gpk[k] = v;
-            } else {
-              us[k - G] = v;
-            }
-          });
-          __syncthreads();
-          direction_step(f, A, B, Cs, vd, us, flag);
-        }))
-      return;
+    {
+      double* A = psm;               // m x m Gram
+      double* B = A + m * m;         // squaring scratch
+      double* Cs = B + m * m;
+      double* vd = Cs + m * m;       // dominant eigenvector
+      double* us = vd + m;           // u
+      auto store = [&](int k, double v) {
+        if (k < G) {
+          int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
+          while (c * (c + 1) / 2 > k) --c;
+          while ((c + 1) * (c + 2) / 2 <= k) ++c;
+          const int d = k - c * (c + 1) / 2;
+          A[c + d * m] = v;
+          A[d + c * m] = v;
+          f.gpk[k] = v;
+        } else {
+          us[k - G] = v;
+        }
+      };
+      if (!group_sync(f, flag, G + m, store, [&] { direction_step(f, A, B, Cs, vd, us, flag); })) return;
+    }
     for (int c = tid; c < m; c += PT) zs[c] = __ldcg(f.scal + SC_Z + c);
     __syncthreads();
     // P2: score partials of the region, t_part[crg][rows] = X[rows, cols] rt[cols]
     // with rt = (S z) / scale (S is not deflated until P7)
     {
-      // thread rows tid and tid + 256 of the row block (kBlockRows = 2 PT),
-      // the region's columns in order
+      // thread rows tid and tid + 256 of the row block (kBlockRows = 2 PT);
+      // each row's sum over the region's columns runs as four interleaved
+      // sums (column j into sum j % 4) added at the end, a fixed order
       constexpr int SC = Ring<T>::kCols;
-      double acc0 = 0.0, acc1 = 0.0;
+      double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
       const int r1 = tid + PT;
       const bool in0 = tid < rg.rows, in1 = r1 < rg.rows;
       auto rt = [&] {
@@ -568,36 +615,37 @@ __global__ void __launch_bounds__(PT, 2)
             const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
             x[c] = in0 ? as_f64(col[tid]) : 0.0;
           }
-          double a0 = acc0;
 #pragma unroll
-          for (int c = 0; c < SC; ++c) a0 = fma(x[c], w[c], a0);
-          acc0 = a0;
+          for (int c = 0; c < SC; ++c) acc0[c & 3] = fma(x[c], w[c], acc0[c & 3]);
 #pragma unroll
           for (int c = 0; c < SC; ++c) {
             const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
             x[c] = in1 ? as_f64(col[r1]) : 0.0;
           }
-          double a1 = acc1;
 #pragma unroll
-          for (int c = 0; c < SC; ++c) a1 = fma(x[c], w[c], a1);
-          acc1 = a1;
+          for (int c = 0; c < SC; ++c) acc1[c & 3] = fma(x[c], w[c], acc1[c & 3]);
         } else {
-          for (int c = 0; c < nc; ++c) {
-            const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
-            const Segment sg = segment(f, X, rg, cb + c);
-            const T* gcol = X + (long)(cb + c) * f.ld + rg.r0;  // rows outside the copy
-            const double wc = w[c];
-            if (in0) acc0 = fma(as_f64(tid < sg.head || tid >= sg.tail0 ? gcol[tid] : col[tid]), wc, acc0);
-            if (in1) acc1 = fma(as_f64(r1 < sg.head || r1 >= sg.tail0 ? gcol[r1] : col[r1]), wc, acc1);
+          for (int c4 = 0; c4 < nc; c4 += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int c = c4 + u;
+              if (c >= nc) break;
+              const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
+              const Segment sg = segment(f, X, rg, cb + c);
+              const T* gcol = X + (long)(cb + c) * f.ld + rg.r0;  // rows outside the copy
+              const double wc = w[c];
+              if (in0) acc0[u] = fma(as_f64(tid < sg.head || tid >= sg.tail0 ? gcol[tid] : col[tid]), wc, acc0[u]);
+              if (in1) acc1[u] = fma(as_f64(r1 < sg.head || r1 >= sg.tail0 ? gcol[r1] : col[r1]), wc, acc1[u]);
+            }
           }
         }
       });
       if (!ok) return;
       double* out = f.tpart + (long)rg.crg * n + rg.r0;
-      if (tid < rg.rows) out[tid] = acc0;
-      if (r1 < rg.rows) out[r1] = acc1;
+      if (tid < rg.rows) out[tid] = (acc0[0] + acc0[1]) + (acc0[2] + acc0[3]);
+      if (r1 < rg.rows) out[r1] = (acc1[0] + acc1[1]) + (acc1[2] + acc1[3]);
     }
-    if (!group_sync(f, flag, [] {})) return;
+    if (!group_sync(f, flag)) return;
     // P4: loading partials of the region, p_part[rbk][cols] = X[rows, cols]^T t[rows],
     // the stages backward. While the first stages are in flight each CTA
     // forms t for its row block: t = sum of the column ranges' partials - c
@@ -696,9 +744,7 @@ __global__ void __launch_bounds__(PT, 2)
       });
       if (!ok) return;
     }
-    if (!group_sync(f, flag, [&] {
-          reduce_slots(f, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; });
-        }))
+    if (!group_sync(f, flag, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; }, [] {}))
       return;
     // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
     if (tid == 0) {
@@ -751,16 +797,16 @@ __global__ void __launch_bounds__(PT, 2)
         if (lane == 0) f.cpart[(long)cta * f.cslots + k] = s;
       }
     }
-    if (!group_sync(f, flag, [&] {
-          reduce_slots(f, a + m, [&](int k, double v) {
-            if (k < a) {
-              f.scal[SC_H + k] = v;
-            } else {
-              f.scal[SC_Q + k - a] = v;
-              f.Q[(k - a) + (long)a * m] = v;
-            }
-          });
-        }))
+    if (!group_sync(f, flag, a + m,
+                    [&](int k, double v) {
+                      if (k < a) {
+                        f.scal[SC_H + k] = v;
+                      } else {
+                        f.scal[SC_Q + k - a] = v;
+                        f.Q[(k - a) + (long)a * m] = v;
+                      }
+                    },
+                    [] {}))
       return;
     // P6: v = p - V h; partial v.v and S^T v
     double* const hs = psm + kSmemDoubles;  // V^T p (a), beside psm in the idle ring
@@ -790,12 +836,12 @@ __global__ void __launch_bounds__(PT, 2)
       }
       if (tid == 0) f.cpart[(long)cta * f.cslots] = vvp;
     }
-    if (!group_sync(f, flag, [&] {
-          reduce_slots(f, 1 + m, [&](int k, double v) {
-            if (k == 0) f.scal[SC_VV] = v;
-            else f.scal[SC_SV + k - 1] = v;
-          });
-        }))
+    if (!group_sync(f, flag, 1 + m,
+                    [&](int k, double v) {
+                      if (k == 0) f.scal[SC_VV] = v;
+                      else f.scal[SC_SV + k - 1] = v;
+                    },
+                    [] {}))
       return;
     // P7: V[:, a], deflate S, partials of the Gram and u of the deflated S;
     // T[:, a] /= |t|
@@ -942,11 +988,13 @@ bool plan_simpls_persistent(const T* X, int n, int p, long ld, int m, int a, Dev
   plan.part.allocate((size_t)Cc * n + (size_t)Cr * p, stream);
   f.tpart = plan.part.get();
   f.ppart = f.tpart + (size_t)Cc * n;
-  plan.cpart.allocate((size_t)C * f.cslots, stream);
+  const int ngroups = (C + kBarGroup - 1) / kBarGroup;
+  plan.cpart.allocate((size_t)(C + ngroups) * f.cslots, stream);
   plan.scal.allocate((size_t)SC_H + kPersistMaxComponents + 8, stream);
-  plan.bar.allocate(2, stream);
+  plan.bar.allocate(2 + ngroups, stream);
   plan.bar.zero(stream);
   f.cpart = plan.cpart.get();
+  f.gpart = f.cpart + (size_t)C * f.cslots;
   f.scal = plan.scal.get();
   f.bar = plan.bar.get();
   model.a = a;

@@ -27,9 +27,10 @@ struct PersistentFit {
   double *pv, *v;           // p
   double* tpart;            // Cc x n (scores pass, one row per column range)
   double* ppart;            // Cr x p (loading pass, one row per row block)
-  double* cpart;            // C x cslots
+  double* cpart;            // C x cslots (per-CTA partials)
+  double* gpart;            // ceil(C / 32) x cslots (per-group sums)
   double* scal;             // scalar slots
-  unsigned* bar;            // [count, generation]
+  unsigned* bar;            // [groups arrived, generation, CTAs arrived per group...]
   int* flag;                // the fit's error flag
   int cta0, C;              // CTA range of this fit in the launch
   int Cr, rb;               // row blocks of X and their rows (C = Cr Cc)
