@@ -133,8 +133,8 @@ __global__ void direction_kernel(const double* __restrict__ gpk, int m,
   __syncthreads();
   if (count == 1 && m <= kDominantMaxOrder) {
     // one direction: the dominant pair alone (repeated squaring)
-    double* C = E + m * m;
-    double* v = C + m * m;
+    double* C = E + m * m;      // m^2 + 1
+    double* v = C + m * m + 1;  // m + 1
     double lam = 0.0;
     const bool found = dominant_pair(A, E, C, v, m, lam);
     if (threadIdx.x == 0) {
@@ -487,7 +487,7 @@ __global__ void s_times_z(const double* __restrict__ S, int p, int m,
 void dominant_direction(const double* S, int p, int m, const double* gpk,
                         double* zs, double* w, Workspace& ws, cudaStream_t s) {
   // A, B, C, v of the dominant pair (one direction), or A, E of the Jacobi sweeps
-  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m : 2 * (size_t)m * m) * sizeof(double);
+  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m + 2 : 2 * (size_t)m * m) * sizeof(double);
   if (smem_dir > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(direction_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dir));
   direction_kernel<<<1, jacobi_threads(m), smem_dir, s>>>(gpk, m, zs, nullptr, ws.flag.get(), 1);
@@ -577,7 +577,7 @@ void fit_simpls(const T* X, int n, int p, long ld, const double* Yc,
   const size_t smem3 = ((size_t)jb3 * m + (size_t)m * (m + 1) / 2) * sizeof(double);
   const unsigned g1 = ceil_div(p, TB);
   // A, B, C, v of the dominant pair (one direction), or A, E of the Jacobi sweeps
-  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m : 2 * (size_t)m * m) * sizeof(double);
+  const size_t smem_dir = (m <= kDominantMaxOrder ? 3 * (size_t)m * m + m + 2 : 2 * (size_t)m * m) * sizeof(double);
   if (smem3 > 48 * 1024)
     FPLS_CHECK(cudaFuncSetAttribute(tail3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3));
   if (smem_dir > 48 * 1024)

@@ -274,6 +274,15 @@ __device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigne
       : "memory");
 }
 
+template <class T>
+__device__ __forceinline__ T tzero() {
+  return T(0);
+}
+template <>
+__device__ __forceinline__ bf16 tzero<bf16>() {
+  return __ushort_as_bfloat16((unsigned short)0);
+}
+
 // The region of this CTA.
 struct Region {
   long r0;   // first row
@@ -348,6 +357,20 @@ __device__ __forceinline__ Segment segment(const Fit& f, const T* X, const Regio
     sg.tail0 = sg.hi > sg.lo ? (int)((sg.hi - sg.g) / sizeof(T)) : sg.head;
   }
   return sg;
+}
+
+// Whether stage st holds a segment whose cover leaves X (the region's
+// first or last segments only; the same test as Region::ends per stage).
+template <class T>
+__device__ __forceinline__ bool stage_ends(const Fit& f, const T* X, const Region& g, int st) {
+  if (!g.ends) return false;
+  const int cb = g.c0 + st * Ring<T>::kCols;
+  const int ce = min(g.c0 + g.cols, cb + Ring<T>::kCols) - 1;
+  const uintptr_t x0 = reinterpret_cast<uintptr_t>(X);
+  const uintptr_t x1 = reinterpret_cast<uintptr_t>(X + (long)(f.p - 1) * f.ld + f.n);
+  const uintptr_t first = reinterpret_cast<uintptr_t>(X + (long)cb * f.ld + g.r0);
+  const uintptr_t last = reinterpret_cast<uintptr_t>(X + (long)ce * f.ld + g.r0 + g.rows);
+  return (first & ~(uintptr_t)15) < x0 || ((last + 15) & ~(uintptr_t)15) > x1;
 }
 
 // Warp 0: the bulk copies of stage `st` into `slot`, one lane per column,
@@ -566,9 +589,9 @@ __global__ void __launch_bounds__(PT, 2)
     {
       double* A = psm;               // m x m Gram
       double* B = A + m * m;         // squaring scratch
-      double* Cs = B + m * m;
-      double* vd = Cs + m * m;       // dominant eigenvector
-      double* us = vd + m;           // u
+      double* Cs = B + m * m;        // m^2 + 1
+      double* vd = Cs + m * m + 1;   // dominant eigenvector (m + 1)
+      double* us = vd + m + 1;       // u
       auto store = [&](int k, double v) {
         if (k < G) {
           int c = (int)((sqrt(8.0 * k + 1.0) - 1.0) * 0.5);
@@ -608,22 +631,23 @@ __global__ void __launch_bounds__(PT, 2)
         const int nc = min(SC, rg.cols - st * SC);
         const double* w = aux + st * SC;
         const int cb = rg.c0 + st * SC;
-        if (nc == SC && !rg.ends) {
-          double x[SC];
+        if (nc == SC && !stage_ends(f, X, rg, st)) {
+          // the stage's values kept in the storage type (fewer registers,
+          // all loads ahead of the FMAs); rows past the block read stale
+          // shared memory and their sums are never stored
+          T x0[SC], x1[SC];
 #pragma unroll
           for (int c = 0; c < SC; ++c) {
             const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
-            x[c] = in0 ? as_f64(col[tid]) : 0.0;
+            x0[c] = col[tid];
+            x1[c] = col[r1];
           }
-#pragma unroll
-          for (int c = 0; c < SC; ++c) acc0[c & 3] = fma(x[c], w[c], acc0[c & 3]);
 #pragma unroll
           for (int c = 0; c < SC; ++c) {
-            const T* col = reinterpret_cast<const T*>(slot + c * Ring<T>::kColStride + rg.off(cb + c));
-            x[c] = in1 ? as_f64(col[r1]) : 0.0;
+            const double wc = w[c];
+            acc0[c & 3] = fma(as_f64(x0[c]), wc, acc0[c & 3]);
+            acc1[c & 3] = fma(as_f64(x1[c]), wc, acc1[c & 3]);
           }
-#pragma unroll
-          for (int c = 0; c < SC; ++c) acc1[c & 3] = fma(x[c], w[c], acc1[c & 3]);
         } else {
           for (int c4 = 0; c4 < nc; c4 += 4) {
 #pragma unroll
@@ -676,6 +700,7 @@ __global__ void __launch_bounds__(PT, 2)
             s1 += t;
           }
         }
+        for (int r = rg.rows + tid; r < kBlockRows; r += PT) aux[r] = 0.0;
         if (rg.crg == 0) {
           s2 = cta_sum(s2, red);
           s1 = cta_sum(s1, red);
@@ -703,21 +728,26 @@ __global__ void __launch_bounds__(PT, 2)
 #pragma unroll
           for (int u = 0; u < 4; ++u) q[j][u] = 0.0;
         }
-        if (!rg.ends) {
-          int r = lane;
-          for (; r + 96 < rg.rows; r += 128) {
-            double tv[4];
+        // rows lane + 32 u + 128 i (i < kBlockRows / 128) into sum u of each
+        // column, a fixed order; past the block's rows t is staged as zero
+        // and x selected as zero, so those terms add exactly nothing
+        constexpr int RI = kBlockRows / 128;
+        if (!stage_ends(f, X, rg, st)) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) tv[u] = aux[r + 32 * u];
+          for (int i = 0; i < RI; ++i) {
+            double tv[4];
+            T xr[CPW][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int r = lane + 128 * i + 32 * u;
+              tv[u] = aux[r];
+#pragma unroll
+              for (int j = 0; j < CPW; ++j) xr[j][u] = r < rg.rows ? col[j][r] : tzero<T>();
+            }
 #pragma unroll
             for (int j = 0; j < CPW; ++j)
 #pragma unroll
-              for (int u = 0; u < 4; ++u) q[j][u] = fma(as_f64(col[j][r + 32 * u]), tv[u], q[j][u]);
-          }
-          for (; r < rg.rows; r += 32) {
-            const double tv = aux[r];
-#pragma unroll
-            for (int j = 0; j < CPW; ++j) q[j][0] = fma(as_f64(col[j][r]), tv, q[j][0]);
+              for (int u = 0; u < 4; ++u) q[j][u] = fma(as_f64(xr[j][u]), tv[u], q[j][u]);
           }
         } else {
 #pragma unroll
@@ -726,13 +756,15 @@ __global__ void __launch_bounds__(PT, 2)
             if (cl >= nc) continue;
             const Segment sg = segment(f, X, rg, cb + cl);
             const T* gcol = X + (long)(cb + cl) * f.ld + rg.r0;  // rows outside the copy
-            auto xv = [&](int r) { return as_f64(r < sg.head || r >= sg.tail0 ? gcol[r] : col[j][r]); };
-            int r = lane;
-            for (; r + 96 < rg.rows; r += 128) {
 #pragma unroll
-              for (int u = 0; u < 4; ++u) q[j][u] = fma(xv(r + 32 * u), aux[r + 32 * u], q[j][u]);
-            }
-            for (; r < rg.rows; r += 32) q[j][0] = fma(xv(r), aux[r], q[j][0]);
+            for (int i = 0; i < RI; ++i)
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int r = lane + 128 * i + 32 * u;
+                const double x =
+                    r < rg.rows ? as_f64(r < sg.head || r >= sg.tail0 ? gcol[r] : col[j][r]) : 0.0;
+                q[j][u] = fma(x, aux[r], q[j][u]);
+              }
           }
         }
 #pragma unroll

@@ -172,18 +172,50 @@ __device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps =
 // (clustered, rank one, condition 1e12) the residual |A v - lam v| / |A|
 // stays below 1e-15 in about 13 squarings (at most 64; an exactly repeated
 // leading eigenvalue yields a vector of its eigenspace). B and C are m x m
-// shared scratch, v (m) the shared output; lam is returned in every thread.
-// Returns false (nothing written) when tr(A) is not positive and finite.
-constexpr int kDominantMaxOrder = 64;  // callers size 3 m^2 + m shared doubles up to this order
+// shared scratch (C with one extra slot), v (m + 1 slots) the shared
+// output; lam is returned in every thread. Returns false when tr(A) is not
+// positive and finite.
+constexpr int kDominantMaxOrder = 64;  // callers size 3 m^2 + m + 2 shared doubles up to this order
 __device__ inline bool dominant_pair(const double* A, double* B, double* C, double* v, int m,
                                      double& lam, int max_squarings = 64) {
-  const int tid = threadIdx.x, nt = blockDim.x, mm = m * m;
+  // orders up to 8: the first warp alone with warp barriers (the squarings
+  // are a few FMAs per lane; block barriers would dominate); the other
+  // warps wait at the final barrier and read lam from the shared v slot
+  const bool one_warp = m <= 8;
+  if (one_warp && threadIdx.x >= 32) {
+    __syncthreads();
+    const bool found = v[m] != 0.0;
+    lam = C[m];
+    __syncthreads();
+    return found;
+  }
+  const int tid = threadIdx.x, nt = one_warp ? 32 : blockDim.x, mm = m * m;
+  auto sync = [&] {
+    if (one_warp) __syncwarp();
+    else __syncthreads();
+  };
+  // the result for the other warps (one_warp): v[m] = found, C[m] = lam
+  auto finish = [&](bool found, double l) {
+    if (one_warp) {
+      if (tid == 0) {
+        v[m] = found ? 1.0 : 0.0;
+        C[m] = l;
+      }
+      __syncwarp();
+      __syncthreads();
+      __syncthreads();
+    }
+    return found;
+  };
   double tr = 0.0;
   for (int i = 0; i < m; ++i) tr += A[i * (m + 1)];
-  if (!(tr > 0.0) || !isfinite(tr)) return false;
+  if (!(tr > 0.0) || !isfinite(tr)) {
+    lam = 0.0;
+    return finish(false, 0.0);
+  }
   const double inv_tr = 1.0 / tr;
   for (int k = tid; k < mm; k += nt) B[k] = A[k] * inv_tr;
-  __syncthreads();
+  sync();
   int left = -1;  // squarings still to run once converged
   for (int it = 0; it < max_squarings; ++it) {
     for (int k = tid; k < mm; k += nt) {
@@ -192,14 +224,14 @@ __device__ inline bool dominant_pair(const double* A, double* B, double* C, doub
       for (int l = 0; l < m; ++l) acc = fma(B[i + l * m], B[l + j * m], acc);
       C[k] = acc;
     }
-    __syncthreads();
+    sync();
     double s = 0.0;  // tr(B^2), the same in every thread
     for (int i = 0; i < m; ++i) s += C[i * (m + 1)];
     if (left < 0 && 1.0 - s <= 1e-12) left = 2;
     if (left == 0) break;
     const double inv_s = 1.0 / s;
     for (int k = tid; k < mm; k += nt) B[k] = C[k] * inv_s;
-    __syncthreads();
+    sync();
     if (left > 0) --left;
   }
   int j = 0;
@@ -208,19 +240,19 @@ __device__ inline bool dominant_pair(const double* A, double* B, double* C, doub
   double n2 = 0.0;
   for (int i = 0; i < m; ++i) n2 = fma(B[i + j * m], B[i + j * m], n2);
   const double inv_n = 1.0 / sqrt(n2);
-  __syncthreads();  // every thread has read B
+  sync();  // every thread has read B
   for (int i = tid; i < m; i += nt) v[i] = B[i + j * m] * inv_n;
-  __syncthreads();
+  sync();
   for (int i = tid; i < m; i += nt) {
     double acc = 0.0;
     for (int l = 0; l < m; ++l) acc = fma(A[i + l * m], v[l], acc);
     C[i] = acc;
   }
-  __syncthreads();
+  sync();
   lam = 0.0;
   for (int i = 0; i < m; ++i) lam = fma(v[i], C[i], lam);
-  __syncthreads();
-  return true;
+  sync();
+  return finish(true, lam);
 }
 
 // In-place Cholesky (lower) of an SPD k x k matrix A (+ ridge on the
