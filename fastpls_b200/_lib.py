@@ -67,6 +67,7 @@ SIGNATURES = {
     "fastpls_b200_server_stats": (_i, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                        C.POINTER(C.c_size_t)]),
     "fastpls_b200_server_batch_stats": (_i, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "fastpls_b200_server_set_borrow": (_i, [_vp, _i]),
     "fastpls_b200_fastcor": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _cp, _sz]),
     "fastpls_b200_fastsvd": (_i, [_vp, _i, _i, _i, _i, _i, _i, _ull, _vp, _vp, _vp, _cp, _sz]),
     "fastpls_b200_simpls_cv_permutation_classification": (

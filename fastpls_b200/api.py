@@ -636,9 +636,13 @@ def cv_permutation_classification(X, labels, classes, folds, permutations, prefi
 class Server:
     """Serving loop on the device (fastpls_b200_server_*): continuous
     admission of fit and predict requests by HBM footprint, resident models,
-    merged predictions per model. Fit tickets double as model ids."""
+    merged predictions per model. Fit tickets double as model ids.
 
-    def __init__(self, budget_bytes=150 * 10**9, workers=4):
+    borrow=True (default) submits inputs without a host copy: the server
+    reads the arrays in place, and this object keeps a reference to each
+    request's arrays until its wait() has returned (or close())."""
+
+    def __init__(self, budget_bytes=150 * 10**9, workers=4, borrow=True):
         err, cap = _lib.error_buffer()
         self._lib = _lib.load()
         self._h = self._lib.fastpls_b200_server_create(int(budget_bytes), int(workers), err, cap)
@@ -646,6 +650,9 @@ class Server:
             raise _lib.FastplsError(err.value.decode())
         self._models = {}
         self._pending = {}
+        self._held = {}
+        self._borrow = bool(borrow)
+        self._lib.fastpls_b200_server_set_borrow(self._h, 1 if self._borrow else 0)
 
     def submit_fit(self, X, Y=None, labels=None, classes=None, ncomp=2,
                    method="simpls", scaling="centering", precision=32, north=1,
@@ -671,6 +678,8 @@ class Server:
             C.byref(t), err, cap)
         _lib.check(rc, err)
         self._models[t.value] = (q, precision, p)
+        if self._borrow:
+            self._held[t.value] = (x, y, lab)
         return t.value
 
     def submit_predict(self, model, X, prefixes, lda=False):
@@ -684,6 +693,8 @@ class Server:
             _p(pre), len(pre), int(lda), C.byref(t), err, cap)
         _lib.check(rc, err)
         self._pending[t.value] = (x.shape[0], q, len(pre), precision)
+        if self._borrow:
+            self._held[t.value] = (x,)
         return t.value
 
     def wait(self, ticket, timeout=600.0):
@@ -698,11 +709,13 @@ class Server:
                 self._h, C.c_ulonglong(ticket), float(timeout), _p(out), out.nbytes,
                 C.byref(qms), C.byref(sms), err, cap)
             _lib.check(rc, err)
+            self._held.pop(ticket, None)  # the request has finished reading x
             return out.reshape((k, q, rows)).transpose(0, 2, 1), qms.value, sms.value
         rc = self._lib.fastpls_b200_server_wait(
             self._h, C.c_ulonglong(ticket), float(timeout), None, 0,
             C.byref(qms), C.byref(sms), err, cap)
         _lib.check(rc, err)
+        self._held.pop(ticket, None)
         return ticket, qms.value, sms.value
 
     def release(self, model):
@@ -725,6 +738,7 @@ class Server:
         if self._h:
             self._lib.fastpls_b200_server_destroy(self._h)
             self._h = None
+        self._held = {}  # no worker reads borrowed inputs any more
 
     def __del__(self):
         try:

@@ -46,6 +46,14 @@ struct Request {
   FitRequest fit;
   std::vector<unsigned char> x, y;
   std::vector<int> labels;
+  // borrowed inputs (the server's borrow mode): the caller's buffers, valid
+  // until the request has finished; null when the request owns copies
+  const unsigned char* bx = nullptr;
+  const unsigned char* by = nullptr;
+  const int* blabels = nullptr;
+  const unsigned char* xdata() const { return bx ? bx : x.data(); }
+  const void* ydata() const { return by ? static_cast<const void*>(by) : (y.empty() ? nullptr : y.data()); }
+  const int* labdata() const { return blabels ? blabels : (labels.empty() ? nullptr : labels.data()); }
   // prediction
   unsigned long long model = 0;
   int rows = 0;
@@ -365,9 +373,9 @@ class Server {
   void run_fit(Request* r, size_t charged) {
     size_t keep = 0;
     try {
-      r->fit.x = r->x.data();
-      r->fit.y = r->y.empty() ? nullptr : r->y.data();
-      r->fit.labels = r->labels.empty() ? nullptr : r->labels.data();
+      r->fit.x = r->xdata();
+      r->fit.y = r->ydata();
+      r->fit.labels = r->labdata();
       std::unique_ptr<ResidentHandle> h(make_handle(r->precision, r->fit));
       h->compact(false);  // training predictors are not needed for serving
       Model m;
@@ -405,9 +413,9 @@ class Server {
     for (size_t i = 0; i < batch.size(); ++i) {
       Request* r = batch[i];
       try {
-        r->fit.x = r->x.data();
-        r->fit.y = r->y.empty() ? nullptr : r->y.data();
-        r->fit.labels = r->labels.empty() ? nullptr : r->labels.data();
+        r->fit.x = r->xdata();
+        r->fit.y = r->ydata();
+        r->fit.labels = r->labdata();
         handles[i].reset(make_handle(r->precision, r->fit, true));
         if (PersistentPlan* pl = handles[i]->pending_plan()) {
           plans.push_back(pl);
@@ -500,7 +508,7 @@ class Server {
       for (auto* r : batch) {
         for (int j = 0; j < p; ++j)
           std::memcpy(x.data() + ((size_t)j * rows + off) * es,
-                      r->x.data() + (size_t)j * r->rows * es, (size_t)r->rows * es);
+                      r->xdata() + (size_t)j * r->rows * es, (size_t)r->rows * es);
         off += r->rows;
       }
       std::vector<unsigned char> out((size_t)rows * q * count * es);
@@ -528,6 +536,11 @@ class Server {
   }
 
   static constexpr int kFitBatchMax = 32;
+ public:
+  // borrow mode: submitted inputs are read in place (no host copy)
+  bool borrow = false;
+
+ private:
   size_t batched_launches_ = 0, batched_fits_ = 0;
   size_t budget_, in_use_ = 0;
   int device_ = 0;
@@ -599,9 +612,15 @@ FASTPLS_B200_API int fastpls_b200_server_submit_fit(
     r->kind = fpls::kFit;
     r->precision = precision;
     const size_t es = precision == 32 ? 4 : 8;
-    r->x.assign(static_cast<const unsigned char*>(x), static_cast<const unsigned char*>(x) + (size_t)n * p * es);
-    if (y) r->y.assign(static_cast<const unsigned char*>(y), static_cast<const unsigned char*>(y) + (size_t)n * q * es);
-    if (labels) r->labels.assign(labels, labels + n);
+    if (static_cast<Server*>(server)->borrow) {
+      r->bx = static_cast<const unsigned char*>(x);
+      r->by = static_cast<const unsigned char*>(y);
+      r->blabels = labels;
+    } else {
+      r->x.assign(static_cast<const unsigned char*>(x), static_cast<const unsigned char*>(x) + (size_t)n * p * es);
+      if (y) r->y.assign(static_cast<const unsigned char*>(y), static_cast<const unsigned char*>(y) + (size_t)n * q * es);
+      if (labels) r->labels.assign(labels, labels + n);
+    }
     auto& f = r->fit;
     f.method = method;
     f.n = n;
@@ -635,7 +654,10 @@ FASTPLS_B200_API int fastpls_b200_server_submit_predict(
     r->lda = lda;
     r->prefixes.assign(prefixes, prefixes + prefix_count);
     const size_t es = precision == 32 ? 4 : 8;
-    r->x.assign(static_cast<const unsigned char*>(x), static_cast<const unsigned char*>(x) + (size_t)rows * p * es);
+    if (static_cast<Server*>(server)->borrow)
+      r->bx = static_cast<const unsigned char*>(x);
+    else
+      r->x.assign(static_cast<const unsigned char*>(x), static_cast<const unsigned char*>(x) + (size_t)rows * p * es);
     *ticket = static_cast<Server*>(server)->submit(std::move(r));
   });
 }
@@ -689,6 +711,12 @@ FASTPLS_B200_API int fastpls_b200_server_batch_stats(void* server, size_t* launc
                                                      size_t* fits) {
   if (!server) return 1;
   static_cast<Server*>(server)->batch_stats(launches, fits);
+  return 0;
+}
+
+FASTPLS_B200_API int fastpls_b200_server_set_borrow(void* server, int on) {
+  if (!server) return 1;
+  static_cast<Server*>(server)->borrow = on != 0;
   return 0;
 }
 

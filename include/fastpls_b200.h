@@ -475,6 +475,13 @@ FASTPLS_B200_API int fastpls_b200_server_stats(void* server, size_t* bytes_in_us
  * they carried. */
 FASTPLS_B200_API int fastpls_b200_server_batch_stats(void* server, size_t* launches,
                                                      size_t* fits);
+/* Borrow mode (off by default): with on != 0, requests submitted afterwards
+ * read their x, y and labels in place instead of copying them at
+ * submission; the caller keeps those buffers valid and unchanged until
+ * fastpls_b200_server_wait has returned for the request (or the server is
+ * destroyed). Saves a host copy of every input (the Python Server holds
+ * references to the arrays until then). */
+FASTPLS_B200_API int fastpls_b200_server_set_borrow(void* server, int on);
 
 /* out (p x nb, FP64) = X^T V for device-resident X (n x p, leading
  * dimension ldx, FP32 or FP64 by `precision`), V (n x nb FP64, ldv) and out

@@ -30,9 +30,12 @@ def _kw(method, p):
     return dict(kernel="rbf", gamma=1.0 / p) if method == "kernelpls" else {}
 
 
-@pytest.mark.parametrize("budget,workers", [(150 * 10**9, 4), (300 * 10**6, 2)])
-def test_mixed_requests_match_standalone(budget, workers):
-    srv = api.Server(budget_bytes=budget, workers=workers)
+@pytest.mark.parametrize("budget,workers,borrow", [(150 * 10**9, 4, True), (300 * 10**6, 2, True),
+                                                    (150 * 10**9, 4, False)])
+def test_mixed_requests_match_standalone(budget, workers, borrow):
+    """Borrowed inputs (read in place, the default) and copied inputs give the
+    same bits as standalone calls."""
+    srv = api.Server(budget_bytes=budget, workers=workers, borrow=borrow)
     fits, preds = {}, {}
     for i, (method, n, p, q, a, cls) in enumerate(SPECS):
         x, y, lab = _data(i, method, n, p, q, cls)
