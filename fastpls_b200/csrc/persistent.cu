@@ -66,6 +66,19 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+// Arrival: releases this CTA's earlier writes (ordered before it by the CTA
+// barrier) and acquires those released by earlier arrivals, in one atomic.
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_add_release(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Barrier of the fit's CTAs with a deterministic reduction of their
 // partials (slots 0 .. count-1 of each CTA's row of cpart). Every thread of
@@ -84,9 +97,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 constexpr int kBarGroup = 32;
 constexpr int kFlatSlots = 64;
 template <class S, class A>
-__device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& after) {
+__device__ bool group_sync(const Fit& f, int* flag, unsigned& epoch, int count, S&& store, A&& after) {
   __shared__ int role_s, ok_s;  // role: 0 waits, 1 reduced its group, 2 reduces all
-  __shared__ unsigned gen_s;
   // per-thread sums of the flat reduction: dynamic shared memory past psm and
   // hs (the ring is idle at barriers; a static array would be duplicated per
   // instantiation)
@@ -97,18 +109,16 @@ __device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& af
   const int g = cta / kBarGroup;
   const int ngroups = (f.C + kBarGroup - 1) / kBarGroup;
   const int gsize = min(kBarGroup, f.C - g * kBarGroup);
+  // the generation after this barrier (every CTA passes the same barriers)
+  const unsigned target = epoch + 1u;
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    gen_s = ld_acquire(f.bar + 1);
-    __threadfence();
     ok_s = 1;
-    if (flat) role_s = atomicAdd(f.bar, 1u) == (unsigned)f.C - 1u ? 2 : 0;
-    else role_s = atomicAdd(f.bar + 2 + g, 1u) == (unsigned)gsize - 1u ? 1 : 0;
+    if (flat) role_s = atom_add_acq_rel(f.bar, 1u) == (unsigned)f.C - 1u ? 2 : 0;
+    else role_s = atom_add_acq_rel(f.bar + 2 + g, 1u) == (unsigned)gsize - 1u ? 1 : 0;
   }
   __syncthreads();
   if (role_s == 1) {
-    __threadfence();
     for (int k = threadIdx.x; k < count; k += PT) {
       const double* src = f.cpart + (long)g * kBarGroup * f.cslots + k;
       double sum = 0.0;
@@ -118,14 +128,12 @@ __device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& af
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      atomicExch(f.bar + 2 + g, 0u);
-      __threadfence();
-      if (atomicAdd(f.bar, 1u) == (unsigned)ngroups - 1u) role_s = 2;
+      st_relaxed(f.bar + 2 + g, 0u);
+      if (atom_add_acq_rel(f.bar, 1u) == (unsigned)ngroups - 1u) role_s = 2;
     }
     __syncthreads();
   }
   if (role_s == 2) {
-    __threadfence();
     if (flat) {
       if (count > 0) {
         const int Q = PT / count;
@@ -155,14 +163,12 @@ __device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& af
     after();
     __syncthreads();
     if (threadIdx.x == 0) {
-      __threadfence();
-      atomicExch(f.bar, 0u);
-      __threadfence();
-      atomicAdd(f.bar + 1, 1u);
+      st_relaxed(f.bar, 0u);
+      red_add_release(f.bar + 1, 1u);
     }
   } else if (threadIdx.x == 0) {
     const long long t0 = clock64();
-    while (ld_acquire(f.bar + 1) == gen_s) {
+    while ((int)(ld_acquire(f.bar + 1) - target) < 0) {
       if (clock64() - t0 > f.barrier_cycles) {
         flag_error(flag, 5);
         ok_s = 0;
@@ -172,13 +178,13 @@ __device__ bool group_sync(const Fit& f, int* flag, int count, S&& store, A&& af
     }
   }
   __syncthreads();
-  __threadfence();
+  epoch = target;
   return ok_s != 0;
 }
 
 // Barrier without partials.
-__device__ __forceinline__ bool group_sync(const Fit& f, int* flag) {
-  return group_sync(f, flag, 0, [](int, double) {}, [] {});
+__device__ __forceinline__ bool group_sync(const Fit& f, int* flag, unsigned& epoch) {
+  return group_sync(f, flag, epoch, 0, [](int, double) {}, [] {});
 }
 
 // CTA-level sum; every thread receives it.
@@ -571,6 +577,7 @@ __global__ void __launch_bounds__(PT, 2)
   double* const aux = reinterpret_cast<double*>(ring + Ring<T>::kBytes);
   const Region rg = region_of<T>(f, cta);
   unsigned seq = 0;  // stages streamed by this CTA so far
+  unsigned bar_epoch = 0;  // group barriers passed
   if (tid == 0) {
     for (int k = 0; k < Ring<T>::kStages; ++k) {
       ring_bar_init(ring_bars + k);
@@ -605,7 +612,7 @@ __global__ void __launch_bounds__(PT, 2)
           us[k - G] = v;
         }
       };
-      if (!group_sync(f, flag, G + m, store, [&] { direction_step(f, A, B, Cs, vd, us, flag); })) return;
+      if (!group_sync(f, flag, bar_epoch, G + m, store, [&] { direction_step(f, A, B, Cs, vd, us, flag); })) return;
     }
     for (int c = tid; c < m; c += PT) zs[c] = __ldcg(f.scal + SC_Z + c);
     __syncthreads();
@@ -669,7 +676,7 @@ __global__ void __launch_bounds__(PT, 2)
       if (tid < rg.rows) out[tid] = (acc0[0] + acc0[1]) + (acc0[2] + acc0[3]);
       if (r1 < rg.rows) out[r1] = (acc1[0] + acc1[1]) + (acc1[2] + acc1[3]);
     }
-    if (!group_sync(f, flag)) return;
+    if (!group_sync(f, flag, bar_epoch)) return;
     // P4: loading partials of the region, p_part[rbk][cols] = X[rows, cols]^T t[rows],
     // the stages backward. While the first stages are in flight each CTA
     // forms t for its row block: t = sum of the column ranges' partials - c
@@ -776,7 +783,7 @@ __global__ void __launch_bounds__(PT, 2)
       });
       if (!ok) return;
     }
-    if (!group_sync(f, flag, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; }, [] {}))
+    if (!group_sync(f, flag, bar_epoch, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; }, [] {}))
       return;
     // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
     if (tid == 0) {
@@ -829,7 +836,7 @@ __global__ void __launch_bounds__(PT, 2)
         if (lane == 0) f.cpart[(long)cta * f.cslots + k] = s;
       }
     }
-    if (!group_sync(f, flag, a + m,
+    if (!group_sync(f, flag, bar_epoch, a + m,
                     [&](int k, double v) {
                       if (k < a) {
                         f.scal[SC_H + k] = v;
@@ -868,7 +875,7 @@ __global__ void __launch_bounds__(PT, 2)
       }
       if (tid == 0) f.cpart[(long)cta * f.cslots] = vvp;
     }
-    if (!group_sync(f, flag, 1 + m,
+    if (!group_sync(f, flag, bar_epoch, 1 + m,
                     [&](int k, double v) {
                       if (k == 0) f.scal[SC_VV] = v;
                       else f.scal[SC_SV + k - 1] = v;

@@ -175,12 +175,104 @@ __device__ inline int jacobi_eigen(double* A, double* E, int m, int max_sweeps =
 // shared scratch (C with one extra slot), v (m + 1 slots) the shared
 // output; lam is returned in every thread. Returns false when tr(A) is not
 // positive and finite.
+// dominant_pair for order M <= 4 in one thread's registers: the same
+// operations in the same order as the shared-memory form below (so the same
+// bits), without its barriers. A is read from shared memory; v (M + 1) and
+// C[M] receive the result as in that form.
+template <int M>
+__device__ inline void dominant_pair_regs(const double* A, double* C, double* v, int max_squarings) {
+  double a[M * M], b[M * M], c[M * M];
+#pragma unroll
+  for (int k = 0; k < M * M; ++k) a[k] = A[k];
+  double tr = 0.0;
+#pragma unroll
+  for (int i = 0; i < M; ++i) tr += a[i * (M + 1)];
+  if (!(tr > 0.0) || !isfinite(tr)) {
+    v[M] = 0.0;
+    C[M] = 0.0;
+    return;
+  }
+  const double inv_tr = 1.0 / tr;
+#pragma unroll
+  for (int k = 0; k < M * M; ++k) b[k] = a[k] * inv_tr;
+  int left = -1;
+  for (int it = 0; it < max_squarings; ++it) {
+#pragma unroll
+    for (int k = 0; k < M * M; ++k) {
+      const int i = k % M, j = k / M;
+      double acc = 0.0;
+#pragma unroll
+      for (int l = 0; l < M; ++l) acc = fma(b[i + l * M], b[l + j * M], acc);
+      c[k] = acc;
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) s += c[i * (M + 1)];
+    if (left < 0 && 1.0 - s <= 1e-12) left = 2;
+    if (left == 0) break;
+    const double inv_s = 1.0 / s;
+#pragma unroll
+    for (int k = 0; k < M * M; ++k) b[k] = c[k] * inv_s;
+    if (left > 0) --left;
+  }
+  int j = 0;
+  double bjj = b[0];
+#pragma unroll
+  for (int i = 1; i < M; ++i)
+    if (b[i * (M + 1)] > bjj) {
+      bjj = b[i * (M + 1)];
+      j = i;
+    }
+  double col[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    double bij = b[i];
+#pragma unroll
+    for (int jj = 1; jj < M; ++jj)
+      if (jj == j) bij = b[i + jj * M];
+    col[i] = bij;
+  }
+  double n2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < M; ++i) n2 = fma(col[i], col[i], n2);
+  const double inv_n = 1.0 / sqrt(n2);
+  double vv[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) vv[i] = col[i] * inv_n;
+  double lam = 0.0;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    double acc = 0.0;
+#pragma unroll
+    for (int l = 0; l < M; ++l) acc = fma(a[i + l * M], vv[l], acc);
+    lam = fma(vv[i], acc, lam);
+  }
+#pragma unroll
+  for (int i = 0; i < M; ++i) v[i] = vv[i];
+  v[M] = 1.0;
+  C[M] = lam;
+}
+
 constexpr int kDominantMaxOrder = 64;  // callers size 3 m^2 + m + 2 shared doubles up to this order
 __device__ inline bool dominant_pair(const double* A, double* B, double* C, double* v, int m,
                                      double& lam, int max_squarings = 64) {
   // orders up to 8: the first warp alone with warp barriers (the squarings
   // are a few FMAs per lane; block barriers would dominate); the other
   // warps wait at the final barrier and read lam from the shared v slot
+  if (m <= 4) {
+    // one thread, registers only
+    if (threadIdx.x == 0) {
+      if (m == 1) dominant_pair_regs<1>(A, C, v, max_squarings);
+      else if (m == 2) dominant_pair_regs<2>(A, C, v, max_squarings);
+      else if (m == 3) dominant_pair_regs<3>(A, C, v, max_squarings);
+      else dominant_pair_regs<4>(A, C, v, max_squarings);
+    }
+    __syncthreads();
+    const bool found = v[m] != 0.0;
+    lam = C[m];
+    __syncthreads();
+    return found;
+  }
   const bool one_warp = m <= 8;
   if (one_warp && threadIdx.x >= 32) {
     __syncthreads();
