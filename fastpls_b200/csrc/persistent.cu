@@ -785,23 +785,32 @@ __global__ void __launch_bounds__(PT, 2)
     }
     if (!group_sync(f, flag, bar_epoch, 2, [&](int k, double v) { f.scal[k == 0 ? SC_T2 : SC_ST] = v; }, [] {}))
       return;
-    // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m)
+    // P5: p, R[:, a] = (S z) / |t|; partial V^T p (a) and S0^T R[:, a] (m).
+    // The column partials are loaded while thread 0 fetches |t|^2 and sum t.
     if (tid == 0) {
-      const double t2 = __ldcg(f.scal + SC_T2);
-      const double tn = sqrt(t2);
-      const bool ok = tn > 0.0 && isfinite(tn);
-      if (!ok && cta == 0) flag_error(flag, 1);
-      scal_s[0] = ok ? 1.0 / tn : 0.0;
+      scal_s[0] = __ldcg(f.scal + SC_T2);
       scal_s[1] = __ldcg(f.scal + SC_ST);
     }
-    __syncthreads();
-    const double inv_t = scal_s[0], sum_t = scal_s[1];
     double* ps = psm;          // p values of this CTA's columns (<= 2048)
     double* rs = psm + 2048;   // R values
     for (int jl = tid; jl < j1 - j0; jl += PT) {
       const int j = j0 + jl;
+      // sum u takes the row blocks k = u (mod 4) in order; eight loads per step
       double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
       int k = 0;
+      for (; k + 7 < f.Cr; k += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldcg(f.ppart + (long)(k + u) * p + j);
+        q0 += v[0];
+        q1 += v[1];
+        q2 += v[2];
+        q3 += v[3];
+        q0 += v[4];
+        q1 += v[5];
+        q2 += v[6];
+        q3 += v[7];
+      }
       for (; k + 3 < f.Cr; k += 4) {
         q0 += __ldcg(f.ppart + (long)k * p + j);
         q1 += __ldcg(f.ppart + (long)(k + 1) * p + j);
@@ -809,11 +818,24 @@ __global__ void __launch_bounds__(PT, 2)
         q3 += __ldcg(f.ppart + (long)(k + 3) * p + j);
       }
       for (; k < f.Cr; ++k) q0 += __ldcg(f.ppart + (long)k * p + j);
-      const double pr = (q0 + q1) + (q2 + q3);
       double rv = 0.0;
       for (int c = 0; c < m; ++c) rv = fma(__ldcg(f.S + j + (long)c * p), zs[c], rv);
-      const double pj = (pr - f.mean[j] * sum_t) / f.scale[j] * inv_t;
-      const double rj = rv * inv_t;
+      ps[jl] = (q0 + q1) + (q2 + q3);
+      rs[jl] = rv;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const double tn = sqrt(scal_s[0]);
+      const bool ok = tn > 0.0 && isfinite(tn);
+      if (!ok && cta == 0) flag_error(flag, 1);
+      scal_s[2] = ok ? 1.0 / tn : 0.0;
+    }
+    __syncthreads();
+    const double inv_t = scal_s[2], sum_t = scal_s[1];
+    for (int jl = tid; jl < j1 - j0; jl += PT) {
+      const int j = j0 + jl;
+      const double pj = (ps[jl] - f.mean[j] * sum_t) / f.scale[j] * inv_t;
+      const double rj = rs[jl] * inv_t;
       f.pv[j] = pj;
       f.R[j + (long)a * p] = rj;
       ps[jl] = pj;
@@ -821,19 +843,27 @@ __global__ void __launch_bounds__(PT, 2)
     }
     __syncthreads();
     {
+      // three of a warp's dot products at once (their loads in flight
+      // together); each is the lane-strided sum then the warp tree
       const int lane = tid & 31, warp = tid >> 5;
       const int cols = j1 - j0;
-      for (int k = warp; k < a + m; k += PT / 32) {
-        double s = 0.0;
-        if (k < a) {
-          const double* vk = f.V + (long)k * p + j0;
-          for (int jl = lane; jl < cols; jl += 32) s = fma(__ldcg(vk + jl), ps[jl], s);
-        } else {
-          const double* sk = f.S0 + (long)(k - a) * p + j0;
-          for (int jl = lane; jl < cols; jl += 32) s = fma(sk[jl], rs[jl], s);
+      constexpr int W = PT / 32;
+      for (int kb = warp; kb < a + m; kb += 3 * W) {
+        double sd[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const int k = kb + e * W;
+          if (k >= a + m) continue;
+          const double* src = k < a ? f.V + (long)k * p + j0 : f.S0 + (long)(k - a) * p + j0;
+          const double* w = k < a ? ps : rs;
+          for (int jl = lane; jl < cols; jl += 32) sd[e] = fma(__ldcg(src + jl), w[jl], sd[e]);
         }
-        s = warp_sum(s);
-        if (lane == 0) f.cpart[(long)cta * f.cslots + k] = s;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const int k = kb + e * W;
+          const double v = warp_sum(sd[e]);
+          if (lane == 0 && k < a + m) f.cpart[(long)cta * f.cslots + k] = v;
+        }
       }
     }
     if (!group_sync(f, flag, bar_epoch, a + m,
