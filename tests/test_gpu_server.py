@@ -137,9 +137,15 @@ def test_batched_fits_share_one_persistent_launch():
     for i, (n, p, q, a) in enumerate(specs):
         x, y = W.latent_regression(n, p, q, 4, 0.4, 300 + i, dtype=np.float32)
         data.append((x, y))
+    # a larger fit first keeps the one worker busy while the small fits queue
+    # up behind it (otherwise each small fit may finish before the next one
+    # is submitted, and nothing is left to batch)
+    xb, yb = W.latent_regression(6000, 12000, 3, 4, 0.4, 299, dtype=np.float32)
+    blocker = srv.submit_fit(xb, yb, ncomp=40, precision=32)
     for i, (n, p, q, a) in enumerate(specs):
         x, y = data[i]
         tickets.append(srv.submit_fit(x, y, ncomp=a, precision=32))
+    srv.wait(blocker)
     for t in tickets:
         srv.wait(t)
     stats = srv.batch_stats()
@@ -156,4 +162,5 @@ def test_batched_fits_share_one_persistent_launch():
         assert O.rel_err(got[1].astype(np.float64),
                          O.simpls_predict(ref, xt.astype(np.float64), a)) < 1e-5, i
         srv.release(tickets[i])
+    srv.release(blocker)
     srv.close()
