@@ -5,6 +5,7 @@
 // and the extern "C" shims of src/cuda_resident_api.cuh:1026-1353): return
 // 0 / non-null on success, 1 / NULL on error with a NUL-terminated message
 // in the caller's buffer; nothing throws across the boundary.
+#include "upload.cuh"
 #include "../../include/fastpls_b200.h"
 
 #include "batched.cuh"
@@ -171,7 +172,7 @@ void cv_permutation(const void* predictors, const void* responses,
     if (!device_inputs) {
       X.allocate((size_t)n * p, s);
       Y.allocate((size_t)n * q, s);
-      FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+      upload_h2d(X.get(), predictors, sizeof(T) * n * p, s);
       FPLS_CHECK(cudaMemcpyAsync(Y.get(), responses, sizeof(T) * n * q, cudaMemcpyHostToDevice, s));
       if (permutation_count > 0) {
         P.allocate((size_t)permutation_count * n, s);
@@ -284,7 +285,7 @@ void cv_permutation_classification(const T* predictors, const int* labels, const
   {
     DeviceArray<T> X((size_t)n * p, s), Y((size_t)n * classes, s);
     DeviceArray<int> P, L(n, s);
-    FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+    upload_h2d(X.get(), predictors, sizeof(T) * n * p, s);
     FPLS_CHECK(cudaMemcpyAsync(Y.get(), onehot.data(), sizeof(T) * n * classes, cudaMemcpyHostToDevice, s));
     FPLS_CHECK(cudaMemcpyAsync(L.get(), zero_based.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
     if (permutation_count > 0) {

@@ -8,6 +8,7 @@
 // fold model is fitted by the resident engine (fit.cu / plssvd.cu).
 // Folds run one after another here; the many-fold / many-permutation batched
 // engine lives in batched.cu.
+#include "upload.cuh"
 #include "cv.cuh"
 #include "handle.cuh"
 #include "lda.cuh"
@@ -128,7 +129,7 @@ void cv_regression(int method, const T* predictors, const T* responses,
   } guard{s};
   {
     DeviceArray<T> X((size_t)n * p, s), Y((size_t)n * q, s);
-    FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+    upload_h2d(X.get(), predictors, sizeof(T) * n * p, s);
     FPLS_CHECK(cudaMemcpyAsync(Y.get(), responses, sizeof(T) * n * q, cudaMemcpyHostToDevice, s));
     DeviceArray<double> Y64((size_t)n * q, s);
     to_f64_kernel<T><<<std::min<unsigned>(ceil_div((size_t)n * q, 256), 4 * num_sms()), 256, 0, s>>>(Y.get(), (long)n * q, Y64.get());
@@ -265,7 +266,7 @@ void cv_classification(int method, const T* predictors, const int* labels,
   } guard{s};
   {
     DeviceArray<T> X((size_t)n * p, s);
-    FPLS_CHECK(cudaMemcpyAsync(X.get(), predictors, sizeof(T) * n * p, cudaMemcpyHostToDevice, s));
+    upload_h2d(X.get(), predictors, sizeof(T) * n * p, s);
     DeviceArray<T> Xtr((size_t)fp.max_train * p, s), Xte((size_t)fp.max_test * p, s);
     DeviceArray<int> idx_tr(fp.max_train, s), idx_te(fp.max_test, s);
     DeviceArray<int> lab_tr(fp.max_train, s), top(fp.max_test, s);

@@ -2,6 +2,7 @@
 // kernels). Behavioural contract: src/cuda_resident_api.cuh:69-479 of the
 // reference (validation order, error strings, field sizes, synchronous
 // calls on a per-handle non-blocking stream).
+#include "upload.cuh"
 #include "handle.cuh"
 #include "persistent.cuh"
 #include "lda.cuh"
@@ -473,7 +474,7 @@ class TypedHandle final : public ResidentHandle {
     timer_.reset(new FitTimer(stream_));
     FitTimer& timer = *timer_;
     xtrain_.allocate((size_t)n * p, stream_);
-    FPLS_CHECK(cudaMemcpyAsync(xtrain_.get(), rq_.x, sizeof(T) * n * p, cudaMemcpyHostToDevice, stream_));
+    upload_h2d(xtrain_.get(), rq_.x, sizeof(T) * n * p, stream_);
     DeviceArray<TO> y;
     if (cls) {
       model_.labels.allocate(n, stream_);
@@ -593,7 +594,7 @@ class TypedHandle final : public ResidentHandle {
 
   void upload_rows(const void* x, int rows) {
     xbuf_.reserve((size_t)rows * rq_.p, stream_);
-    FPLS_CHECK(cudaMemcpyAsync(xbuf_.get(), x, sizeof(T) * rows * rq_.p, cudaMemcpyHostToDevice, stream_));
+    upload_h2d(xbuf_.get(), x, sizeof(T) * rows * rq_.p, stream_);
   }
 
   void download(const double* src, long count, TO* dst) {

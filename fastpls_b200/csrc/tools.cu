@@ -17,6 +17,7 @@
 // truncated SVD. The Gaussian draws come from a counter-based generator
 // (SplitMix64 hashing of (seed, index) into Box-Muller pairs), so a seed
 // reproduces the sketch on any device.
+#include "upload.cuh"
 #include "../../include/fastpls_b200.h"
 #include "kernels.cuh"
 #include "small.cuh"
@@ -96,7 +97,7 @@ void fastcor_impl(const T* a, const T* b, int rows_a, int cols_a, int rows_b,
     }
   } guard{s};
   DeviceArray<T> da((size_t)rows_a * cols_a, s), db;
-  FPLS_CHECK(cudaMemcpyAsync(da.get(), a, sizeof(T) * rows_a * cols_a, cudaMemcpyHostToDevice, s));
+  upload_h2d(da.get(), a, sizeof(T) * rows_a * cols_a, s);
   DeviceArray<double> L((size_t)units_a * feats, s), R;
   unit_normalize<T><<<std::min(units_a, 8 * num_sms()), TB, 0, s>>>(da.get(), rows_a, cols_a, byrow,
                                                                       L.get(), units_a, feats);
