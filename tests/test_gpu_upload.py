@@ -36,3 +36,25 @@ def test_staged_upload_matches_pinned_source():
     ref = O.simpls_fit(x.astype(np.float64), y.astype(np.float64), ncomp=a)
     want = O.simpls_predict(ref, probe.astype(np.float64), a)
     assert O.rel_err(got[1].astype(np.float64), want) < 1e-5
+
+
+def test_concurrent_staged_uploads_in_the_server():
+    """Fits above the staging threshold submitted to four server workers at
+    once (their uploads share the pooled pinned slots and copy threads) give
+    the models of the same fits made alone, bit for bit."""
+    specs = [(2100 + 97 * i, 1500 + 53 * i, 1 + i % 3, 4 + i % 3) for i in range(6)]  # 12-20 MB each
+    data = [W.latent_regression(n, p, q, 4, 0.4, 900 + i, dtype=np.float32)
+            for i, (n, p, q, a) in enumerate(specs)]
+    srv = api.Server(workers=4)
+    tickets = [srv.submit_fit(x, y, ncomp=a, precision=32)
+               for (x, y), (n, p, q, a) in zip(data, specs)]
+    for t in tickets:
+        srv.wait(t)
+    for i, ((x, y), (n, p, q, a)) in enumerate(zip(data, specs)):
+        probe = np.asfortranarray(x[::11])
+        got, _, _ = srv.wait(srv.submit_predict(tickets[i], probe, [a]))
+        alone = api.fit_resident(x, y, ncomp=a, precision=32)
+        assert np.array_equal(got, alone.predict_path(probe, [a])), i
+        alone.close()
+        srv.release(tickets[i])
+    srv.close()
