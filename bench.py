@@ -82,19 +82,30 @@ def make_workload(rank: int, perms: int):
 
 
 def clock_sampler_start(path):
-    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     try:
         f = open(path, "w")
         p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
                               "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL)
+        import atexit
+
+        def _end(proc=p):  # never leave the sampler running past this process
+            if proc.poll() is None:
+                proc.kill()
+        atexit.register(_end)
         return p, f
     except Exception:
         return None, None
 
 
-def clock_sampler_stop(handle, path, device_index):
+def clock_sampler_stop(handle, path, device_index, window=None):
+    """Median SM clock and the throttle reasons seen; with window = (t0, t1)
+    (time.time() around the timed region) only the samples taken inside it
+    (the sampler runs from well before, so that its start-up does not fall
+    into the timed steps)."""
+    from datetime import datetime
     p, f = handle
     if p is None:
         return None
@@ -108,14 +119,21 @@ def clock_sampler_stop(handle, path, device_index):
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     for line in open(path):
         parts = [s.strip() for s in line.split(",")]
-        if len(parts) < 9 or parts[0] != str(device_index):
+        if len(parts) < 10 or parts[1] != str(device_index):
             continue
+        if window is not None:
+            try:
+                ts = datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                continue
+            if ts < window[0] or ts > window[1]:
+                continue
         try:
-            sm.append(float(parts[1]))
-            mx = float(parts[2])
+            sm.append(float(parts[2]))
+            mx = float(parts[3])
         except ValueError:
             continue
-        for name, val in zip(names, parts[5:9]):
+        for name, val in zip(names, parts[6:10]):
             if val.lower() == "active":
                 reasons.add(name)
     if not sm:
@@ -658,6 +676,10 @@ def main():
     lib = _lib.load()
     dev = torch.device("cuda", local)
 
+    # clock sampler: started now so that nvidia-smi's start-up is over before
+    # the timed steps; only its samples inside the timed window are used
+    clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
+    clk = clock_sampler_start(clk_path)
     x, y, folds, perms, prefixes = make_workload(rank, a.perms)
     Pn = perms.shape[0]
     fits_per_step = (Pn + 1) * FOLDS
@@ -714,21 +736,22 @@ def main():
     lib.fastpls_b200_set_batch_lanes(a.lanes)
     lanes = lib.fastpls_b200_batch_lanes()
 
-    clk_path = os.path.join(tempfile.gettempdir(), f"fpls_clocks_{rank}.csv")
-    clk = clock_sampler_start(clk_path)
     for _ in range(max(a.warmup, 3)):
         step_device()
     barrier()
     launches0 = lib.fastpls_b200_launch_count()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
     barrier()
+    t_lo = time.time()
     ev[0].record(stream)
     for s in range(a.steps):
         step_device()
         ev[s + 1].record(stream)
     barrier()
+    t_hi = time.time()
     launches = lib.fastpls_b200_launch_count() - launches0
-    clocks = clock_sampler_stop(clk, clk_path, local)
+    # at least the samples of the last 0.6 s for a very short timed region
+    clocks = clock_sampler_stop(clk, clk_path, local, (min(t_lo, t_hi - 0.6), t_hi + 0.05))
     step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(a.steps)]
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     observed_q2 = outs[1].reshape(Pn + 1, k)[0].copy()
