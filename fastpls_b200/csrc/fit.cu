@@ -710,7 +710,7 @@ void project_rows(const DeviceModel& model, const T* X, int rows, long ld,
   count_launch();
   FPLS_LAUNCH("scaled_weights");
   xr_product<T>(X, rows, p, ld, Rs.get(), p, k, roff, out, ldo,
-                ws.stream_partial, stream);
+                ws.stream_partial, stream, ws.flag.get());
 }
 
 void predict_from_scores(const DeviceModel& model, const double* scores,

@@ -59,10 +59,20 @@ void class_moments(const T* X, int n, int p, long ld, const int* labels, int m,
 
 // out[i + c*n] = sum_j X[i,j] * R[j + c*ldr] - offset[c]   (c < nb)
 // (scores of a scaled/centred X folded into R and offset). FP64 result.
+// flag (optional): set to 5 if a bulk-copy stage of the one-pass form never
+// arrives (a bounded wait ran out).
 template <class T>
 void xr_product(const T* X, int n, int p, long ld, const double* R, long ldr,
                 int nb, const double* offset, double* out, long ldo,
-                DeviceArray<double>& scratch, cudaStream_t stream);
+                DeviceArray<double>& scratch, cudaStream_t stream, int* flag = nullptr);
+
+// The one-pass form of xr_product for 3 <= nb <= 16 columns (persistent.cu):
+// X streamed once through the single fit's bulk-copy stages, each stage also
+// carrying its rows of R. Returns false (nothing enqueued) for shapes it does
+// not take.
+template <class T>
+bool xr_ring(const T* X, int n, int p, long ld, const double* R, long ldr, int nb,
+             const double* offset, double* out, long ldo, int* flag, cudaStream_t stream);
 
 // out[j + c*p] = sum_i X[i,j] * V[i + c*ldv]   (c < nb, FP64)
 template <class T>

@@ -218,14 +218,23 @@ constexpr int kAuxDoubles = 1024; // rt of the region's columns / t of its rows
 // rows, kStages stages, about 100 KB of ring per CTA so that two CTAs fit
 // an SM. Each stage carries 8192 elements (16 per thread, 4096 for FP64)
 // so that the per-stage handshake is small beside the consume work.
-template <class T>
+// EXTRA: bytes a stage carries after its column segments (the projection's
+// slice of R; 0 for the fit).
+template <class T, int EXTRA = 0>
 struct Ring {
   static constexpr int kColStride = kBlockRows * (int)sizeof(T) + 16;
   static constexpr int kCols = sizeof(T) == 8 ? 8 : 16;
-  static constexpr int kStageBytes = kCols * kColStride;
+  static constexpr int kStageBytes = kCols * kColStride + EXTRA;
   static constexpr int kStages = sizeof(T) == 2 ? 5 : 3;
   static constexpr int kBytes = kStages * kStageBytes;
   static constexpr int kDynBytes = kBytes + kAuxDoubles * (int)sizeof(double);
+};
+// No extra copy per stage.
+struct NoExtra {
+  __device__ void operator()(int, const void*& src, unsigned& bytes) const {
+    src = nullptr;
+    bytes = 0;
+  }
 };
 constexpr int kMaxRingStages = 8;
 static_assert(kBlockRows == 2 * PT, "the scores pass gives each thread two rows of a block");
@@ -380,26 +389,34 @@ __device__ __forceinline__ bool stage_ends(const Fit& f, const T* X, const Regio
 }
 
 // Warp 0: the bulk copies of stage `st` into `slot`, one lane per column,
-// completing on `bar`.
-template <class T>
+// completing on `bar`; lane G::kCols copies the stage's extra bytes, if any,
+// behind the segments.
+template <class G, class T, class E = NoExtra>
 __device__ void issue_stage(const Fit& f, const T* X, const Region& g, int st, unsigned char* slot,
-                            uint64_t* bar) {
+                            uint64_t* bar, const E& extra = E()) {
   const int lane = threadIdx.x & 31;
-  const int nc = min(Ring<T>::kCols, g.cols - st * Ring<T>::kCols);
+  const int nc = min(G::kCols, g.cols - st * G::kCols);
   Segment sg;
   unsigned bytes = 0;
+  const void* xsrc = nullptr;
   if (lane < nc) {
-    sg = segment(f, X, g, g.c0 + st * Ring<T>::kCols + lane);
+    sg = segment(f, X, g, g.c0 + st * G::kCols + lane);
     if (sg.hi > sg.lo) bytes = (unsigned)(sg.hi - sg.lo);
+  } else if (lane == G::kCols) {
+    extra(st, xsrc, bytes);
   }
   unsigned total = bytes;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
   if (lane == 0) ring_expect(bar, total);
   __syncwarp();
-  if (bytes > 0)
-    bulk_to_smem(slot + lane * Ring<T>::kColStride + sg.off + ((long)sg.lo - (long)sg.g),
-                 reinterpret_cast<const void*>(sg.lo), bytes, bar);
+  if (bytes > 0) {
+    if (lane < nc)
+      bulk_to_smem(slot + lane * G::kColStride + sg.off + ((long)sg.lo - (long)sg.g),
+                   reinterpret_cast<const void*>(sg.lo), bytes, bar);
+    else
+      bulk_to_smem(slot + G::kCols * G::kColStride, xsrc, bytes, bar);
+  }
 }
 
 // Streams the region's stages through the ring: issues the first stages,
@@ -411,21 +428,22 @@ __device__ void issue_stage(const Fit& f, const T* X, const Region& g, int st, u
 // warps, reset by that warp). `seq` numbers the CTA's stages across passes
 // (slot seq % stages, mbarrier parity (seq / stages) & 1). Returns false
 // when a stage never arrived (flag 5 set, the copies in flight waited for).
-template <class T, class P, class F>
+template <class G, class T, class P, class F, class E = NoExtra>
 __device__ bool stream_region(const Fit& f, const T* X, const Region& g, bool backward,
                               unsigned& seq, unsigned char* ring, uint64_t* bars, unsigned* done,
-                              unsigned* issued, int* flag, P&& prepare, F&& consume) {
-  constexpr int NS = Ring<T>::kStages;
+                              unsigned* issued, int* flag, P&& prepare, F&& consume,
+                              const E& extra = E()) {
+  constexpr int NS = G::kStages;
   constexpr unsigned kWarps = PT / 32;
   const int nst = g.nst;
   const int lane = threadIdx.x & 31;
   auto stage_of = [&](int k) { return backward ? nst - 1 - k : k; };
-  auto slot_of = [&](int k) { return ring + (size_t)((seq + k) % NS) * Ring<T>::kStageBytes; };
+  auto slot_of = [&](int k) { return ring + (size_t)((seq + k) % NS) * G::kStageBytes; };
   __syncthreads();  // the ring is free (earlier passes and phases are done with it)
   if (threadIdx.x < 32) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     for (int k = 0; k < min(NS, nst); ++k)
-      issue_stage(f, X, g, stage_of(k), slot_of(k), bars + (seq + k) % NS);
+      issue_stage<G>(f, X, g, stage_of(k), slot_of(k), bars + (seq + k) % NS, extra);
     if (lane == 0) *issued = (unsigned)min(NS, nst);
   }
   prepare();  // (whole CTA) while the first stages are in flight
@@ -449,7 +467,7 @@ __device__ bool stream_region(const Fit& f, const T* X, const Region& g, bool ba
       if (lane == 0) done[sl] = 0u;
       if (k + NS < nst) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_stage(f, X, g, stage_of(k + NS), slot_of(k), bars + sl);
+        issue_stage<G>(f, X, g, stage_of(k + NS), slot_of(k), bars + sl, extra);
         if (lane == 0) atomicAdd(issued, 1u);
       }
     }
@@ -633,7 +651,7 @@ __global__ void __launch_bounds__(PT, 2)
           aux[j] = rv / f.scale[rg.c0 + j];
         }
       };
-      const bool ok = stream_region(f, X, rg, false, seq, ring, ring_bars, ring_done, &ring_issued, flag, rt,
+      const bool ok = stream_region<Ring<T>>(f, X, rg, false, seq, ring, ring_bars, ring_done, &ring_issued, flag, rt,
                                     [&](int st, const unsigned char* slot) {
         const int nc = min(SC, rg.cols - st * SC);
         const double* w = aux + st * SC;
@@ -722,7 +740,7 @@ __global__ void __launch_bounds__(PT, 2)
       // interleaved sums over the rows in a fixed order, then the warp tree
       constexpr int SC = Ring<T>::kCols;
       constexpr int CPW = SC / (PT / 32);
-      const bool ok = stream_region(f, X, rg, true, seq, ring, ring_bars, ring_done, &ring_issued, flag, tv,
+      const bool ok = stream_region<Ring<T>>(f, X, rg, true, seq, ring, ring_bars, ring_done, &ring_issued, flag, tv,
                                     [&](int st, const unsigned char* slot) {
         const int nc = min(SC, rg.cols - st * SC);
         const int cb = rg.c0 + st * SC;
@@ -928,6 +946,103 @@ __global__ void __launch_bounds__(PT, 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Projection X R (n x p times p x nb, nb <= NB <= 16) in one pass over X: the
+// regions and ring of the fit's scores pass, each stage also carrying the
+// matching rows of Rt (R row-major, NB doubles per row, zero past nb) behind
+// its column segments. Each thread keeps its two rows' NB sums over the
+// region's columns in order; part[(range * nb + b) * n + row] receives them
+// (the column ranges are summed in order afterwards). A normal launch: CTAs
+// never wait on each other.
+constexpr int kRSlice = 16 * 16 * 8;  // bytes of Rt a stage can carry (16 rows x 16)
+
+template <class T, int NB>
+__global__ void __launch_bounds__(PT, 2)
+    xr_ring_kernel(const Fit f, const double* __restrict__ Rt, int nb, double* __restrict__ part) {
+  using G = Ring<T, kRSlice>;
+  constexpr int SC = G::kCols;
+  static_assert(NB % 2 == 0 && NB <= 16 && SC * NB * 8 <= kRSlice, "Rt slice of a stage");
+  extern __shared__ __align__(16) double psm[];
+  __shared__ __align__(8) uint64_t ring_bars[kMaxRingStages];
+  __shared__ unsigned ring_done[kMaxRingStages], ring_issued;
+  const T* X = static_cast<const T*>(f.X);
+  const int tid = threadIdx.x;
+  unsigned char* const ring = reinterpret_cast<unsigned char*>(psm);
+  const Region rg = region_of<T>(f, blockIdx.x);
+  if (tid == 0) {
+    for (int k = 0; k < G::kStages; ++k) {
+      ring_bar_init(ring_bars + k);
+      ring_done[k] = 0u;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned seq = 0;
+  double acc0[NB], acc1[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) acc0[b] = acc1[b] = 0.0;
+  const int r1 = tid + PT;
+  const bool in0 = tid < rg.rows, in1 = r1 < rg.rows;
+  auto extra = [&](int st, const void*& src, unsigned& bytes) {
+    const int cb = rg.c0 + st * SC;
+    const int nc = min(SC, rg.cols - st * SC);
+    src = Rt + (long)cb * NB;
+    bytes = (unsigned)(nc * NB * (int)sizeof(double));
+  };
+  const bool ok = stream_region<G>(f, X, rg, false, seq, ring, ring_bars, ring_done, &ring_issued, f.flag,
+                                   [] {}, [&](int st, const unsigned char* slot) {
+    const int nc = min(SC, rg.cols - st * SC);
+    const int cb = rg.c0 + st * SC;
+    const double* rs = reinterpret_cast<const double*>(slot + SC * G::kColStride);
+    if (nc == SC && !stage_ends(f, X, rg, st)) {
+      // rows past the block read stale shared memory; their sums are never stored
+#pragma unroll 2
+      for (int c = 0; c < SC; ++c) {
+        const T* col = reinterpret_cast<const T*>(slot + c * G::kColStride + rg.off(cb + c));
+        const double x0 = as_f64(col[tid]), x1 = as_f64(col[r1]);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const double w = rs[c * NB + b];
+          acc0[b] = fma(x0, w, acc0[b]);
+          acc1[b] = fma(x1, w, acc1[b]);
+        }
+      }
+    } else {
+      for (int c = 0; c < nc; ++c) {
+        const T* col = reinterpret_cast<const T*>(slot + c * G::kColStride + rg.off(cb + c));
+        const Segment sg = segment(f, X, rg, cb + c);
+        const T* gcol = X + (long)(cb + c) * f.ld + rg.r0;  // rows outside the copy
+        const double x0 = in0 ? as_f64(tid < sg.head || tid >= sg.tail0 ? gcol[tid] : col[tid]) : 0.0;
+        const double x1 = in1 ? as_f64(r1 < sg.head || r1 >= sg.tail0 ? gcol[r1] : col[r1]) : 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          const double w = rs[c * NB + b];
+          acc0[b] = fma(x0, w, acc0[b]);
+          acc1[b] = fma(x1, w, acc1[b]);
+        }
+      }
+    }
+  }, extra);
+  if (!ok) return;
+  double* out = part + (long)rg.crg * nb * f.n + rg.r0;
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    if (b < nb) {
+      if (in0) out[(long)b * f.n + tid] = acc0[b];
+      if (in1) out[(long)b * f.n + r1] = acc1[b];
+    }
+  }
+}
+
+// Rt[j * NB + b] = R[j + b * ldr] for b < nb, 0 for nb <= b < NB.
+__global__ void transpose_rows(const double* __restrict__ R, long ldr, int p, int nb, int NB,
+                               double* __restrict__ Rt) {
+  const long total = (long)p * NB;
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < total; k += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(k / NB), b = (int)(k % NB);
+    Rt[k] = b < nb ? R[j + (long)b * ldr] : 0.0;
+  }
+}
 
 }  // namespace
 
@@ -1100,6 +1215,88 @@ void launch_persistent(const std::vector<PersistentPlan*>& plans, cudaStream_t s
   FPLS_LAUNCH("persistent_simpls");
   // the descriptors are freed stream-ordered, behind the launch
 }
+
+namespace {
+
+// out[i + b ldo] = sum over the column ranges k (in order) of
+// part[(k nb + b) n + i] - offset[b].
+__global__ void ring_finish(const double* __restrict__ part, int ranges, int n, int nb,
+                            const double* offset, double* out, long ldo) {
+  const long total = (long)n * nb;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % n), b = (int)(idx / n);
+    double v = 0.0;
+    for (int k = 0; k < ranges; ++k) v += part[((long)k * nb + b) * n + i];
+    if (offset) v -= offset[b];
+    out[i + (long)b * ldo] = v;
+  }
+}
+
+template <class T, int NB>
+void launch_xr_ring(const Fit& f, const double* Rt, int nb, double* part, cudaStream_t s) {
+  const int dyn = Ring<T, kRSlice>::kBytes;
+  static const bool configured = [dyn] {
+    FPLS_CHECK(cudaFuncSetAttribute(xr_ring_kernel<T, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return true;
+  }();
+  (void)configured;
+  xr_ring_kernel<T, NB><<<f.C, PT, dyn, s>>>(f, Rt, nb, part);
+  count_launch();
+  FPLS_LAUNCH("xr_ring_kernel");
+}
+
+}  // namespace
+
+template <class T>
+bool xr_ring(const T* X, int n, int p, long ld, const double* R, long ldr, int nb,
+             const double* offset, double* out, long ldo, int* flag, cudaStream_t s) {
+  if (nb < 3 || nb > 16 || n < 1 || p < 1) return false;
+  const int NB = nb <= 4 ? 4 : nb <= 8 ? 8 : nb <= 10 ? 10 : nb <= 12 ? 12 : 16;
+  // row blocks of at most kBlockRows rows, about one wave of two CTAs per SM
+  int Cr = (n + kBlockRows - 1) / kBlockRows;
+  const int rb = round_up((n + Cr - 1) / Cr, 8);
+  Cr = (n + rb - 1) / rb;
+  const int Cc = std::max(1, 2 * num_sms() / Cr);
+  Fit f{};
+  f.X = X;
+  f.ld = ld;
+  f.n = n;
+  f.p = p;
+  f.Cr = Cr;
+  f.rb = rb;
+  f.Cc = Cc;
+  f.pc = (p + Cc - 1) / Cc;
+  f.C = Cr * Cc;
+  f.elem = (int)sizeof(T);
+  f.flag = flag;
+  DeviceArray<double> Rt((size_t)p * NB, s), part((size_t)Cc * nb * n, s);
+  const long tot = (long)p * NB;
+  transpose_rows<<<(unsigned)std::min<long>((tot + 255) / 256, 8L * num_sms()), 256, 0, s>>>(R, ldr, p, nb, NB,
+                                                                                            Rt.get());
+  count_launch();
+  FPLS_LAUNCH("transpose_rows");
+  switch (NB) {
+    case 4: launch_xr_ring<T, 4>(f, Rt.get(), nb, part.get(), s); break;
+    case 8: launch_xr_ring<T, 8>(f, Rt.get(), nb, part.get(), s); break;
+    case 10: launch_xr_ring<T, 10>(f, Rt.get(), nb, part.get(), s); break;
+    case 12: launch_xr_ring<T, 12>(f, Rt.get(), nb, part.get(), s); break;
+    default: launch_xr_ring<T, 16>(f, Rt.get(), nb, part.get(), s); break;
+  }
+  const long total = (long)n * nb;
+  ring_finish<<<(unsigned)std::min<long>((total + 255) / 256, 8L * num_sms()), 256, 0, s>>>(
+      part.get(), Cc, n, nb, offset, out, ldo);
+  count_launch();
+  FPLS_LAUNCH("ring_finish");
+  return true;
+}
+
+template bool xr_ring<float>(const float*, int, int, long, const double*, long, int, const double*,
+                             double*, long, int*, cudaStream_t);
+template bool xr_ring<double>(const double*, int, int, long, const double*, long, int, const double*,
+                              double*, long, int*, cudaStream_t);
+template bool xr_ring<bf16>(const bf16*, int, int, long, const double*, long, int, const double*,
+                            double*, long, int*, cudaStream_t);
 
 template bool plan_simpls_persistent<float>(const float*, int, int, long, int, int, DeviceModel&,
                                             DeviceArray<double>&, double*, Workspace&, cudaStream_t,

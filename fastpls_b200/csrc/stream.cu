@@ -701,7 +701,12 @@ void xtv_product(const T* X, int n, int p, long ld, const double* V, long ldv,
 template <class T>
 void xr_product(const T* X, int n, int p, long ld, const double* R, long ldr,
                 int nb, const double* offset, double* out, long ldo,
-                DeviceArray<double>& scratch, cudaStream_t stream) {
+                DeviceArray<double>& scratch, cudaStream_t stream, int* flag) {
+  // 3..16 columns of a large X: one pass over X on bulk-copy stages instead
+  // of a pass per 8 columns
+  if (nb >= 3 && nb <= 16 && (long)n * p >= (1L << 24) &&
+      xr_ring<T>(X, n, p, ld, R, ldr, nb, offset, out, ldo, flag, stream))
+    return;
   for (int c0 = 0; c0 < nb; c0 += 8) {
     const int w = std::min(8, nb - c0);
     const double* off = offset ? offset + c0 : nullptr;
@@ -747,7 +752,7 @@ void topk_rows(const double* values, int rows, int classes, int top, int* out,
                                cudaStream_t);                                 \
   template void xr_product<T>(const T*, int, int, long, const double*, long,  \
                               int, const double*, double*, long,              \
-                              DeviceArray<double>&, cudaStream_t);            \
+                              DeviceArray<double>&, cudaStream_t, int*);      \
   template void gather_rows<T>(const T*, long, int, const int*, int, T*,      \
                                long, cudaStream_t);
 FPLS_INSTANTIATE(float)
